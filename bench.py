@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Scan-path benchmark: one JSON line on rank 0.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME]
+
+A "step" is one scan of the configuration's whole input (already resident in
+HBM) by the full pattern set.  The default configuration is the 500-regex
+scan over 1 GiB of Markov text (learned-speculative DFA walk, with the plain
+thread-per-start kernel timed beside it).  Under torchrun every rank scans its
+own copy of the workload (weak scaling, no collective on the data path); the
+reported time is the max over ranks.
+
+--impl reference times the oracle port of the reference's CPU algorithm for
+the same configuration on the host cores (the reference is a Rust crate with
+un-vendored dependencies and a wgpu GPU path, neither runnable here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import workloads as W  # noqa: E402
+
+CONFIGS = {
+    "regex": "500 regexes (2-4 literal alternations joined by [class]{1,8}), 1 GiB order-1 Markov printable ASCII",
+    "literals_large": "10,000 literals (8-32 B, printable Zipf 1.1), 1 GiB order-1 Markov printable ASCII",
+    "literals_small": "100 literals (4-16 B, a-z), 16 MiB iid a-z",
+    "batch": "200,000 lognormal items (median 4 KiB, sigma 1.5), 1,500 literals + 500 regexes",
+    "dna": "4 GiB ACGT with 1% N runs, 50,000 k-mers + 200 IUPAC regexes",
+}
+METRIC = "scan GB/s, learned-speculative vs plain DFA kernel, exact match sets, 1 B200"
+
+
+def make_workload(name: str, size: int | None):
+    if name == "regex":
+        return W.regex(size=size or W.GiB)
+    if name == "literals_large":
+        return W.literals_large(size=size or W.GiB)
+    if name == "literals_small":
+        return W.literals_small(size=size or 16 * W.MiB)
+    if name == "batch":
+        return W.batch()
+    if name == "dna":
+        return W.dna(size=size or 4 * W.GiB)
+    raise SystemExit(f"unknown config {name}")
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(kernel: str, config: str):
+    """Bytes per launch from the committed ncu summary, if one exists."""
+    p = ROOT / "profiles" / f"{kernel}_{config}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "100", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(wl, seconds: float = 12.0):
+    """Oracle port of the reference's CPU algorithm on a bounded sample."""
+    import oracle
+    threads = oracle.hw_threads()
+    pats = wl.patterns
+    data = wl.data
+    probe = min(len(data), 1 << 20)
+    t = time.perf_counter()
+    oracle.scan_patterns(pats, data[:probe], threads)
+    dt = max(time.perf_counter() - t, 1e-6)
+    n = int(min(len(data), max(probe, probe * seconds / dt)))
+    t = time.perf_counter()
+    oracle.scan_patterns(pats, data[:n], threads)
+    dt = time.perf_counter() - t
+    return {"value": round(n / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} bytes of the same input ({n / dt / 1e6:.1f} MB/s over {dt:.1f} s)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    wl = make_workload(args.config, args.size)
+    base = cpu_baseline(wl, seconds=max(2.0, 60.0 / max(args.steps + args.warmup, 1)))
+    vals = [base["value"]]
+    line = {"metric": METRIC, "value": base["value"], "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": args.config, "description": CONFIGS[args.config]},
+            "impl": "reference", "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "oracle port of the reference CPU algorithm (the Rust crate and its wgpu path cannot run here)"}
+    del vals
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="regex", choices=sorted(CONFIGS))
+    ap.add_argument("--size", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import warpstate_b200 as ws
+
+    wl = make_workload(args.config, args.size)
+    n_bytes = int(wl.data.nbytes)
+    ps = ws.PatternSet.builder()
+    for kind, p in wl.patterns:
+        ps = ps.literal_bytes(p) if kind == 0 else ps.regex(p.decode())
+    ps = ps.build()
+
+    cfg = ws.AutoMatcherConfig().max_matches(8 << 20).profile(True)
+    plain = None
+    if args.config == "regex":
+        cfg.regex_mode(ws.REGEX_SPECULATIVE)
+        pcfg = ws.AutoMatcherConfig().max_matches(8 << 20).profile(True).regex_mode(ws.REGEX_PLAIN)
+        plain = ws.GpuMatcher.with_config(ps, pcfg)
+    m = ws.GpuMatcher.with_config(ps, cfg)
+
+    d_in = torch.from_numpy(wl.data).to(f"cuda:{local}")
+    cap = 8 << 20
+    d_out = torch.empty((cap, 3), dtype=torch.int32, device=f"cuda:{local}")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    flush = None
+    if n_bytes < (256 << 20):
+        flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def timed_steps(matcher, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            matcher.scan_device(d_in.data_ptr(), n_bytes, d_out.data_ptr(), cap, d_cnt.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total = 0.0
+        kern = []
+        infos = []
+        for _ in range(steps):
+            if flush is not None:
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            matcher.scan_device(d_in.data_ptr(), n_bytes, d_out.data_ptr(), cap, d_cnt.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            inf = matcher.info()
+            kern.append(inf["last_kernel_ms"])
+            infos.append(inf)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return total / steps, kern, infos
+
+    # speculative (or the only) path
+    with ClockSampler(local) as clk:
+        ms, kern, infos = timed_steps(m, args.steps, args.warmup)
+    clocks = clk.summary()
+    count = int(d_cnt.item())
+    if count > cap:
+        raise SystemExit(f"match overflow ({count} > {cap})")
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * n_bytes / (ms_max * 1e-3) / 1e9
+
+    plain_gbs = None
+    plain_ms = None
+    if plain is not None:
+        pms, _, _ = timed_steps(plain, max(2, args.steps // 2), 1)
+        pt = torch.tensor([pms], dtype=torch.float64, device=f"cuda:{local}")
+        if dist:
+            dist.all_reduce(pt, op=dist.ReduceOp.MAX)
+        plain_ms = float(pt.item())
+        plain_gbs = world * n_bytes / (plain_ms * 1e-3) / 1e9
+        plain_count = int(d_cnt.item())
+        if plain_count != count:
+            raise SystemExit(f"plain/speculative match counts differ: {plain_count} vs {count}")
+
+    # roofline of the dominant kernel
+    peak, peak_kind = load_peaks()
+    if args.config == "regex":
+        kidx, kname = 1, "dfa_walk"
+    else:
+        kidx, kname = 0, "literal_scan"
+    kms = statistics.mean(k[kidx] for k in kern) if kern else None
+    alg_bytes = n_bytes + 12 * count
+    achieved = alg_bytes / (kms * 1e-3) / 1e9 if kms else None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 2) if achieved else None, "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4) if achieved else None,
+                "traffic": read_traffic(kname, args.config), "kernel": kname,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": alg_bytes}
+
+    # end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty(n_bytes, dtype=torch.uint8, pin_memory=True)
+        pinned.numpy()[:] = wl.data
+        hv = pinned.numpy()
+        m.scan_array(hv)
+        torch.cuda.synchronize()
+        k = max(2, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(k):
+            res = m.scan_array(hv)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / k
+        if len(res) != count:
+            raise SystemExit(f"e2e count {len(res)} != device count {count}")
+        e2e = {"value": round(world * n_bytes / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": n_bytes,
+               "d2h_bytes_per_step": 8 + 12 * count, "ms_per_step": round(dt * 1e3, 3)}
+
+    base = None
+    if rank == 0 and not args.no_cpu:
+        base = cpu_baseline(wl)
+
+    launches = infos[-1]["last_launches"] if infos else 0
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_max, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": args.config, "description": CONFIGS[args.config], "bytes_per_rank": n_bytes,
+                   "patterns": len(wl.patterns), "matches": count,
+                   "l2": "input larger than L2" if flush is None else "L2 flushed (512 MiB write) between steps",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": roofline,
+        "cpu_baseline": base,
+        "e2e": e2e,
+        "gpu_launches": int(launches) * args.steps,
+        "clocks": clocks,
+    }
+    if plain_gbs is not None:
+        last = infos[-1]
+        line["regex"] = {"speculative_gbs": round(value, 3), "plain_gbs": round(plain_gbs, 3),
+                         "speedup_vs_plain": round(value / plain_gbs, 3), "plain_ms_per_step": round(plain_ms, 4),
+                         "proposer_top1": last["proposer_top1"], "proposer_top4": last["proposer_top4"],
+                         "fixup_chunks": last["last_fixup_chunks"], "chunks": last["last_chunks"],
+                         "groups": last["n_groups"], "states": last["total_states"],
+                         "phase_ms": [round(x, 4) for x in last["last_kernel_ms"]]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

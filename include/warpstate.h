@@ -1,0 +1,223 @@
+/*
+ * warpstate_b200 -- C ABI of the B200-native scan path.
+ *
+ * The reference (a Rust crate) drives its GPU scan through GpuMatcher
+ * (core/src/gpu/mod.rs), the batch helpers (core/src/batch.rs) and
+ * StreamPipeline (core/src/pipeline.rs).  This header is what a Rust shim binds
+ * in their place: plain pointers and sizes, caller-owned output buffers, no
+ * allocation handed across the boundary, status codes that map 1:1 onto the
+ * reference's Error enum (core/src/error.rs:6-91).
+ *
+ * Semantics of a scan (the parity contract):
+ *   - literal patterns: every occurrence, overlapping, duplicates reported under
+ *     each id (what the reference's GPU literal kernels compute,
+ *     core/src/gpu/shader.rs:56-98,174-227);
+ *   - regex patterns: per regex, regex::bytes find_iter with multi_line(true) and
+ *     unicode(false): leftmost-first, non-overlapping (what GpuMatcher::scan
+ *     returns for regexes, core/src/gpu/dispatch.rs:357-378 ->
+ *     core/src/dfa/scan.rs:433-456);
+ *   - output sorted by (start, pattern_id, end) (core/src/cpu/mod.rs:56-78).
+ *
+ * Threading: a ws_matcher is immutable after creation; ws_scan* may be called
+ * concurrently from many host threads (each call takes its own stream and
+ * scratch from the matcher's pool), as GpuMatcher is shared across threads in
+ * the reference (tests/adversarial/adversarial_gpu.rs:537-580).
+ */
+#ifndef WARPSTATE_B200_H
+#define WARPSTATE_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; each maps to one variant of core/src/error.rs:6-91. */
+typedef enum {
+  WS_OK = 0,
+  WS_ERR_EMPTY_PATTERN_SET = 1,     /* Error::EmptyPatternSet */
+  WS_ERR_EMPTY_PATTERN = 2,         /* Error::EmptyPattern{index} */
+  WS_ERR_NO_DEVICE = 3,             /* Error::NoGpuAdapter */
+  WS_ERR_DEVICE = 4,                /* Error::GpuDeviceError{reason} */
+  WS_ERR_BUFFER_MAP = 5,            /* Error::BufferMapFailed */
+  WS_ERR_COMPILE = 6,               /* Error::PatternCompilationFailed{reason} */
+  WS_ERR_DFA_OOB = 7,               /* Error::DfaOutOfBounds */
+  WS_ERR_PATTERN_TOO_LARGE = 8,     /* Error::PatternTooLarge */
+  WS_ERR_PATTERN_SET_TOO_LARGE = 9, /* Error::PatternSetTooLarge */
+  WS_ERR_INPUT_TOO_LARGE = 10,      /* Error::InputTooLarge{bytes,max_bytes} */
+  WS_ERR_OVERFLOW = 11,             /* Error::MatchBufferOverflow{count,max} */
+  WS_ERR_PATHOLOGICAL = 12,         /* Error::PathologicalRegex{index} */
+  WS_ERR_TIMEOUT = 13,              /* Error::GpuDeviceError{"... timed out"} */
+  WS_ERR_INVALID_ARGUMENT = 14      /* caller bug (null pointer, bad size) */
+} ws_status;
+
+/* Match { pattern_id, start, end } -- three u32, 12 bytes, the reference's
+ * layout (asserted at core/src/dfa/mod.rs:416-419). */
+typedef struct { uint32_t pattern_id, start, end; } ws_match;
+
+/* batch::TaggedMatch (core/src/batch.rs:22-27): offsets relative to the item. */
+typedef struct { uint64_t source_id; uint32_t pattern_id, start, end, reserved; } ws_tagged_match;
+
+/* batch::ScanItem (core/src/batch.rs:13-18). */
+typedef struct { uint64_t id; const uint8_t* data; uint64_t len; } ws_item;
+
+/* Matches of a stream carry 64-bit offsets (a stream may exceed 4 GiB). */
+typedef struct { uint32_t pattern_id, reserved; uint64_t start, end; } ws_match64;
+
+/* Extra error detail filled by calls that can fail with a payload. */
+typedef struct {
+  uint64_t index;      /* EmptyPattern / PatternTooLarge / PathologicalRegex */
+  uint64_t count;      /* MatchBufferOverflow.count, InputTooLarge.bytes */
+  uint64_t max;        /* MatchBufferOverflow.max, InputTooLarge.max_bytes */
+  char message[512];   /* reason text for GpuDeviceError / PatternCompilationFailed */
+} ws_error_info;
+
+typedef struct ws_ctx ws_ctx;
+typedef struct ws_ir ws_ir;
+typedef struct ws_matcher ws_matcher;
+typedef struct ws_stream ws_stream;
+
+/* ------------------------------------------------------------------ context */
+/* One context per device: holds the CUDA context binding and the caching
+ * allocator.  Replaces acquire_device / GpuBufferPool
+ * (core/src/gpu/device.rs:9-84,158-189). */
+ws_status ws_ctx_create(int device, ws_ctx** out, ws_error_info* err);
+void ws_ctx_destroy(ws_ctx* ctx);
+int ws_device_count(void);
+
+/* --------------------------------------------------------------- pattern IR */
+/* Pattern kinds for ws_ir_build. */
+enum { WS_PATTERN_LITERAL = 0, WS_PATTERN_REGEX = 1 };
+typedef struct {
+  uint32_t kind;            /* WS_PATTERN_LITERAL or WS_PATTERN_REGEX */
+  const uint8_t* bytes;     /* literal bytes, or the regex source (UTF-8) */
+  uint64_t len;
+} ws_pattern_spec;
+
+/* PatternSetBuilder::build (core/src/pattern/compiler.rs:97-340), host only:
+ * literal packing, FNV-1a prefix hashes with hash_window_len = 8, regex parse
+ * and validation, pathological-repetition rejection, literal demotion, and the
+ * LiteralPrefilterTable.  Pattern ids are the insertion indices. */
+ws_status ws_ir_build(const ws_pattern_spec* patterns, uint64_t n, int case_insensitive,
+                      ws_ir** out, ws_error_info* err);
+void ws_ir_destroy(ws_ir* ir);
+
+/* A read-only view of the IR, laid out as the reference's PatternIR
+ * (core/src/pattern/ir.rs:6-34) and LiteralPrefilterTable
+ * (core/src/literal_prefilter.rs:10-19).  A Rust shim fills this struct from
+ * its own PatternIR and passes it to ws_matcher_create. */
+typedef struct {
+  const uint8_t* packed_bytes; uint64_t packed_len;
+  const uint32_t* offsets;             /* 2 per literal: (start, len) */
+  const uint32_t* literal_pattern_ids; /* user pattern id per literal */
+  uint32_t n_literals;
+  uint32_t hash_window_len;            /* 8 in the reference */
+  const uint32_t* prefix_meta;         /* 4 per prefix length */
+  const uint32_t* bucket_ranges;       /* 2 per bucket */
+  uint32_t n_buckets;
+  const uint32_t* entries;             /* 2 per literal: (hash, literal index) */
+  const char* const* regex_sources;    /* NUL-terminated sources */
+  const uint32_t* regex_pattern_ids;
+  uint32_t n_regex;
+  uint32_t n_patterns;                 /* total patterns (literals + regexes) */
+  uint32_t case_insensitive;
+} ws_pattern_tables;
+
+ws_status ws_ir_tables(const ws_ir* ir, ws_pattern_tables* out);
+
+/* ------------------------------------------------------------------ matcher */
+/* AutoMatcherConfig (core/src/config.rs:39-173) plus the B200 plan knobs. */
+typedef struct {
+  uint64_t gpu_threshold;          /* default 65536 */
+  uint64_t gpu_max_input_size;     /* default 128 MiB */
+  uint64_t max_matches;            /* default 1,000,000 */
+  uint64_t chunk_size;             /* default 128 MiB */
+  uint64_t chunk_overlap;          /* default 4096 */
+  uint32_t regex_mode;             /* WS_REGEX_* below */
+  uint32_t dfa_max_states;         /* per DFA group; default 8192 */
+  uint32_t walk_chunk;             /* speculative chunk bytes; default 4096 */
+  uint32_t proposer;               /* WS_PROPOSER_* below */
+  uint64_t proposer_train_bytes;   /* default 256 MiB */
+  uint64_t proposer_seed;          /* corpus seed for proposer training */
+  uint32_t flags;                  /* WS_FLAG_* below */
+  uint32_t reserved[7];
+} ws_config;
+
+enum { WS_REGEX_SPECULATIVE = 0, WS_REGEX_PLAIN = 1 };
+enum { WS_PROPOSER_MLP = 0, WS_PROPOSER_NONE = 1 };
+/* WS_FLAG_PROFILE: record CUDA events around every kernel phase of a scan so
+ * ws_matcher_get_info reports per-phase device times (one caller at a time). */
+enum { WS_FLAG_PROFILE = 1 };
+
+void ws_config_default(ws_config* cfg);
+
+/* GpuMatcher::with_config (core/src/gpu/mod.rs:113-220): uploads the literal
+ * tables, builds the regex DFAs (forward, reverse, per-pattern priority), trains
+ * the boundary proposer and keeps everything resident on the device. */
+ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* tables,
+                            const ws_config* cfg, ws_matcher** out, ws_error_info* err);
+void ws_matcher_destroy(ws_matcher* m);
+
+/* GpuMatcher::scan (core/src/gpu/mod.rs:223-388).  data/len are host memory
+ * (pinned or pageable).  Writes up to cap matches sorted by (start, pattern_id,
+ * end); *n_out receives the true count.  When the count exceeds cap or the
+ * configured max_matches, returns WS_ERR_OVERFLOW with err->count = true count
+ * (re-call with a larger buffer; there is no CPU fallback). */
+ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len,
+                  ws_match* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
+
+/* Device-resident variant: d_data is a 16-byte aligned device pointer, d_out a
+ * device buffer of cap matches, d_count a device u64 that receives the true
+ * match count (only min(count, cap) matches are written; count > cap means
+ * overflow).  Nothing is copied to the host and the output is unsorted.  All
+ * work is enqueued on `stream` (a cudaStream_t, 0 = legacy default stream) and
+ * the call returns without synchronising. */
+ws_status ws_scan_device(ws_matcher* m, const uint8_t* d_data, uint64_t len,
+                         ws_match* d_out, uint64_t cap, uint64_t* d_count,
+                         void* stream, ws_error_info* err);
+
+/* scan_batch / scan_batch_gpu (core/src/batch.rs:170-363): every item scanned
+ * independently in one launch sequence, matches tagged with the item id and
+ * sorted by (source_id, start, pattern_id, end); no cross-item matches. */
+ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t n_items,
+                        ws_tagged_match* out, uint64_t cap, uint64_t* n_out,
+                        ws_error_info* err);
+
+/* StreamPipeline (core/src/pipeline.rs:87-153) with state carry: feed bytes in
+ * pieces of any size; matches are reported once, with global 64-bit offsets,
+ * as soon as they are final.  The union over all feeds plus end equals ws_scan
+ * of the concatenation. */
+ws_status ws_stream_begin(ws_matcher* m, ws_stream** out, ws_error_info* err);
+ws_status ws_stream_feed(ws_stream* s, const uint8_t* data, uint64_t len,
+                         ws_match64* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
+ws_status ws_stream_end(ws_stream* s, ws_match64* out, uint64_t cap, uint64_t* n_out,
+                        ws_error_info* err);
+void ws_stream_destroy(ws_stream* s);
+
+/* Introspection for tests and the benchmark. */
+typedef struct {
+  uint32_t n_literals, n_regex, n_groups;
+  uint32_t total_states;         /* forward DFA states over all groups */
+  uint32_t max_classes;
+  uint32_t filter_q, filter_period, filter_bits;
+  double proposer_top1, proposer_top4;  /* held-out hit rates after training */
+  uint64_t last_fixup_chunks, last_chunks;
+  uint64_t last_kcandidates;
+  double last_kernel_ms[8];      /* literal, walk, propose, fixup, reverse, resolve, plain, total */
+  uint32_t last_launches;
+} ws_matcher_info;
+ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
+
+/* Diagnostic entry points used by the parity tests: the K-candidate set
+ * (pattern_id, start, end) of every anchored regex match, computed by the plain
+ * thread-per-start kernel (mode WS_REGEX_PLAIN) or by the speculative walk plus
+ * reverse walk (WS_REGEX_SPECULATIVE).  Host buffers, unsorted. */
+ws_status ws_regex_candidates(ws_matcher* m, const uint8_t* data, uint64_t len, uint32_t mode,
+                              ws_match* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
+
+const char* ws_status_name(ws_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

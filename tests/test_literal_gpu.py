@@ -1,0 +1,129 @@
+"""Literal path on the GPU against the oracle (contract L), bit-exact."""
+import numpy as np
+import pytest
+
+import oracle
+import workloads as w
+from conftest import case_input
+
+pytestmark = pytest.mark.gpu
+
+
+def _ws():
+    import warpstate_b200 as ws
+    return ws
+
+
+def gpu_scan(patterns, data, **cfg):
+    ws = _ws()
+    b = ws.PatternSet.builder()
+    for kind, p in patterns:
+        b = b.literal_bytes(p) if kind == 0 else b.regex(p.decode() if isinstance(p, bytes) else p)
+    c = ws.AutoMatcherConfig()
+    for k, v in cfg.items():
+        getattr(c, k)(v)
+    m = ws.GpuMatcher.with_config(b.build(), c)
+    return m, m.scan_array(data)
+
+
+def check(patterns, data, **cfg):
+    _, got = gpu_scan(patterns, data, **cfg)
+    exp = oracle.scan_patterns(patterns, data)
+    assert got.shape == exp.shape, (got.shape, exp.shape)
+    assert np.array_equal(got, exp)
+    return got
+
+
+def test_golden_literal_cases(golden):
+    for case in golden["literal_overlapping"]:
+        pats = [(0, p.encode()) for p in case["patterns"]]
+        _, got = gpu_scan(pats, case_input(case))
+        exp = oracle.sort_matches(np.array(case["expected"], dtype=np.uint32).reshape(-1, 3))
+        assert got.tolist() == exp.tolist(), case["src"]
+
+
+def test_literals_small_full_size():
+    wl = w.literals_small()  # 100 literals, 16 MiB
+    got = check(wl.patterns, wl.data)
+    assert len(got) >= 256
+
+
+def test_literals_large_scaled():
+    wl = w.literals_large(size=64 << 20)
+    got = check(wl.patterns, wl.data)
+    assert len(got) >= 4096
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 15, 16, 17, 31, 33, 63, 64, 65, 511, 512, 513, 4097])
+def test_ragged_lengths_and_tail_matches(n):
+    rng = np.random.default_rng(n)
+    data = bytearray(rng.integers(ord("a"), ord("d"), size=n, dtype=np.uint8).tobytes())
+    lits = [b"a", b"ab", b"abc", b"abcd", b"bcda", b"cabcab", b"dcbadcb", b"abcdabcd", b"d" * 9]
+    tail = lits[n % len(lits)]
+    if len(tail) <= n:
+        data[n - len(tail):] = tail  # a literal ending on the last byte
+    check([(0, l) for l in lits], bytes(data))
+
+
+def test_binary_and_duplicate_literals():
+    rng = np.random.default_rng(5)
+    data = rng.integers(0, 256, size=1 << 20, dtype=np.uint8)
+    lits = [bytes([0, 255, 66, 19, 55]), bytes([0, 0, 0, 0]), bytes([255]), b"\x00\x01", b"\x00\x01"]
+    data[1000:1005] = np.frombuffer(lits[0], dtype=np.uint8)
+    data[5000:5010] = 0
+    check([(0, l) for l in lits], data)
+
+
+def test_mixed_lengths_periods():
+    # minimum long-literal length 4, 5 and 7 select filter periods 1, 2 and 4
+    rng = np.random.default_rng(9)
+    data = rng.integers(ord("a"), ord("h"), size=3 << 20, dtype=np.uint8)
+    for lmin in (4, 5, 6, 7, 8):
+        lits = [bytes(rng.integers(ord("a"), ord("h"), size=int(rng.integers(lmin, lmin + 10)), dtype=np.uint8))
+                for _ in range(300)]
+        check([(0, l) for l in lits], data)
+
+
+def test_empty_input_and_overflow():
+    ws = _ws()
+    m, got = gpu_scan([(0, b"aa")], b"")
+    assert len(got) == 0
+    c = ws.AutoMatcherConfig().max_matches(10)
+    mm = ws.GpuMatcher.with_config(ws.PatternSet.builder().literal("aa").build(), c)
+    with pytest.raises(ws.MatchBufferOverflow) as ei:
+        mm.scan(b"a" * 101)
+    assert ei.value.count == 100 and ei.value.max == 10
+
+
+def test_device_resident_scan_equals_host_scan():
+    import torch
+    ws = _ws()
+    wl = w.literals_small(size=4 << 20)
+    m, host = gpu_scan(wl.patterns, wl.data)
+    d = torch.from_numpy(wl.data.copy()).cuda()
+    cap = 1 << 16
+    out = torch.zeros((cap, 3), dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    m.scan_device(d.data_ptr(), d.numel(), out.data_ptr(), cap, cnt.data_ptr())
+    n = int(cnt.item())
+    dev = oracle.sort_matches(out[:n].cpu().numpy().astype(np.uint32))
+    assert np.array_equal(dev, host)
+
+
+def test_concurrent_scans_share_one_matcher():
+    import threading
+    wl = w.literals_small(size=2 << 20)
+    m, ref = gpu_scan(wl.patterns, wl.data)
+    errs = []
+
+    def run():
+        try:
+            for _ in range(3):
+                assert np.array_equal(m.scan_array(wl.data), ref)
+        except Exception as e:  # pragma: no cover
+            errs.append(e)
+
+    th = [threading.Thread(target=run) for _ in range(4)]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    assert not errs

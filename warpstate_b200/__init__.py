@@ -1,0 +1,686 @@
+"""warpstate_b200 -- B200-native (sm_100a) GPU scan path of warpstate.
+
+Python mirror of the reference's Rust API for the scan path, over the C ABI in
+include/warpstate.h:
+
+* ``PatternSet.builder() ... .build()``  (core/src/pattern/compiler.rs:97)
+* ``GpuMatcher`` / ``WarpStateer``: ``new``, ``with_config``, ``scan``,
+  ``scan_blocking``, ``scan_block``, ``max_block_size`` (core/src/gpu/mod.rs:95-445)
+* ``GpuScanner`` (core/src/gpu/scanner.rs:14-120)
+* ``AutoMatcher``: always routes to the GPU (core/src/router.rs:59-305)
+* ``ScanItem``, ``TaggedMatch``, ``scan_batch``, ``scan_batch_gpu``,
+  ``scan_batch_auto``, ``BatchConfig`` (core/src/batch.rs)
+* ``StreamPipeline`` (core/src/pipeline.rs:87-153)
+* ``AutoMatcherConfig`` (core/src/config.rs:39-173) and the ``Error`` family
+  (core/src/error.rs:6-91).
+
+Scan semantics: literal patterns report every (overlapping) occurrence;
+regex patterns report regex::bytes ``find_iter`` matches (leftmost-first,
+non-overlapping, multi_line on, Unicode off); results are sorted by
+``(start, pattern_id, end)``.  Everything runs on the GPU; there is no CPU
+fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Iterable, NamedTuple, Sequence
+
+import numpy as np
+
+from . import _native as N
+
+__all__ = [
+    "Match", "Error", "EmptyPatternSet", "EmptyPattern", "NoGpuAdapter", "GpuDeviceError", "BufferMapFailed",
+    "PatternCompilationFailed", "DfaOutOfBounds", "PatternTooLarge", "PatternSetTooLarge", "InputTooLarge",
+    "MatchBufferOverflow", "PathologicalRegex", "PatternSet", "PatternSetBuilder", "AutoMatcherConfig",
+    "GpuMatcher", "WarpStateer", "GpuScanner", "AutoMatcher", "ScanItem", "TaggedMatch", "BatchConfig",
+    "scan_batch", "scan_batch_gpu", "scan_batch_auto", "StreamPipeline", "REGEX_SPECULATIVE", "REGEX_PLAIN",
+]
+
+REGEX_SPECULATIVE = 0
+REGEX_PLAIN = 1
+PROPOSER_MLP = 0
+PROPOSER_NONE = 1
+
+
+class Match(NamedTuple):
+    """``Match { pattern_id, start, end }`` (three u32)."""
+    pattern_id: int
+    start: int
+    end: int
+
+
+# ------------------------------------------------------------------ errors
+class Error(Exception):
+    """Base of the error family of core/src/error.rs:6-91."""
+
+
+class EmptyPatternSet(Error):
+    pass
+
+
+class EmptyPattern(Error):
+    def __init__(self, index, msg=""):
+        super().__init__(msg or f"pattern {index} is empty")
+        self.index = index
+
+
+class NoGpuAdapter(Error):
+    pass
+
+
+class GpuDeviceError(Error):
+    def __init__(self, reason):
+        super().__init__(reason)
+        self.reason = reason
+
+
+class BufferMapFailed(Error):
+    pass
+
+
+class PatternCompilationFailed(Error):
+    def __init__(self, reason):
+        super().__init__(reason)
+        self.reason = reason
+
+
+class DfaOutOfBounds(Error):
+    pass
+
+
+class PatternTooLarge(Error):
+    def __init__(self, index, nbytes, maximum):
+        super().__init__(f"pattern {index} has {nbytes} bytes (max {maximum})")
+        self.index, self.bytes, self.max = index, nbytes, maximum
+
+
+class PatternSetTooLarge(Error):
+    pass
+
+
+class InputTooLarge(Error):
+    def __init__(self, nbytes, max_bytes):
+        super().__init__(f"scan input is too large ({nbytes} bytes, max {max_bytes})")
+        self.bytes, self.max_bytes = nbytes, max_bytes
+
+
+class MatchBufferOverflow(Error):
+    def __init__(self, count, maximum):
+        super().__init__(f"too many matches ({count} exceeds {maximum})")
+        self.count, self.max = count, maximum
+
+
+class PathologicalRegex(Error):
+    def __init__(self, index):
+        super().__init__(f"regex pattern {index} contains nested repetitions (pathological)")
+        self.index = index
+
+
+def _raise(status: int, err: N.WsErrorInfo):
+    msg = err.message.decode(errors="replace")
+    if status == 1:
+        raise EmptyPatternSet(msg)
+    if status == 2:
+        raise EmptyPattern(err.index, msg)
+    if status == 3:
+        raise NoGpuAdapter(msg)
+    if status == 4:
+        raise GpuDeviceError(msg)
+    if status == 5:
+        raise BufferMapFailed(msg)
+    if status == 6:
+        raise PatternCompilationFailed(msg)
+    if status == 7:
+        raise DfaOutOfBounds(msg)
+    if status == 8:
+        raise PatternTooLarge(err.index, err.count, err.max)
+    if status == 9:
+        raise PatternSetTooLarge(msg)
+    if status == 10:
+        raise InputTooLarge(err.count, err.max)
+    if status == 11:
+        raise MatchBufferOverflow(err.count, err.max)
+    if status == 12:
+        raise PathologicalRegex(err.index)
+    if status == 13:
+        raise GpuDeviceError(msg or "GPU operation timed out")
+    raise ValueError(msg or f"invalid argument (status {status})")
+
+
+def _call(fn, *args):
+    err = N.WsErrorInfo()
+    st = fn(*args, ctypes.byref(err))
+    if st != 0:
+        _raise(st, err)
+
+
+# ------------------------------------------------------------ input views
+def _buffer(data):
+    """(pointer, length, keepalive) for bytes-like or numpy input, zero-copy."""
+    if isinstance(data, np.ndarray):
+        a = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+        return a.ctypes.data, a.nbytes, a
+    if isinstance(data, (bytes,)):
+        p = ctypes.c_char_p(data)
+        return ctypes.cast(p, ctypes.c_void_p).value, len(data), (data, p)
+    if isinstance(data, (bytearray, memoryview)):
+        mv = memoryview(data).cast("B")
+        if mv.readonly:
+            b = bytes(mv)
+            return _buffer(b)
+        arr = (ctypes.c_char * mv.nbytes).from_buffer(mv) if mv.nbytes else None
+        return (ctypes.addressof(arr) if arr is not None else 0), mv.nbytes, (mv, arr)
+    if hasattr(data, "data_ptr") and hasattr(data, "numel"):  # a CPU torch tensor (e.g. pinned)
+        return data.data_ptr(), data.numel() * data.element_size(), data
+    raise TypeError(f"unsupported input type {type(data)!r}")
+
+
+# ---------------------------------------------------------- pattern set
+class PatternSetBuilder:
+    """Builder for PatternSet (core/src/pattern/compiler.rs:13-93)."""
+
+    def __init__(self):
+        self._patterns: list[tuple[int, bytes, str | None]] = []
+        self._ci = False
+        self._dfa_size_limit = 50_000_000
+
+    def literal(self, pattern: str):
+        self._patterns.append((0, pattern.encode("utf-8"), None))
+        return self
+
+    def literal_bytes(self, pattern: bytes):
+        self._patterns.append((0, bytes(pattern), None))
+        return self
+
+    def named_literal(self, name: str, pattern: str):
+        self._patterns.append((0, pattern.encode("utf-8"), name))
+        return self
+
+    def regex(self, pattern: str):
+        self._patterns.append((1, pattern.encode("utf-8"), None))
+        return self
+
+    def named_regex(self, name: str, pattern: str):
+        self._patterns.append((1, pattern.encode("utf-8"), name))
+        return self
+
+    def case_insensitive(self, yes: bool):
+        self._ci = bool(yes)
+        return self
+
+    def dfa_size_limit(self, limit: int):
+        self._dfa_size_limit = int(limit)
+        return self
+
+    def build(self) -> "PatternSet":
+        L = N.lib()
+        n = len(self._patterns)
+        specs = (N.WsPatternSpec * max(n, 1))()
+        keep = []
+        for i, (k, b, _) in enumerate(self._patterns):
+            buf = ctypes.create_string_buffer(b, len(b)) if b else None
+            keep.append(buf)
+            specs[i].kind = k
+            specs[i].bytes = ctypes.cast(buf, ctypes.c_void_p).value if buf is not None else None
+            specs[i].len = len(b)
+        h = ctypes.c_void_p()
+        _call(L.ws_ir_build, specs, n, 1 if self._ci else 0, ctypes.byref(h))
+        return PatternSet(h, [p[2] for p in self._patterns], self._dfa_size_limit)
+
+
+class PatternSet:
+    """A compiled pattern set (core/src/pattern/mod.rs:74-279), host side."""
+
+    def __init__(self, handle, names, dfa_size_limit):
+        self._h = handle
+        self.names = names
+        self.dfa_size_limit = dfa_size_limit
+        t = N.WsPatternTables()
+        _call_noerr(N.lib().ws_ir_tables, self._h, ctypes.byref(t))
+        self._tables = t
+
+    @staticmethod
+    def builder() -> PatternSetBuilder:
+        return PatternSetBuilder()
+
+    def __len__(self):
+        return self._tables.n_patterns
+
+    def len(self):
+        return self._tables.n_patterns
+
+    def is_empty(self):
+        return self._tables.n_patterns == 0
+
+    def tables(self) -> N.WsPatternTables:
+        return self._tables
+
+    def ir(self) -> dict:
+        """The PatternIR tables (core/src/pattern/ir.rs:6-34) as numpy arrays."""
+        t = self._tables
+
+        def arr(p, n, dt=np.uint32):
+            if n == 0:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True)
+
+        return {
+            "packed_bytes": bytes(arr(t.packed_bytes, t.packed_len, np.uint8)),
+            "offsets": arr(t.offsets, 2 * t.n_literals).reshape(-1, 2),
+            "literal_pattern_ids": arr(t.literal_pattern_ids, t.n_literals),
+            "hash_window_len": t.hash_window_len,
+            "prefix_meta": arr(t.prefix_meta, 4 * t.hash_window_len).reshape(-1, 4),
+            "bucket_ranges": arr(t.bucket_ranges, 2 * t.n_buckets).reshape(-1, 2),
+            "entries": arr(t.entries, 2 * t.n_literals).reshape(-1, 2),
+            "regex_patterns": [(int(t.regex_pattern_ids[i]), t.regex_sources[i].decode())
+                               for i in range(t.n_regex)],
+            "max_pattern_len": int(max([int(t.offsets[2 * i + 1]) for i in range(t.n_literals)], default=0)),
+        }
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                N.lib().ws_ir_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def _call_noerr(fn, *args):
+    st = fn(*args)
+    if st != 0:
+        raise ValueError(f"status {st}")
+
+
+# ---------------------------------------------------------------- config
+class AutoMatcherConfig:
+    """AutoMatcherConfig (core/src/config.rs:39-173) plus the B200 plan knobs."""
+
+    def __init__(self):
+        self.c = N.WsConfig()
+        N.lib().ws_config_default(ctypes.byref(self.c))
+        self._gpu_max_regex_input_size = 16 << 20
+        self._max_scan_depth = None
+
+    @staticmethod
+    def new():
+        return AutoMatcherConfig()
+
+    def gpu_threshold(self, n):
+        self.c.gpu_threshold = max(int(n), 1)
+        return self
+
+    def gpu_max_input_size(self, n):
+        self.c.gpu_max_input_size = max(int(n), 1)
+        return self
+
+    def gpu_max_regex_input_size(self, n):
+        # Kept for API compatibility: the DFA kernels have no input-size cap.
+        self._gpu_max_regex_input_size = int(n)
+        return self
+
+    def max_matches(self, n):
+        self.c.max_matches = int(n)
+        return self
+
+    def chunk_size(self, n):
+        self.c.chunk_size = max(int(n), 1)
+        if self.c.chunk_overlap >= self.c.chunk_size:
+            self.c.chunk_overlap = self.c.chunk_size - 1
+        return self
+
+    def chunk_overlap(self, n):
+        self.c.chunk_overlap = min(int(n), max(self.c.chunk_size - 1, 0))
+        return self
+
+    def max_scan_depth(self, depth):
+        self._max_scan_depth = depth
+        return self
+
+    # B200 knobs
+    def regex_mode(self, mode: int):
+        self.c.regex_mode = int(mode)
+        return self
+
+    def dfa_max_states(self, n: int):
+        self.c.dfa_max_states = int(n)
+        return self
+
+    def walk_chunk(self, n: int):
+        self.c.walk_chunk = int(n)
+        return self
+
+    def proposer(self, kind: int, train_bytes: int | None = None, seed: int | None = None):
+        self.c.proposer = int(kind)
+        if train_bytes is not None:
+            self.c.proposer_train_bytes = int(train_bytes)
+        if seed is not None:
+            self.c.proposer_seed = int(seed)
+        return self
+
+    def profile(self, yes: bool = True):
+        """Record CUDA events around each kernel phase (GpuMatcher.info())."""
+        self.c.flags = (self.c.flags | 1) if yes else (self.c.flags & ~1)
+        return self
+
+    def configured_gpu_threshold(self):
+        return self.c.gpu_threshold
+
+    def configured_gpu_max_input_size(self):
+        return self.c.gpu_max_input_size
+
+    def configured_gpu_max_regex_input_size(self):
+        return self._gpu_max_regex_input_size
+
+    def configured_max_matches(self):
+        return self.c.max_matches
+
+    def configured_chunk_size(self):
+        return self.c.chunk_size
+
+    def configured_chunk_overlap(self):
+        return self.c.chunk_overlap
+
+    def configured_max_scan_depth(self):
+        return self._max_scan_depth
+
+
+# --------------------------------------------------------------- matcher
+_CTX = {}
+
+
+def _context(device: int = 0):
+    if device not in _CTX:
+        h = ctypes.c_void_p()
+        _call(N.lib().ws_ctx_create, device, ctypes.byref(h))
+        _CTX[device] = h
+    return _CTX[device]
+
+
+def _matches_from(buf, n) -> list[Match]:
+    if n == 0:
+        return []
+    a = np.ctypeslib.as_array(ctypes.cast(buf, ctypes.POINTER(ctypes.c_uint32)), shape=(n * 3,)).reshape(n, 3)
+    return [Match(int(p), int(s), int(e)) for p, s, e in a.tolist()]
+
+
+class GpuMatcher:
+    """GPU matcher over the sm_100a kernels (core/src/gpu/mod.rs:77-445)."""
+
+    def __init__(self, patterns: PatternSet, config: AutoMatcherConfig | None = None, device: int = 0):
+        self.patterns = patterns
+        self.config = config or AutoMatcherConfig()
+        ctx = _context(device)
+        h = ctypes.c_void_p()
+        _call(N.lib().ws_matcher_create, ctx, ctypes.byref(patterns.tables()), ctypes.byref(self.config.c),
+              ctypes.byref(h))
+        self._h = h
+        ir = patterns.ir()
+        self._chunk_overlap = max(self.config.c.chunk_overlap, ir["max_pattern_len"])
+
+    @classmethod
+    def new(cls, patterns: PatternSet) -> "GpuMatcher":
+        return cls(patterns)
+
+    @classmethod
+    def with_config(cls, patterns: PatternSet, config: AutoMatcherConfig) -> "GpuMatcher":
+        return cls(patterns, config)
+
+    def scan_array(self, data) -> np.ndarray:
+        """Scan and return an (n, 3) uint32 array of (pattern_id, start, end)."""
+        ptr, n, keep = _buffer(data)
+        cap = max(int(self.config.c.max_matches), 1)
+        out = np.empty((cap, 3), dtype=np.uint32)
+        cnt = ctypes.c_uint64()
+        _call(N.lib().ws_scan, self._h, ptr, n, out.ctypes.data_as(ctypes.POINTER(N.WsMatch)), cap, ctypes.byref(cnt))
+        del keep
+        return out[: cnt.value].copy()
+
+    def scan(self, data) -> list[Match]:
+        a = self.scan_array(data)
+        return [Match(int(p), int(s), int(e)) for p, s, e in a.tolist()]
+
+    scan_blocking = scan
+
+    def scan_block(self, data) -> list[Match]:
+        return self.scan(data)
+
+    def max_block_size(self) -> int:
+        return int(self.config.c.chunk_size)
+
+    def chunk_overlap(self) -> int:
+        return self._chunk_overlap
+
+    def scan_device(self, d_data: int, length: int, d_out: int, cap: int, d_count: int, stream: int = 0):
+        """Device-resident scan (pointers are CUDA device addresses)."""
+        _call(N.lib().ws_scan_device, self._h, d_data, length, d_out, cap, d_count, stream)
+
+    def regex_candidates(self, data, mode: int) -> np.ndarray:
+        ptr, n, keep = _buffer(data)
+        cap = max(int(self.config.c.max_matches), 1) * 4
+        out = np.empty((cap, 3), dtype=np.uint32)
+        cnt = ctypes.c_uint64()
+        _call(N.lib().ws_regex_candidates, self._h, ptr, n, mode, out.ctypes.data_as(ctypes.POINTER(N.WsMatch)),
+              cap, ctypes.byref(cnt))
+        del keep
+        return out[: cnt.value].copy()
+
+    def info(self) -> dict:
+        i = N.WsMatcherInfo()
+        N.lib().ws_matcher_get_info(self._h, ctypes.byref(i))
+        d = {f: getattr(i, f) for f, _ in N.WsMatcherInfo._fields_}
+        d["last_kernel_ms"] = list(i.last_kernel_ms)
+        return d
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().ws_matcher_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+WarpStateer = GpuMatcher  # the name used in the reference's README
+
+
+class GpuScanner:
+    """Synchronous shareable scanner (core/src/gpu/scanner.rs:14-120)."""
+
+    def __init__(self, patterns: PatternSet, config: AutoMatcherConfig | None = None):
+        self._m = GpuMatcher(patterns, config)
+
+    @classmethod
+    def new(cls, patterns: PatternSet):
+        return cls(patterns)
+
+    def scan(self, data) -> list[Match]:
+        return self._m.scan(data)
+
+
+class AutoMatcher:
+    """Router that always sends input to the GPU (core/src/router.rs:59-305).
+
+    The reference returns NoGpuAdapter for inputs below ``gpu_threshold``; this
+    implementation scans every input on the GPU (the threshold is kept as a
+    configuration value only)."""
+
+    def __init__(self, patterns: PatternSet, config: AutoMatcherConfig | None = None):
+        self.patterns = patterns
+        self.config = config or AutoMatcherConfig()
+        self._gpu: GpuMatcher | None = None
+
+    @classmethod
+    def new(cls, patterns: PatternSet):
+        return cls(patterns)
+
+    @classmethod
+    def with_config(cls, patterns: PatternSet, config: AutoMatcherConfig):
+        return cls(patterns, config)
+
+    new_blocking = new
+
+    def gpu_threshold(self) -> int:
+        return int(self.config.c.gpu_threshold)
+
+    def gpu_max_input_size(self) -> int:
+        return int(self.config.c.gpu_max_input_size)
+
+    def _backend(self) -> GpuMatcher:
+        if self._gpu is None:
+            self._gpu = GpuMatcher(self.patterns, self.config)
+        return self._gpu
+
+    def has_gpu(self) -> bool:
+        try:
+            self._backend()
+            return True
+        except NoGpuAdapter:
+            return False
+
+    def scan(self, data) -> list[Match]:
+        return self._backend().scan(data)
+
+    scan_blocking = scan
+    scan_gpu = scan
+
+    def matcher(self) -> GpuMatcher:
+        return self._backend()
+
+
+# ----------------------------------------------------------------- batch
+@dataclass
+class ScanItem:
+    id: int
+    data: object
+
+
+@dataclass(frozen=True)
+class TaggedMatch:
+    source_id: int
+    matched: Match
+
+
+@dataclass
+class BatchConfig:
+    max_inputs: int = 4096
+    max_bytes: int = 256 * 1024 * 1024
+    sort_by_size: bool = True
+
+
+def _batch_raw(matcher: GpuMatcher, items: Sequence[ScanItem]) -> list[TaggedMatch]:
+    n = len(items)
+    if n == 0:
+        return []
+    arr = (N.WsItem * n)()
+    keep = []
+    for i, it in enumerate(items):
+        ptr, ln, k = _buffer(it.data)
+        keep.append(k)
+        arr[i].id = int(it.id)
+        arr[i].data = ptr
+        arr[i].len = ln
+    cap = max(int(matcher.config.c.max_matches), 1)
+    out = (N.WsTaggedMatch * cap)()
+    cnt = ctypes.c_uint64()
+    _call(N.lib().ws_scan_batch, matcher._h, arr, n, out, cap, ctypes.byref(cnt))
+    res = []
+    for k in range(cnt.value):
+        o = out[k]
+        res.append(TaggedMatch(int(o.source_id), Match(int(o.pattern_id), int(o.start), int(o.end))))
+    return res
+
+
+def scan_batch(matcher: GpuMatcher, inputs: Sequence, config: BatchConfig | None = None) -> list[list[Match]]:
+    """batch::scan_batch (core/src/batch.rs:296-303): per-input match lists."""
+    items = [ScanItem(i, d) for i, d in enumerate(inputs)]
+    grouped: list[list[Match]] = [[] for _ in inputs]
+    for t in _batch_raw(matcher, items):
+        grouped[t.source_id].append(t.matched)
+    return grouped
+
+
+def scan_batch_auto(matcher: AutoMatcher, inputs: Sequence, config: BatchConfig | None = None) -> list[list[Match]]:
+    return scan_batch(matcher.matcher(), inputs, config)
+
+
+def scan_batch_gpu(matcher: AutoMatcher | GpuMatcher, items: Iterable[ScanItem]) -> list[TaggedMatch]:
+    """batch::scan_batch_gpu (core/src/batch.rs:336-363): tagged, sorted by
+    (source_id, start, pattern_id, end)."""
+    m = matcher.matcher() if isinstance(matcher, AutoMatcher) else matcher
+    return _batch_raw(m, list(items))
+
+
+# ---------------------------------------------------------------- stream
+class StreamPipeline:
+    """StreamPipeline (core/src/pipeline.rs:15-153) with DFA-state carry.
+
+    ``scan(data)`` feeds the data through the device stream API in blocks of
+    the backend's ``max_block_size``; matches equal a whole-input scan."""
+
+    def __init__(self, backend: GpuMatcher, overlap_window: int = 0):
+        self.backend = backend
+        self.overlap_window = overlap_window
+
+    def scan(self, data) -> list[Match]:
+        ptr, n, keep = _buffer(data)
+        if n == 0:
+            return []
+        block = max(int(self.backend.max_block_size()), 1)
+        out: list[Match] = []
+        with Stream(self.backend) as s:
+            base = ctypes.c_void_p(ptr).value
+            for off in range(0, n, block):
+                out.extend(s.feed_ptr(base + off, min(block, n - off)))
+            out.extend(s.end())
+        del keep
+        out.sort(key=lambda m: (m.start, m.pattern_id, m.end))
+        return out
+
+
+class Stream:
+    """Incremental scan with 64-bit offsets (ws_stream_*)."""
+
+    def __init__(self, matcher: GpuMatcher):
+        self.m = matcher
+        h = ctypes.c_void_p()
+        _call(N.lib().ws_stream_begin, matcher._h, ctypes.byref(h))
+        self._h = h
+        self._cap = max(int(matcher.config.c.max_matches), 1)
+        self._out = (N.WsMatch64 * self._cap)()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _collect(self, n) -> list[Match]:
+        return [Match(int(self._out[k].pattern_id), int(self._out[k].start), int(self._out[k].end)) for k in range(n)]
+
+    def feed_ptr(self, ptr: int, n: int) -> list[Match]:
+        cnt = ctypes.c_uint64()
+        _call(N.lib().ws_stream_feed, self._h, ptr, n, self._out, self._cap, ctypes.byref(cnt))
+        return self._collect(cnt.value)
+
+    def feed(self, data) -> list[Match]:
+        ptr, n, keep = _buffer(data)
+        r = self.feed_ptr(ptr, n)
+        del keep
+        return r
+
+    def end(self) -> list[Match]:
+        cnt = ctypes.c_uint64()
+        _call(N.lib().ws_stream_end, self._h, self._out, self._cap, ctypes.byref(cnt))
+        return self._collect(cnt.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().ws_stream_destroy(self._h)
+            self._h = None

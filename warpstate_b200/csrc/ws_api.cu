@@ -1,0 +1,367 @@
+// C ABI of the B200 scan path: context, matcher, scan, batch and stream.
+//
+// Orchestration replaces GpuMatcher::scan / scan_once / scan_chunk
+// (core/src/gpu/mod.rs:223-388) and the dispatch helpers
+// (core/src/gpu/dispatch.rs:57-301): one device-resident copy of the pattern
+// tables per matcher, per-call streams and scratch from a pool, inputs copied
+// once, the whole input scanned in one launch sequence (no 128 MiB chunking and
+// no 16 MiB regex cap -- those limits came from wgpu buffer bindings and the
+// WGSL shader's quadratic worst case), overflow reported with the true count
+// and never answered by a CPU fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "ws_internal.h"
+#include "ws_dfa.h"
+
+using namespace ws;
+
+struct ws_ctx {
+  int device = 0;
+  int sm_count = 0;
+};
+
+namespace {
+
+// Per-call scratch: a stream, the device input copy, the output and counters.
+struct Scratch {
+  cudaStream_t stream = nullptr;
+  DeviceBuffer input;        // padded device copy of the input
+  DeviceBuffer out;          // ws_match[capacity]
+  DeviceBuffer counters;     // unsigned long long[8]
+  DeviceBuffer rx;           // regex scratch (ws_dfa.cu manages the layout)
+  void* pinned = nullptr;    // pinned staging for pageable host input
+  size_t pinned_bytes = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t busy = nullptr;  // recorded after the last use
+  ~Scratch() {
+    if (busy) cudaEventDestroy(busy);
+    if (stream) cudaStreamDestroy(stream);
+    if (pinned) cudaFreeHost(pinned);
+    for (auto e : ev) if (e) cudaEventDestroy(e);
+  }
+};
+
+void ensure(DeviceBuffer& b, size_t need) {
+  if (b.bytes >= need) return;
+  size_t n = 1;
+  while (n < need) n <<= 1;
+  b.alloc(n);
+}
+
+void fill_err(ws_error_info* err, const Failure& f) {
+  if (!err) return;
+  err->index = f.index;
+  err->count = f.count;
+  err->max = f.max;
+  std::snprintf(err->message, sizeof(err->message), "%s", f.message.c_str());
+}
+
+template <class F>
+ws_status guarded(ws_error_info* err, F&& fn) {
+  if (err) std::memset(err, 0, sizeof(*err));
+  try {
+    fn();
+    return WS_OK;
+  } catch (const WsError& e) {
+    fill_err(err, e.f);
+    return e.f.status;
+  } catch (const CompileError& e) {
+    if (err) std::snprintf(err->message, sizeof(err->message), "%s", e.what());
+    return WS_ERR_COMPILE;
+  } catch (const std::bad_alloc&) {
+    if (err) std::snprintf(err->message, sizeof(err->message), "host allocation failed");
+    return WS_ERR_DEVICE;
+  } catch (const std::exception& e) {
+    if (err) std::snprintf(err->message, sizeof(err->message), "%s", e.what());
+    return WS_ERR_DEVICE;
+  }
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+struct ws_matcher {
+  ws_ctx* ctx = nullptr;
+  ws_config cfg;
+  LiteralPlan lit;
+  RegexPlan rx;
+  uint32_t n_patterns = 0;
+  std::mutex pool_mu;
+  std::vector<std::unique_ptr<Scratch>> pool;
+  std::mutex info_mu;
+  ws_matcher_info info;
+  bool profile = false;          // record phase events (single caller at a time)
+  cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t rx_events[8] = {};
+  ~ws_matcher() {
+    for (auto e : pev) if (e) cudaEventDestroy(e);
+    for (auto e : rx_events) if (e) cudaEventDestroy(e);
+  }
+
+  std::unique_ptr<Scratch> take() {
+    {
+      std::lock_guard<std::mutex> g(pool_mu);
+      if (!pool.empty()) {
+        auto s = std::move(pool.back());
+        pool.pop_back();
+        return s;
+      }
+    }
+    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+    auto s = std::make_unique<Scratch>();
+    check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : s->ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+    check_cuda(cudaEventCreateWithFlags(&s->busy, cudaEventDisableTiming), "cudaEventCreate");
+    s->counters.alloc(64);
+    return s;
+  }
+  void give(std::unique_ptr<Scratch> s) {
+    std::lock_guard<std::mutex> g(pool_mu);
+    pool.push_back(std::move(s));
+  }
+};
+
+namespace {
+
+// Copies host input into the scratch's device buffer (zero padding after it).
+void stage_input(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len) {
+  ensure(s.input, len + 64);
+  if (len == 0) return;
+  if (is_pinned(data)) {
+    check_cuda(cudaMemcpyAsync(s.input.ptr, data, len, cudaMemcpyHostToDevice, s.stream), "H2D input");
+    return;
+  }
+  // pageable: double-buffered staging through pinned memory
+  const size_t piece = 8u << 20;
+  if (s.pinned_bytes < 2 * piece) {
+    if (s.pinned) cudaFreeHost(s.pinned);
+    s.pinned = nullptr;
+    check_cuda(cudaHostAlloc(&s.pinned, 2 * piece, cudaHostAllocDefault), "cudaHostAlloc");
+    s.pinned_bytes = 2 * piece;
+  }
+  uint8_t* pin = static_cast<uint8_t*>(s.pinned);
+  cudaEvent_t done[2] = {s.ev[2], s.ev[3]};
+  bool used[2] = {false, false};
+  for (uint64_t off = 0, k = 0; off < len; off += piece, ++k) {
+    int slot = (int)(k & 1);
+    if (used[slot]) check_cuda(cudaEventSynchronize(done[slot]), "staging sync");
+    size_t n = (size_t)std::min<uint64_t>(piece, len - off);
+    std::memcpy(pin + slot * piece, data + off, n);
+    check_cuda(cudaMemcpyAsync(static_cast<uint8_t*>(s.input.ptr) + off, pin + slot * piece, n,
+                               cudaMemcpyHostToDevice, s.stream), "H2D input");
+    check_cuda(cudaEventRecord(done[slot], s.stream), "event record");
+    used[slot] = true;
+  }
+  (void)m;
+}
+
+uint64_t device_capacity(const ws_matcher* m) { return std::max<uint64_t>(m->cfg.max_matches, 1); }
+
+// Enqueues the full scan of a device-resident input on `st`; nothing is read
+// back.  With profiling enabled, phase events are recorded on `st` as well.
+void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
+                  ws_match* d_out, uint64_t cap, unsigned long long* d_counter) {
+  const bool prof = m->profile;
+  check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
+  if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
+  LiteralLaunch ll{d_data, len, d_out, cap, d_counter};
+  launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
+  if (prof) check_cuda(cudaEventRecord(m->pev[1], st), "event");
+  if (m->rx.n_regex) {
+    RegexLaunch rl{d_data, len, d_out, cap, d_counter, m->cfg.regex_mode};
+    run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
+  }
+  if (prof) check_cuda(cudaEventRecord(m->pev[2], st), "event");
+  check_cuda(cudaEventRecord(s.busy, st), "event");
+}
+
+void sort_matches(ws_match* p, uint64_t n) {
+  std::sort(p, p + n, [](const ws_match& a, const ws_match& b) {
+    if (a.start != b.start) return a.start < b.start;
+    if (a.pattern_id != b.pattern_id) return a.pattern_id < b.pattern_id;
+    return a.end < b.end;
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int ws_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n;
+}
+
+ws_status ws_ctx_create(int device, ws_ctx** out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!out) raise(WS_ERR_INVALID_ARGUMENT, "null out");
+    int n = ws_device_count();
+    if (n <= 0) raise(WS_ERR_NO_DEVICE, "no GPU adapter available (no CUDA device)");
+    if (device < 0 || device >= n) raise(WS_ERR_NO_DEVICE, "device index out of range");
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop;
+    check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major < 10) raise(WS_ERR_NO_DEVICE, "device is not sm_100 class (B200 required)");
+    auto* c = new ws_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    *out = c;
+  });
+}
+
+void ws_ctx_destroy(ws_ctx* ctx) { delete ctx; }
+
+void ws_config_default(ws_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->gpu_threshold = 65536;                  // core/src/config.rs:28
+  c->gpu_max_input_size = 128ull << 20;       // core/src/config.rs:4
+  c->max_matches = 1000000;                  // core/src/config.rs:35
+  c->chunk_size = 128ull << 20;               // core/src/config.rs:14
+  c->chunk_overlap = 4096;                   // core/src/config.rs:21
+  c->regex_mode = WS_REGEX_SPECULATIVE;
+  c->dfa_max_states = 8192;
+  c->walk_chunk = 4096;
+  c->proposer = WS_PROPOSER_MLP;
+  c->proposer_train_bytes = 256ull << 20;
+  c->proposer_seed = 0x5EEDF00Dull;
+}
+
+ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_config* cfg,
+                            ws_matcher** out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!ctx || !t || !out) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (t->n_literals + t->n_regex == 0) raise(WS_ERR_EMPTY_PATTERN_SET, "pattern set is empty");
+    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+    auto m = std::make_unique<ws_matcher>();
+    m->ctx = ctx;
+    if (cfg) m->cfg = *cfg; else ws_config_default(&m->cfg);
+    m->n_patterns = t->n_patterns;
+    std::memset(&m->info, 0, sizeof(m->info));
+    plan_literals(*t, m->lit);
+    plan_regex(*t, m->cfg, ctx->sm_count, m->rx);
+    m->info.n_literals = t->n_literals;
+    m->info.n_regex = t->n_regex;
+    m->info.filter_q = 4;
+    m->info.filter_period = m->lit.period;
+    m->info.filter_bits = m->lit.table_bits;
+    regex_fill_info(m->rx, m->info);
+    m->profile = (m->cfg.flags & WS_FLAG_PROFILE) != 0;
+    if (m->profile) {
+      for (auto& e : m->pev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+      for (auto& e : m->rx_events) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+    }
+    *out = m.release();
+  });
+}
+
+void ws_matcher_destroy(ws_matcher* m) {
+  if (!m) return;
+  cudaSetDevice(m->ctx->device);
+  delete m;
+}
+
+ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len, ws_match* out, uint64_t cap,
+                  uint64_t* n_out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !n_out || (len && !data) || (cap && !out)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *n_out = 0;
+    if (len > 0xFFFFFFFFull)
+      raise(WS_ERR_INPUT_TOO_LARGE, "scan input is too large for 32-bit match offsets", 0, len, 0xFFFFFFFFull);
+    if (len == 0) return;  // no pattern matches empty input on the GPU path
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    auto s = m->take();
+    struct Return { ws_matcher* m; std::unique_ptr<Scratch>& s; ~Return() { if (s) m->give(std::move(s)); } } ret{m, s};
+    check_cuda(cudaStreamWaitEvent(s->stream, s->busy, 0), "wait");
+    stage_input(m, *s, data, len);
+    uint64_t dcap = device_capacity(m);
+    ensure(s->out, dcap * sizeof(ws_match));
+    auto* d_counter = s->counters.as<unsigned long long>();
+    enqueue_scan(m, *s, s->stream, s->input.as<uint8_t>(), len, s->out.as<ws_match>(), dcap, d_counter);
+    unsigned long long count = 0;
+    check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");
+    check_cuda(cudaStreamSynchronize(s->stream), "scan");
+    *n_out = count;
+    if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
+    if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);
+    if (count) {
+      check_cuda(cudaMemcpyAsync(out, s->out.ptr, count * sizeof(ws_match), cudaMemcpyDeviceToHost, s->stream), "D2H matches");
+      check_cuda(cudaStreamSynchronize(s->stream), "D2H sync");
+      sort_matches(out, count);
+    }
+  });
+}
+
+ws_status ws_scan_device(ws_matcher* m, const uint8_t* d_data, uint64_t len, ws_match* d_out, uint64_t cap,
+                         uint64_t* d_count, void* stream, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !d_count || (len && !d_data)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    if (((uintptr_t)d_data & 15) != 0) raise(WS_ERR_INVALID_ARGUMENT, "device input must be 16-byte aligned");
+    if (len > 0xFFFFFFFFull)
+      raise(WS_ERR_INPUT_TOO_LARGE, "scan input is too large for 32-bit match offsets", 0, len, 0xFFFFFFFFull);
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    auto s = m->take();
+    struct Return { ws_matcher* m; std::unique_ptr<Scratch>& s; ~Return() { if (s) m->give(std::move(s)); } } ret{m, s};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Reuse of this scratch is ordered after its previous user's work.
+    check_cuda(cudaStreamWaitEvent(st, s->busy, 0), "wait");
+    auto* d_counter = reinterpret_cast<unsigned long long*>(d_count);
+    if (len == 0) {
+      check_cuda(cudaMemsetAsync(d_counter, 0, 8, st), "memset");
+      return;
+    }
+    enqueue_scan(m, *s, st, d_data, len, d_out, cap, d_counter);
+  });
+}
+
+ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out) {
+  if (!m || !out) return WS_ERR_INVALID_ARGUMENT;
+  auto* mm = const_cast<ws_matcher*>(m);
+  std::lock_guard<std::mutex> g(mm->info_mu);
+  if (mm->profile && mm->pev[2] && cudaEventQuery(mm->pev[2]) != cudaErrorNotReady) {
+    cudaEventSynchronize(mm->pev[2]);
+    float a = 0, b = 0;
+    if (cudaEventElapsedTime(&a, mm->pev[0], mm->pev[1]) == cudaSuccess) mm->info.last_kernel_ms[0] = a;
+    if (cudaEventElapsedTime(&b, mm->pev[0], mm->pev[2]) == cudaSuccess) mm->info.last_kernel_ms[7] = b;
+    regex_collect_timing(mm->rx, mm->rx_events, mm->info);
+    cudaGetLastError();
+  }
+  *out = mm->info;
+  return WS_OK;
+}
+
+const char* ws_status_name(ws_status s) {
+  switch (s) {
+    case WS_OK: return "Ok";
+    case WS_ERR_EMPTY_PATTERN_SET: return "EmptyPatternSet";
+    case WS_ERR_EMPTY_PATTERN: return "EmptyPattern";
+    case WS_ERR_NO_DEVICE: return "NoGpuAdapter";
+    case WS_ERR_DEVICE: return "GpuDeviceError";
+    case WS_ERR_BUFFER_MAP: return "BufferMapFailed";
+    case WS_ERR_COMPILE: return "PatternCompilationFailed";
+    case WS_ERR_DFA_OOB: return "DfaOutOfBounds";
+    case WS_ERR_PATTERN_TOO_LARGE: return "PatternTooLarge";
+    case WS_ERR_PATTERN_SET_TOO_LARGE: return "PatternSetTooLarge";
+    case WS_ERR_INPUT_TOO_LARGE: return "InputTooLarge";
+    case WS_ERR_OVERFLOW: return "MatchBufferOverflow";
+    case WS_ERR_PATHOLOGICAL: return "PathologicalRegex";
+    case WS_ERR_TIMEOUT: return "Timeout";
+    case WS_ERR_INVALID_ARGUMENT: return "InvalidArgument";
+  }
+  return "Unknown";
+}
+
+}  // extern "C"

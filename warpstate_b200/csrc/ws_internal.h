@@ -1,0 +1,114 @@
+// Internal structures shared by the host compiler, the C ABI and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/warpstate.h"
+#include "ws_regex.h"
+
+namespace ws {
+
+constexpr uint32_t FNV_BASIS = 2166136261u;
+constexpr uint32_t FNV_PRIME = 16777619u;
+constexpr uint32_t HASH_WINDOW = 8;  // hash_window_len, core/src/pattern/compiler.rs:118
+
+// Status carrier for the C ABI.
+struct Failure {
+  ws_status status;
+  std::string message;
+  uint64_t index = 0, count = 0, max = 0;
+};
+
+struct WsError : std::exception {
+  Failure f;
+  explicit WsError(Failure x) : f(std::move(x)) {}
+  const char* what() const noexcept override { return f.message.c_str(); }
+};
+
+[[noreturn]] void raise(ws_status s, const std::string& msg, uint64_t index = 0, uint64_t count = 0,
+                        uint64_t max = 0);
+void check_cuda(cudaError_t e, const char* what);
+
+uint32_t fnv1a(const uint8_t* p, size_t len, size_t window);
+
+// ------------------------------------------------------------------ IR (host)
+struct IrData {
+  std::vector<uint8_t> packed_bytes;
+  std::vector<uint32_t> offsets;              // (start, len) pairs
+  std::vector<uint32_t> literal_pattern_ids;
+  std::vector<uint32_t> literal_hashes;
+  std::vector<uint32_t> prefix_meta;          // 4 * HASH_WINDOW
+  std::vector<uint32_t> bucket_ranges;        // 2 per bucket
+  std::vector<uint32_t> entries;              // 2 per literal
+  std::vector<std::string> regex_sources;
+  std::vector<uint32_t> regex_pattern_ids;
+  std::vector<const char*> regex_ptrs;        // views for ws_pattern_tables
+  uint32_t n_patterns = 0;
+  bool case_insensitive = false;
+};
+
+// LiteralPrefilterTable::build (core/src/literal_prefilter.rs:23-88).
+void build_prefilter_table(const std::vector<uint32_t>& offsets, const std::vector<uint32_t>& hashes,
+                           uint32_t window, std::vector<uint32_t>& meta,
+                           std::vector<uint32_t>& ranges, std::vector<uint32_t>& entries);
+
+// ------------------------------------------------------------ device memory
+// A device allocation that frees itself.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer();
+  void alloc(size_t n);
+  void upload(const void* src, size_t n);
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ------------------------------------------------------- literal device plan
+// Stage 1 of the literal scan: a sampled q-gram filter.  Every long literal
+// (length >= 4) registers its 4-byte grams at offsets k = 0..P-1 in a table of
+// 2^bits nibbles; bit (P-1-k) of entry hash(gram) records offset k.  A scan
+// position s can start a long literal only if the entry of the gram at the
+// first P-aligned position a >= s has bit (P-1-(a-s)) set.  Short literals
+// (length 1..3) register their first two bytes in a 64 Ki-bit table checked at
+// every position.  Stage 2 runs the reference's own FNV-1a probe of the
+// LiteralPrefilterTable at each surviving position and verifies exactly.
+struct LiteralPlan {
+  uint32_t n_literals = 0;
+  uint32_t period = 4;       // P: 1, 2 or 4
+  uint32_t table_bits = 18;  // 2^bits nibble entries
+  uint32_t has_long = 0, has_short = 0;
+  uint32_t max_len = 0;
+  std::vector<uint32_t> filter;       // 2^bits nibbles packed 8 per word
+  std::vector<uint32_t> short_bits;   // 65536 bits
+  std::vector<uint32_t> lit_info;     // 4 per literal: offset (in lit_bytes), len, pattern id, 0
+  std::vector<uint8_t> lit_bytes;     // literals, each 4-byte aligned
+  DeviceBuffer d_filter, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries;
+  uint32_t n_buckets = 0;
+};
+
+// Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).
+inline uint32_t gram_hash(uint32_t gram, uint32_t bits) { return (gram * 0x9E3779B1u) >> (32 - bits); }
+
+void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan);
+
+// Kernel launchers (ws_literal.cu).
+struct LiteralLaunch {
+  const uint8_t* data;
+  uint64_t len;
+  ws_match* out;
+  uint64_t cap;
+  unsigned long long* counter;  // device; incremented per match (true count)
+};
+void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& a, cudaStream_t st, int sm_count);
+size_t literal_smem_bytes(const LiteralPlan& plan);
+
+}  // namespace ws
