@@ -84,6 +84,14 @@ def test_mixed_lengths_periods():
         check([(0, l) for l in lits], data)
 
 
+def test_dense_matches_overflow_survivor_list():
+    # every position is a candidate: the survivor list (len/64 + 4096 entries)
+    # fills up and the filter kernel verifies the rest in place
+    data = np.full(1 << 20, ord("a"), dtype=np.uint8)
+    data[::997] = ord("b")
+    check([(0, b"aa"), (0, b"aaaa"), (0, b"ab")], data, max_matches=4 << 20)
+
+
 def test_empty_input_and_overflow():
     ws = _ws()
     m, got = gpu_scan([(0, b"aa")], b"")

@@ -33,6 +33,7 @@ struct Scratch {
   DeviceBuffer out;          // ws_match[capacity]
   DeviceBuffer counters;     // unsigned long long[8]
   DeviceBuffer rx;           // regex scratch (ws_dfa.cu manages the layout)
+  DeviceBuffer lit;          // literal survivor list
   void* pinned = nullptr;    // pinned staging for pageable host input
   size_t pinned_bytes = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -176,8 +177,12 @@ void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_d
   const bool prof = m->profile;
   check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
   if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
-  LiteralLaunch ll{d_data, len, d_out, cap, d_counter};
-  launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
+  if (m->lit.n_literals) {
+    uint64_t scap = literal_survivor_cap(len);
+    ensure(s.lit, literal_scratch_bytes(scap));
+    LiteralLaunch ll{d_data, len, d_out, cap, d_counter, s.lit.ptr, scap};
+    launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
+  }
   if (prof) check_cuda(cudaEventRecord(m->pev[1], st), "event");
   if (m->rx.n_regex) {
     RegexLaunch rl{d_data, len, d_out, cap, d_counter, m->cfg.regex_mode};

@@ -87,11 +87,13 @@ struct LiteralPlan {
   uint32_t table_bits = 18;  // 2^bits nibble entries
   uint32_t has_long = 0, has_short = 0;
   uint32_t max_len = 0;
+  uint32_t parts = 0;                 // bit i: some literal has prefix length i+1
   std::vector<uint32_t> filter;       // 2^bits nibbles packed 8 per word
+  std::vector<uint32_t> bloom;        // 2^18-bit Bloom bitmap of prefix hashes
   std::vector<uint32_t> short_bits;   // 65536 bits
   std::vector<uint32_t> lit_info;     // 4 per literal: offset (in lit_bytes), len, pattern id, 0
   std::vector<uint8_t> lit_bytes;     // literals, each 4-byte aligned
-  DeviceBuffer d_filter, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries;
+  DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries;
   uint32_t n_buckets = 0;
 };
 
@@ -107,7 +109,11 @@ struct LiteralLaunch {
   ws_match* out;
   uint64_t cap;
   unsigned long long* counter;  // device; incremented per match (true count)
+  void* scratch;                // literal_scratch_bytes(survivor_cap) bytes
+  uint64_t survivor_cap;
 };
+size_t literal_scratch_bytes(uint64_t survivor_cap);
+inline uint64_t literal_survivor_cap(uint64_t len) { return len / 64 + 4096; }
 void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& a, cudaStream_t st, int sm_count);
 size_t literal_smem_bytes(const LiteralPlan& plan);
 

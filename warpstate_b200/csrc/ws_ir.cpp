@@ -113,7 +113,9 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
   plan.table_bits = 18;
   const uint32_t P = plan.period, bits = plan.table_bits;
   plan.filter.assign((size_t)1 << (bits - 3), 0);
+  plan.bloom.assign((size_t)1 << (18 - 5), 0);
   plan.short_bits.assign(65536 / 32, 0);
+  plan.parts = 0;
   plan.lit_info.assign(4 * (size_t)t.n_literals, 0);
   plan.lit_bytes.clear();
   for (uint32_t li = 0; li < t.n_literals; ++li) {
@@ -124,6 +126,18 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
     plan.lit_info[4 * li + 1] = len;
     plan.lit_info[4 * li + 2] = t.literal_pattern_ids[li];
     plan.lit_bytes.insert(plan.lit_bytes.end(), lit, lit + len);
+    {
+      // Bloom bitmap of the first min(len, 8) bytes (the kernel's prefix_key)
+      uint32_t pl = std::max<uint32_t>(std::min<uint32_t>(len, HASH_WINDOW), 1);
+      uint8_t x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      std::memcpy(x, lit, pl);
+      uint32_t lo, hi;
+      std::memcpy(&lo, x, 4);
+      std::memcpy(&hi, x + 4, 4);
+      uint32_t k = (lo * 0x9E3779B1u + hi * 0x85EBCA77u + pl * 0xC2B2AE3Du) >> (32 - 18);
+      plan.bloom[k >> 5] |= 1u << (k & 31);
+      plan.parts |= 1u << (pl - 1);
+    }
     if (len >= 4) {
       for (uint32_t k = 0; k < P; ++k) {
         uint32_t gram;
@@ -147,6 +161,7 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
   while (plan.lit_bytes.size() % 16) plan.lit_bytes.push_back(0);
   plan.n_buckets = t.n_buckets;
   plan.d_filter.upload(plan.filter.data(), plan.filter.size() * 4);
+  plan.d_bloom.upload(plan.bloom.data(), plan.bloom.size() * 4);
   plan.d_short.upload(plan.short_bits.data(), plan.short_bits.size() * 4);
   plan.d_info.upload(plan.lit_info.data(), plan.lit_info.size() * 4);
   plan.d_bytes.upload(plan.lit_bytes.data(), plan.lit_bytes.size());
