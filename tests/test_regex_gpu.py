@@ -1,0 +1,147 @@
+"""Regex DFA path on the GPU against the oracle (contract R), bit-exact.
+
+Both candidate paths are checked: the plain thread-per-start kernel and the
+speculative chunked walk (proposer, fix-up, reverse walk); their K candidate
+sets (every (pattern, start, end) of an anchored match) must be identical, and
+the resolved find_iter spans must equal the oracle's.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import workloads as w
+from conftest import case_input
+
+pytestmark = pytest.mark.gpu
+
+PLAIN, SPEC = 1, 0
+
+
+def _ws():
+    import warpstate_b200 as ws
+    return ws
+
+
+def matcher(patterns, mode=SPEC, proposer=None, **cfg):
+    ws = _ws()
+    b = ws.PatternSet.builder()
+    for kind, p in patterns:
+        b = b.literal_bytes(p) if kind == 0 else b.regex(p.decode() if isinstance(p, bytes) else p)
+    c = ws.AutoMatcherConfig().regex_mode(mode)
+    if proposer is not None:
+        c.proposer(proposer)
+    for k, v in cfg.items():
+        getattr(c, k)(v)
+    return ws.GpuMatcher.with_config(b.build(), c)
+
+
+def supported(pattern: str) -> bool:
+    r = oracle.Regex(pattern)
+    return not r.nullable and not any(a in pattern for a in ("^", "$", "\\b", "\\B", "\\A", "\\z"))
+
+
+def test_golden_regex_cases(golden):
+    for case in golden["regex_find_iter"]:
+        if not supported(case["pattern"]):
+            continue
+        data = case_input(case)
+        for mode in (PLAIN, SPEC):
+            m = matcher([(1, case["pattern"].encode())], mode=mode)
+            got = m.scan_array(data)
+            assert [[s, e] for _, s, e in got.tolist()] == case["expected"], (case["src"], case["pattern"], mode)
+
+
+def test_regex_bitmap_known_answer():
+    # core/src/gpu/ensemble.rs:375-410 -- here with spans, not just a bitmap
+    data = bytearray(b"x" * (1 << 20))
+    for i in range(100):
+        if i % 3 == 0:
+            needle = f"R{i:03}Z42".encode()
+            data[i * 7919:i * 7919 + len(needle)] = needle
+    pats = [(1, f"R{i:03}Z[0-9]{{2}}".encode()) for i in range(100)]
+    for mode in (PLAIN, SPEC):
+        got = matcher(pats, mode=mode).scan_array(bytes(data))
+        assert sorted(set(got[:, 0].tolist())) == [i for i in range(100) if i % 3 == 0]
+        for p, s, e in got.tolist():
+            assert (s, e) == (p * 7919, p * 7919 + 7)
+
+
+def _regex_workload(size, n, seed):
+    wl = w.regex(size=size, n=n, seed=seed)
+    return wl.patterns, wl.data
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_regex_config_scaled_vs_oracle(mode):
+    pats, data = _regex_workload(4 << 20, 500, 3)
+    got = matcher(pats, mode=mode).scan_array(data)
+    exp = oracle.scan_patterns(pats, data)
+    assert len(exp) > 100
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
+def test_candidate_sets_plain_equals_speculative():
+    pats, data = _regex_workload(2 << 20, 200, 5)
+    m = matcher(pats)
+    a = oracle.sort_matches(m.regex_candidates(data, PLAIN))
+    b = oracle.sort_matches(m.regex_candidates(data, SPEC))
+    assert len(a) > 50
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("chunk", [256, 512, 4096])
+def test_chunk_boundaries_without_proposer(chunk):
+    # small chunks put many matches across chunk boundaries; with no proposer
+    # every boundary guess is the unanchored start, so the fix-up does the work
+    pats, data = _regex_workload(1 << 20, 60, 7)
+    m = matcher(pats, mode=SPEC, proposer=1, walk_chunk=chunk)
+    got = m.scan_array(data)
+    exp = oracle.scan_patterns(pats, data)
+    assert np.array_equal(got, exp)
+
+
+def test_long_partial_matches_across_chunks():
+    # a regex whose partial matches run for hundreds of bytes keeps the walk
+    # away from its start state across many chunk boundaries
+    rng = np.random.default_rng(1)
+    data = bytearray(rng.integers(ord("a"), ord("c"), size=1 << 18, dtype=np.uint8).tobytes())
+    for k in range(0, len(data) - 3000, 5000):
+        data[k:k + 1] = b"X"
+        data[k + 2000:k + 2001] = b"Y"
+    pats = [(1, b"X[ab]{1,2500}Y"), (1, b"(?:ab|ba)[ab]{3}X"), (1, b"b[ab]{0,3}Y")]
+    for mode in (PLAIN, SPEC):
+        m = matcher(pats, mode=mode, proposer=1, walk_chunk=256, max_matches=1 << 22)
+        got = m.scan_array(bytes(data))
+        exp = oracle.scan_patterns(pats, bytes(data))
+        assert np.array_equal(got, exp), mode
+
+
+def test_mixed_literals_and_regexes():
+    wl = w.batch(n_items=200, n_lit=300, n_rx=100, seed=9)
+    data = wl.data
+    got = matcher(wl.patterns).scan_array(data)
+    exp = oracle.scan_patterns(wl.patterns, data)
+    assert np.array_equal(got, exp)
+
+
+def test_leftmost_first_semantics_on_gpu():
+    cases = [
+        ("a|ab", b"ab ab", [[0, 1], [3, 4]]),
+        ("ab|a", b"ab ab", [[0, 2], [3, 5]]),
+        ("a+?", b"aaa", [[0, 1], [1, 2], [2, 3]]),
+        ("(?:ab|abcd)x", b"abx abcdx", [[0, 3], [4, 9]]),
+        ("a{2,3}", b"aaaaaaa", [[0, 3], [3, 6]]),
+        ("[a-c]+d", b"abcabcd xd cd", [[0, 7], [11, 13]]),
+    ]
+    for pat, data, exp in cases:
+        for mode in (PLAIN, SPEC):
+            got = matcher([(1, pat.encode())], mode=mode).scan_array(data)
+            assert [[s, e] for _, s, e in got.tolist()] == exp, (pat, mode)
+            assert [list(x) for x in oracle.Regex(pat).find_iter(data)] == exp
+
+
+def test_unsupported_regexes_fail_loudly():
+    ws = _ws()
+    for pat in ["^abc", "abc$", "\\bword", "a*", "a|"]:
+        with pytest.raises(ws.PatternCompilationFailed):
+            matcher([(1, pat.encode())])

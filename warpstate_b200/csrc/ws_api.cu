@@ -175,6 +175,7 @@ uint64_t device_capacity(const ws_matcher* m) { return std::max<uint64_t>(m->cfg
 void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
                   ws_match* d_out, uint64_t cap, unsigned long long* d_counter) {
   const bool prof = m->profile;
+  uint32_t launches = 0;
   check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
   if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
   if (m->lit.n_literals) {
@@ -182,14 +183,27 @@ void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_d
     ensure(s.lit, literal_scratch_bytes(scap));
     LiteralLaunch ll{d_data, len, d_out, cap, d_counter, s.lit.ptr, scap};
     launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
+    launches += 2;
   }
   if (prof) check_cuda(cudaEventRecord(m->pev[1], st), "event");
   if (m->rx.n_regex) {
     RegexLaunch rl{d_data, len, d_out, cap, d_counter, m->cfg.regex_mode};
-    run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
+    launches += run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
   }
   if (prof) check_cuda(cudaEventRecord(m->pev[2], st), "event");
   check_cuda(cudaEventRecord(s.busy, st), "event");
+  std::lock_guard<std::mutex> g(m->info_mu);
+  m->info.last_launches = launches;
+  m->info.last_chunks = m->rx.last_chunks;
+}
+
+// Raises MatchBufferOverflow when a regex scratch buffer overflowed.
+void check_regex_overflow(ws_matcher* m, Scratch& s) {
+  if (!m->rx.n_regex || !s.rx.ptr) return;
+  unsigned long long flag = 0;
+  check_cuda(cudaMemcpy(&flag, static_cast<uint8_t*>(s.rx.ptr) + kRegexErrorFlagOffset, 8, cudaMemcpyDeviceToHost),
+             "D2H flag");
+  if (flag) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow (raise max_matches)", 0, 0, m->cfg.max_matches);
 }
 
 void sort_matches(ws_match* p, uint64_t n) {
@@ -300,6 +314,7 @@ ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len, ws_match* ou
     check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");
     check_cuda(cudaStreamSynchronize(s->stream), "scan");
     *n_out = count;
+    check_regex_overflow(m, *s);
     if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
     if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);
     if (count) {
@@ -370,3 +385,21 @@ const char* ws_status_name(ws_status s) {
 }
 
 }  // extern "C"
+
+extern "C" ws_status ws_regex_candidates(ws_matcher* m, const uint8_t* data, uint64_t len, uint32_t mode,
+                                         ws_match* out, uint64_t cap, uint64_t* n_out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !n_out || (len && !data) || (cap && !out)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *n_out = 0;
+    if (len > 0xFFFFFFFFull)
+      raise(WS_ERR_INPUT_TOO_LARGE, "scan input is too large for 32-bit match offsets", 0, len, 0xFFFFFFFFull);
+    if (len == 0 || !m->rx.n_regex) return;
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    auto s = m->take();
+    struct Return { ws_matcher* m; std::unique_ptr<Scratch>& s; ~Return() { if (s) m->give(std::move(s)); } } ret{m, s};
+    check_cuda(cudaStreamWaitEvent(s->stream, s->busy, 0), "wait");
+    stage_input(m, *s, data, len);
+    *n_out = regex_candidates(m->rx, s->input.as<uint8_t>(), len, mode, s->stream, s->rx, m->ctx->sm_count, out, cap);
+    check_cuda(cudaEventRecord(s->busy, s->stream), "event");
+  });
+}

@@ -1,19 +1,824 @@
+// Regex DFA path for sm_100a (see ws_dfa.h for the pipeline).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <functional>
+
 #include "ws_dfa.h"
+#include "ws_proposer.h"
+
+namespace cg = cooperative_groups;
 
 namespace ws {
 
-void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, RegexPlan& plan) {
-  (void)cfg; (void)sm_count;
-  plan.n_regex = t.n_regex;
-  if (t.n_regex) raise(WS_ERR_COMPILE, "regex DFA path not built yet");
+namespace {
+
+constexpr uint32_t F_MATCH = 0x80000000u;
+constexpr uint32_t F_DEAD = 0x40000000u;
+constexpr uint32_t F_MASK = 0x3FFFFFFFu;
+constexpr uint32_t kCkpt = 256;       // bytes between recorded walk states
+constexpr int kFixRounds = 3;         // parallel fix-up rounds before the serial sweep
+
+// ------------------------------------------------------------ scratch layout
+struct RxLayout {
+  uint64_t n_chunks = 0, chunk = 0, nck = 0, n_q = 0;
+  uint64_t k_cap = 0, ev_cap = 0;
+  size_t off_ctr, off_k, off_ev, off_guess, off_used, off_end, off_spec, off_conv, off_round, off_ckpt,
+      off_count, off_offs, off_cursor, off_starts, total;
+};
+
+struct KCand { uint32_t r, s, e; };
+struct Event { uint32_t e, state, q, tag; };
+
+// counters block (unsigned long long[16]):
+//  [0] K count  [1] event count  [2] error flags  [3..3+kFixRounds] round-changed flags
+enum { C_K = 0, C_EV = 1, C_ERR = 2, C_ROUND = 3 };
+
+RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_matches) {
+  RxLayout L;
+  L.chunk = chunk;
+  L.n_chunks = (len + chunk - 1) / chunk;
+  L.nck = chunk / kCkpt;
+  L.n_q = L.n_chunks * p.n_groups;
+  L.k_cap = std::max<uint64_t>(2 * max_matches, len / 256 + 65536);
+  L.ev_cap = L.k_cap;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o = (o + bytes + 255) & ~(size_t)255; return r; };
+  L.off_ctr = take(16 * 8);
+  L.off_k = take(L.k_cap * sizeof(KCand));
+  L.off_ev = take(L.ev_cap * sizeof(Event));
+  L.off_guess = take(L.n_q * 4);
+  L.off_used = take(L.n_q * 4);
+  L.off_end = take(L.n_q * 4);
+  L.off_spec = take(L.n_q * 4);
+  L.off_conv = take(L.n_q * 4);
+  L.off_round = take(L.n_q * 4);
+  L.off_ckpt = take(L.n_q * L.nck * 4);
+  L.off_count = take((size_t)p.n_regex * 4);
+  L.off_offs = take(((size_t)p.n_regex + 1) * 4);
+  L.off_cursor = take((size_t)p.n_regex * 4);
+  L.off_starts = take(L.k_cap * 4);
+  L.total = o;
+  return L;
 }
-void regex_fill_info(const RegexPlan& plan, ws_matcher_info& info) { (void)plan; (void)info; }
-void run_regex_scan(RegexPlan& plan, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch, int sm_count,
-                    cudaEvent_t* events) {
-  (void)plan; (void)l; (void)st; (void)scratch; (void)sm_count; (void)events;
+
+struct DevTables {
+  const GroupDev* groups;
+  const uint32_t* fwd;
+  const uint32_t* rev;
+  const uint32_t* lf;
+  const uint8_t* cls;
+  const uint32_t* mptr;
+  const uint32_t* mlist;
+  const uint32_t* rmptr;
+  const uint32_t* rmlist;
+  const uint4* lfinfo;   // per regex: {lf_off, lf_start (premultiplied), group, 0}
+  const uint32_t* pid;
+  uint32_t n_groups, n_regex;
+};
+
+struct ScanPtrs {
+  const uint8_t* data;
+  uint64_t len;
+  unsigned long long* ctr;
+  KCand* k;
+  uint64_t k_cap;
+  Event* ev;
+  uint64_t ev_cap;
+  uint32_t* guess;
+  uint32_t* used;
+  uint32_t* end;
+  uint32_t* spec;
+  uint32_t* conv;
+  uint32_t* round;
+  uint32_t* ckpt;
+  uint32_t* count;
+  uint32_t* offs;
+  uint32_t* cursor;
+  uint32_t* starts;
+  uint64_t n_chunks, chunk, nck;
+  ws_match* out;
+  uint64_t out_cap;
+  unsigned long long* out_counter;
+};
+
+ScanPtrs make_ptrs(const RxLayout& L, void* base, const RegexLaunch& l) {
+  uint8_t* b = static_cast<uint8_t*>(base);
+  ScanPtrs p;
+  p.data = l.data;
+  p.len = l.len;
+  p.ctr = reinterpret_cast<unsigned long long*>(b + L.off_ctr);
+  p.k = reinterpret_cast<KCand*>(b + L.off_k);
+  p.k_cap = L.k_cap;
+  p.ev = reinterpret_cast<Event*>(b + L.off_ev);
+  p.ev_cap = L.ev_cap;
+  p.guess = reinterpret_cast<uint32_t*>(b + L.off_guess);
+  p.used = reinterpret_cast<uint32_t*>(b + L.off_used);
+  p.end = reinterpret_cast<uint32_t*>(b + L.off_end);
+  p.spec = reinterpret_cast<uint32_t*>(b + L.off_spec);
+  p.conv = reinterpret_cast<uint32_t*>(b + L.off_conv);
+  p.round = reinterpret_cast<uint32_t*>(b + L.off_round);
+  p.ckpt = reinterpret_cast<uint32_t*>(b + L.off_ckpt);
+  p.count = reinterpret_cast<uint32_t*>(b + L.off_count);
+  p.offs = reinterpret_cast<uint32_t*>(b + L.off_offs);
+  p.cursor = reinterpret_cast<uint32_t*>(b + L.off_cursor);
+  p.starts = reinterpret_cast<uint32_t*>(b + L.off_starts);
+  p.n_chunks = L.n_chunks;
+  p.chunk = L.chunk;
+  p.nck = L.nck;
+  p.out = l.out;
+  p.out_cap = l.cap;
+  p.out_counter = l.counter;
+  return p;
 }
-void regex_collect_timing(const RegexPlan& plan, cudaEvent_t* events, ws_matcher_info& info) {
-  (void)plan; (void)events; (void)info;
+
+// One slot of an append buffer, one atomic per group of converged lanes.
+__device__ __forceinline__ unsigned long long warp_append(unsigned long long* counter) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(counter, (unsigned long long)g.size());
+  base = g.shfl(base, 0);
+  return base + g.thread_rank();
+}
+
+__device__ __forceinline__ void emit_k(const ScanPtrs& p, uint32_t r, uint32_t s, uint32_t e) {
+  unsigned long long i = warp_append(&p.ctr[C_K]);
+  if (i < p.k_cap) p.k[i] = KCand{r, s, e};
+  else atomicOr(&p.ctr[C_ERR], 1ull);
+}
+
+__device__ __forceinline__ void emit_event(const ScanPtrs& p, uint32_t e, uint32_t st, uint32_t q, uint32_t tag) {
+  unsigned long long i = warp_append(&p.ctr[C_EV]);
+  if (i < p.ev_cap) p.ev[i] = Event{e, st, q, tag};
+  else atomicOr(&p.ctr[C_ERR], 2ull);
+}
+
+// ------------------------------------------------------------- plain kernel
+// One thread per start position; per group an anchored walk until the dead
+// state, every match state reached yields K candidates (the reference's
+// per-start walk, core/src/gpu/ensemble_shader.wgsl:92-124, over the merged
+// group DFA and reporting every match instead of stopping at the first).
+__global__ void __launch_bounds__(256) dfa_plain_kernel(DevTables t, ScanPtrs p) {
+  extern __shared__ uint8_t cls_s[];  // n_groups * 256
+  for (uint32_t k = threadIdx.x; k < t.n_groups * 256; k += blockDim.x) cls_s[k] = t.cls[k];
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < p.len; s += stride) {
+    for (uint32_t g = 0; g < t.n_groups; ++g) {
+      const GroupDev gd = t.groups[g];
+      const uint8_t* cm = cls_s + g * 256;
+      const uint32_t* tab = t.fwd + gd.fwd_off;
+      uint32_t st = gd.start_anchored;
+      for (uint64_t e = s; e < p.len; ++e) {
+        uint32_t w = __ldg(tab + st + cm[__ldg(p.data + e)]);
+        if (w & F_DEAD) break;
+        st = w & F_MASK;
+        if (w & F_MATCH) {
+          uint32_t state = st / gd.n_classes;
+          const uint32_t* mp = t.mptr + gd.mptr_off;
+          for (uint32_t j = __ldg(mp + state); j < __ldg(mp + state + 1); ++j)
+            emit_k(p, __ldg(t.mlist + j), (uint32_t)s, (uint32_t)(e + 1));
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------- speculative walk
+// Thread per (group, chunk): unanchored walk from the proposed start state,
+// recording the state every kCkpt bytes, the end state and every match event.
+__global__ void __launch_bounds__(128) dfa_walk_kernel(DevTables t, ScanPtrs p) {
+  __shared__ uint8_t cm[256];
+  const uint32_t g = blockIdx.y;
+  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cm[k] = t.cls[g * 256 + k];
+  __syncthreads();
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n_chunks) return;
+  const GroupDev gd = t.groups[g];
+  const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint64_t q = (uint64_t)g * p.n_chunks + i;
+  const uint64_t c0 = i * p.chunk;
+  const uint64_t c1 = min(p.len, c0 + p.chunk);
+  uint32_t st = (i == 0) ? gd.start_unanchored : p.guess[q];
+  p.used[q] = st;
+  p.conv[q] = (uint32_t)c0;
+  p.round[q] = 0;
+  uint32_t* ck = p.ckpt + q * p.nck;
+  uint64_t pos = c0;
+  // full 16-byte vectors
+  for (; pos + 16 <= c1; pos += 16) {
+    uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + pos));
+    uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      uint32_t b = (words[k >> 2] >> ((k & 3) * 8)) & 0xFFu;
+      uint32_t w = __ldg(tab + st + cm[b]);
+      st = w & F_MASK;
+      if (w & F_MATCH) emit_event(p, (uint32_t)(pos + k + 1), st, (uint32_t)q, 0);
+    }
+    if (((pos + 16 - c0) % kCkpt) == 0) ck[(pos + 16 - c0) / kCkpt - 1] = st;
+  }
+  for (; pos < c1; ++pos) {
+    uint32_t w = __ldg(tab + st + cm[__ldg(p.data + pos)]);
+    st = w & F_MASK;
+    if (w & F_MATCH) emit_event(p, (uint32_t)(pos + 1), st, (uint32_t)q, 0);
+  }
+  p.end[q] = st;
+  p.spec[q] = st;
+}
+
+// One chunk of a fix-up round: re-walk from the predecessor's end state until
+// the walk meets a recorded state of the speculative walk (after that the two
+// walks are identical), or to the end of the chunk.
+__device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uint64_t i, uint32_t tag,
+                          const uint8_t* cm, unsigned long long* changed) {
+  const uint64_t q = (uint64_t)g * p.n_chunks + i;
+  volatile uint32_t* endv = p.end;
+  const uint32_t S = endv[q - 1];
+  if (S == p.used[q]) return;
+  const GroupDev gd = t.groups[g];
+  const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint64_t c0 = i * p.chunk;
+  const uint64_t c1 = min(p.len, c0 + p.chunk);
+  const uint32_t* ck = p.ckpt + q * p.nck;
+  uint32_t st = S;
+  uint64_t pos = c0;
+  bool converged = false;
+  uint64_t conv = c1;
+  for (uint64_t k = 0; pos < c1; ++k) {
+    uint64_t stop = min(c1, c0 + (k + 1) * kCkpt);
+    for (; pos < stop; ++pos) {
+      uint32_t w = __ldg(tab + st + cm[__ldg(p.data + pos)]);
+      st = w & F_MASK;
+      if (w & F_MATCH) emit_event(p, (uint32_t)(pos + 1), st, (uint32_t)q, tag);
+    }
+    if (stop == c0 + (k + 1) * kCkpt && k < p.nck && st == ck[k]) {
+      converged = true;
+      conv = stop;
+      break;
+    }
+  }
+  p.used[q] = S;
+  p.round[q] = tag;
+  p.conv[q] = (uint32_t)conv;
+  uint32_t new_end = converged ? p.spec[q] : st;
+  if (new_end != endv[q]) {
+    endv[q] = new_end;
+    atomicOr(changed, 1ull);
+  }
+}
+
+__global__ void __launch_bounds__(128) dfa_fixup_kernel(DevTables t, ScanPtrs p, int round) {
+  if (round > 0 && p.ctr[C_ROUND + round - 1] == 0) return;  // nothing changed last round
+  __shared__ uint8_t cm[256];
+  const uint32_t g = blockIdx.y;
+  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cm[k] = t.cls[g * 256 + k];
+  __syncthreads();
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i >= p.n_chunks) return;
+  fix_chunk(t, p, g, i, (uint32_t)round + 1, cm, &p.ctr[C_ROUND + round]);
+}
+
+// Final sweep, one thread per group, in chunk order: exact whatever happened
+// in the parallel rounds (runs only if the last round still changed something).
+__global__ void dfa_fixup_serial_kernel(DevTables t, ScanPtrs p) {
+  if (p.ctr[C_ROUND + kFixRounds - 1] == 0) return;
+  __shared__ uint8_t cm[256];
+  const uint32_t g = blockIdx.x;
+  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cm[k] = t.cls[g * 256 + k];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (uint64_t i = 1; i < p.n_chunks; ++i)
+    fix_chunk(t, p, g, i, (uint32_t)kFixRounds + 1, cm, &p.ctr[C_ROUND + kFixRounds]);
+}
+
+// Valid match events -> reverse walk -> K candidates.
+__global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs p) {
+  unsigned long long n = p.ctr[C_EV];
+  if (n > p.ev_cap) n = p.ev_cap;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    Event ev = p.ev[k];
+    uint32_t conv = p.conv[ev.q];
+    bool valid = (ev.tag == 0) ? (ev.e > conv) : (ev.tag == p.round[ev.q] && ev.e <= conv);
+    if (!valid) continue;
+    const uint32_t g = (uint32_t)(ev.q / p.n_chunks);
+    const GroupDev gd = t.groups[g];
+    const uint8_t* cm = t.cls + g * 256;
+    const uint32_t* tab = t.rev + gd.rev_off;
+    const uint32_t* rmp = t.rmptr + gd.rmptr_off;
+    uint32_t st = gd.rev_start;
+    for (uint64_t pos = ev.e; pos > 0; --pos) {
+      uint32_t w = __ldg(tab + st + __ldg(cm + __ldg(p.data + pos - 1)));
+      if (w & F_DEAD) break;
+      st = w & F_MASK;
+      if (w & F_MATCH) {
+        uint32_t state = st / gd.n_classes;
+        for (uint32_t j = __ldg(rmp + state); j < __ldg(rmp + state + 1); ++j)
+          emit_k(p, __ldg(t.rmlist + j), (uint32_t)(pos - 1), ev.e);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- resolution
+__global__ void k_hist_kernel(ScanPtrs p) {
+  unsigned long long n = min(p.ctr[C_K], (unsigned long long)p.k_cap);
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(&p.count[p.k[k].r], 1u);
+}
+
+__global__ void k_scan_kernel(ScanPtrs p, uint32_t n_regex) {
+  // single block exclusive scan
+  __shared__ uint32_t part[1024];
+  const uint32_t per = (n_regex + blockDim.x - 1) / blockDim.x;
+  const uint32_t a = threadIdx.x * per, b = min(n_regex, a + per);
+  uint32_t sum = 0;
+  for (uint32_t r = a; r < b; ++r) sum += p.count[r];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < blockDim.x; ++k) { uint32_t x = part[k]; part[k] = acc; acc += x; }
+    p.offs[n_regex] = acc;
+  }
+  __syncthreads();
+  uint32_t acc = part[threadIdx.x];
+  for (uint32_t r = a; r < b; ++r) { p.offs[r] = acc; p.cursor[r] = acc; acc += p.count[r]; }
+}
+
+__global__ void k_scatter_kernel(ScanPtrs p) {
+  unsigned long long n = min(p.ctr[C_K], (unsigned long long)p.k_cap);
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+    KCand c = p.k[k];
+    uint32_t slot = atomicAdd(&p.cursor[c.r], 1u);
+    p.starts[slot] = c.s;
+  }
+}
+
+// Sorts each regex's starts ascending: bitonic sort in shared memory for
+// segments of up to 4096, an in-place block-wide odd-even transposition sort
+// in global memory beyond that.
+__global__ void __launch_bounds__(512) k_sort_kernel(ScanPtrs p, uint32_t n_regex) {
+  __shared__ uint32_t buf[4096];
+  for (uint32_t r = blockIdx.x; r < n_regex; r += gridDim.x) {
+    const uint32_t a = p.offs[r], n = p.offs[r + 1] - a;
+    if (n <= 1) continue;
+    if (n <= 4096) {
+      uint32_t m = 1;
+      while (m < n) m <<= 1;
+      for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) buf[k] = (k < n) ? p.starts[a + k] : 0xFFFFFFFFu;
+      __syncthreads();
+      for (uint32_t size = 2; size <= m; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+          for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+            uint32_t j = k ^ stride;
+            if (j > k) {
+              bool up = (k & size) == 0;
+              uint32_t x = buf[k], y = buf[j];
+              if ((x > y) == up) { buf[k] = y; buf[j] = x; }
+            }
+          }
+          __syncthreads();
+        }
+      }
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) p.starts[a + k] = buf[k];
+      __syncthreads();
+    } else {
+      uint32_t* s = p.starts + a;
+      for (uint32_t phase = 0; phase < n; ++phase) {
+        for (uint32_t k = 2 * threadIdx.x + (phase & 1); k + 1 < n; k += 2 * blockDim.x) {
+          uint32_t x = s[k], y = s[k + 1];
+          if (x > y) { s[k] = y; s[k + 1] = x; }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// find_iter chain per regex: leftmost candidate start, its leftmost-first end
+// (the last match position of the regex's priority DFA walked from it), then
+// the next candidate at or after that end.
+__global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= t.n_regex) return;
+  const uint4 info = t.lfinfo[r];
+  const uint8_t* cm = t.cls + info.z * 256;
+  const uint32_t* tab = t.lf + info.x;
+  const uint32_t a = p.offs[r], b = p.offs[r + 1];
+  const uint32_t pid = t.pid[r];
+  uint64_t last_end = 0;
+  uint32_t prev = 0xFFFFFFFFu;
+  for (uint32_t j = a; j < b; ++j) {
+    uint32_t s = p.starts[j];
+    if (s == prev) continue;
+    prev = s;
+    if (s < last_end) continue;
+    uint32_t st = info.y;
+    int64_t last = -1;
+    for (uint64_t pos = s; pos < p.len; ++pos) {
+      uint32_t w = __ldg(tab + st + __ldg(cm + __ldg(p.data + pos)));
+      if (w & F_DEAD) break;
+      st = w & F_MASK;
+      if (w & F_MATCH) last = (int64_t)pos + 1;
+    }
+    if (last < 0) continue;  // cannot happen for a true candidate
+    unsigned long long idx = atomicAdd(p.out_counter, 1ull);
+    if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, (uint32_t)last};
+    last_end = (uint64_t)last;
+  }
+}
+
+// Copies K candidates into a ws_match buffer (diagnostics).
+__global__ void k_export_kernel(DevTables t, ScanPtrs p, ws_match* out, uint64_t cap) {
+  unsigned long long n = min(p.ctr[C_K], (unsigned long long)p.k_cap);
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n && k < cap;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    KCand c = p.k[k];
+    out[k] = ws_match{t.pid[c.r], c.s, c.e};
+  }
+}
+
+// A candidate or event buffer overflow makes the scan's match count exceed the
+// output capacity, so every caller sees MatchBufferOverflow.
+__global__ void finalize_kernel(ScanPtrs p) {
+  if (p.ctr[C_ERR]) {
+    unsigned long long c = *p.out_counter;
+    if (c <= p.out_cap) atomicMax(p.out_counter, (unsigned long long)p.out_cap + 1);
+  }
+}
+
+__global__ void fill_guess_kernel(DevTables t, ScanPtrs p) {
+  const uint32_t g = blockIdx.y;
+  const uint32_t st = t.groups[g].start_unanchored;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n_chunks; i += (uint64_t)gridDim.x * blockDim.x)
+    p.guess[(uint64_t)g * p.n_chunks + i] = st;
+}
+
+DevTables dev_tables(const RegexPlan& P) {
+  DevTables t;
+  t.groups = P.d_groups.as<GroupDev>();
+  t.fwd = P.d_fwd.as<uint32_t>();
+  t.rev = P.d_rev.as<uint32_t>();
+  t.lf = P.d_lf.as<uint32_t>();
+  t.cls = P.d_cls.as<uint8_t>();
+  t.mptr = P.d_mptr.as<uint32_t>();
+  t.mlist = P.d_mlist.as<uint32_t>();
+  t.rmptr = P.d_rmptr.as<uint32_t>();
+  t.rmlist = P.d_rmlist.as<uint32_t>();
+  t.lfinfo = P.d_lfinfo.as<uint4>();
+  t.pid = P.d_pid.as<uint32_t>();
+  t.n_groups = P.n_groups;
+  t.n_regex = P.n_regex;
+  return t;
+}
+
+// Runs the candidate phase (plain or speculative) and leaves K in scratch.
+uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, uint32_t mode, cudaStream_t st,
+                          int sm_count, cudaEvent_t* ev) {
+  uint32_t launches = 0;
+  auto mark = [&](int k) { if (ev) check_cuda(cudaEventRecord(ev[k], st), "event"); };
+  if (mode == WS_REGEX_PLAIN) {
+    size_t smem = (size_t)P.n_groups * 256;
+    uint64_t want = (p.len + 255) / 256;
+    int grid = (int)std::min<uint64_t>(want, (uint64_t)sm_count * 16);
+    dfa_plain_kernel<<<std::max(grid, 1), 256, smem, st>>>(t, p);
+    check_cuda(cudaGetLastError(), "dfa_plain_kernel");
+    launches++;
+    mark(1);
+    mark(2);
+    mark(3);
+    mark(4);
+    return launches;
+  }
+  dim3 cgrid((unsigned)((p.n_chunks + 127) / 128), P.n_groups);
+  if (P.proposer) {
+    launches += proposer_predict(*P.proposer, t.cls, p.data, p.len, p.chunk, p.n_chunks, p.guess, st);
+  } else {
+    fill_guess_kernel<<<dim3(std::min<unsigned>(cgrid.x, 1024), P.n_groups), 128, 0, st>>>(t, p);
+    check_cuda(cudaGetLastError(), "fill_guess_kernel");
+    launches++;
+  }
+  mark(1);
+  dfa_walk_kernel<<<cgrid, 128, 0, st>>>(t, p);
+  check_cuda(cudaGetLastError(), "dfa_walk_kernel");
+  launches++;
+  mark(2);
+  dim3 fgrid((unsigned)((p.n_chunks + 127) / 128), P.n_groups);
+  for (int r = 0; r < kFixRounds; ++r) {
+    dfa_fixup_kernel<<<fgrid, 128, 0, st>>>(t, p, r);
+    check_cuda(cudaGetLastError(), "dfa_fixup_kernel");
+    launches++;
+  }
+  dfa_fixup_serial_kernel<<<P.n_groups, 32, 0, st>>>(t, p);
+  check_cuda(cudaGetLastError(), "dfa_fixup_serial_kernel");
+  launches++;
+  mark(3);
+  dfa_reverse_kernel<<<sm_count * 8, 256, 0, st>>>(t, p);
+  check_cuda(cudaGetLastError(), "dfa_reverse_kernel");
+  launches++;
+  mark(4);
+  return launches;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- host plan
+RegexPlan::~RegexPlan() { proposer_destroy(proposer); }
+
+namespace {
+
+struct GroupBuild {
+  std::vector<uint32_t> regexes;
+  ByteClasses cls;
+  Dfa fwd, rev;
+  std::vector<Dfa> lf;
+};
+
+bool try_group(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
+               GroupBuild& out) {
+  std::vector<const ReTree*> tp;
+  for (uint32_t r : members) tp.push_back(&trees[r]);
+  Nfa fn = build_nfa(tp, false);
+  ByteClasses bc = compute_classes({&fn});
+  Dfa fwd = build_all_dfa(fn, bc, true, max_states);
+  if (fwd.too_big) return false;
+  Nfa rn = build_nfa(tp, true);
+  Dfa rev = build_all_dfa(rn, bc, false, 1 << 22);
+  if (rev.too_big) return false;
+  // order: dead first, then breadth-first from the unanchored start (the states
+  // a scan visits most), then whatever only the anchored start reaches
+  std::vector<uint32_t> order{0};
+  std::vector<uint8_t> seen((size_t)fwd.n_states, 0);
+  seen[0] = 1;
+  auto bfs = [&](uint32_t root) {
+    if (seen[root]) return;
+    std::deque<uint32_t> dq{root};
+    seen[root] = 1;
+    while (!dq.empty()) {
+      uint32_t s = dq.front();
+      dq.pop_front();
+      order.push_back(s);
+      for (int c = 0; c < fwd.n_classes; ++c) {
+        uint32_t n = fwd.trans[(size_t)s * fwd.n_classes + c] & DFA_MASK_STATE;
+        if (!seen[n]) { seen[n] = 1; dq.push_back(n); }
+      }
+    }
+  };
+  bfs(fwd.start_unanchored);
+  bfs(fwd.start_anchored);
+  for (uint32_t s = 0; s < (uint32_t)fwd.n_states; ++s) if (!seen[s]) order.push_back(s);
+  renumber_dfa(fwd, order);
+  out.regexes = members;
+  out.cls = bc;
+  out.fwd = std::move(fwd);
+  out.rev = std::move(rev);
+  out.lf.clear();
+  for (uint32_t r : members) {
+    Nfa one = build_nfa({&trees[r]}, false);
+    Dfa lf = build_leftmost_first_dfa(one, bc, 1 << 20);
+    if (lf.too_big) throw CompileError("leftmost-first DFA too large for regex " + std::to_string(r));
+    out.lf.push_back(std::move(lf));
+  }
+  return true;
+}
+
+void build_groups(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
+                  std::vector<GroupBuild>& out) {
+  GroupBuild gb;
+  if (try_group(trees, members, max_states, gb)) {
+    out.push_back(std::move(gb));
+    return;
+  }
+  if (members.size() == 1)
+    raise(WS_ERR_COMPILE, "regex " + std::to_string(members[0]) + " needs more than " +
+                              std::to_string(max_states) + " DFA states (raise dfa_max_states)");
+  size_t h = members.size() / 2;
+  build_groups(trees, std::vector<uint32_t>(members.begin(), members.begin() + h), max_states, out);
+  build_groups(trees, std::vector<uint32_t>(members.begin() + h, members.end()), max_states, out);
+}
+
+}  // namespace
+
+void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, RegexPlan& P) {
+  (void)sm_count;
+  P.n_regex = t.n_regex;
+  if (!t.n_regex) return;
+  std::vector<ReTree> trees(t.n_regex);
+  P.max_len = 0;
+  for (uint32_t r = 0; r < t.n_regex; ++r) {
+    std::string src(t.regex_sources[r]);
+    try {
+      trees[r] = parse_regex(src);
+    } catch (const CompileError& e) {
+      raise(WS_ERR_COMPILE, "invalid regex at index " + std::to_string(t.regex_pattern_ids[r]) + ": " + e.what(),
+            t.regex_pattern_ids[r]);
+    }
+    if (tree_has_look(trees[r]))
+      raise(WS_ERR_COMPILE, "regex " + std::to_string(t.regex_pattern_ids[r]) +
+                                " uses a look-around assertion (^ $ \\b \\B \\A \\z), which the GPU DFA path does not support",
+            t.regex_pattern_ids[r]);
+    if (tree_nullable(trees[r]))
+      raise(WS_ERR_COMPILE, "regex " + std::to_string(t.regex_pattern_ids[r]) +
+                                " can match the empty string, which the GPU DFA path does not support",
+            t.regex_pattern_ids[r]);
+    int64_t ml = tree_max_len(trees[r]);
+    if (ml < 0 || P.max_len < 0) P.max_len = -1;
+    else P.max_len = std::max(P.max_len, ml);
+  }
+  const int max_states = (int)std::max<uint32_t>(cfg.dfa_max_states, 16);
+  P.walk_chunk = std::max<uint32_t>(256, cfg.walk_chunk / 256 * 256);
+  // Greedy packing by the size of each regex's own unanchored DFA, then exact
+  // verification of every group (halved while it exceeds the budget).
+  std::vector<int> est(t.n_regex);
+  for (uint32_t r = 0; r < t.n_regex; ++r) {
+    Nfa n = build_nfa({&trees[r]}, false);
+    ByteClasses bc = compute_classes({&n});
+    Dfa d = build_all_dfa(n, bc, true, max_states);
+    if (d.too_big)
+      raise(WS_ERR_COMPILE, "regex " + std::to_string(t.regex_pattern_ids[r]) + " needs more than " +
+                                std::to_string(max_states) + " DFA states (raise dfa_max_states)",
+            t.regex_pattern_ids[r]);
+    est[r] = d.n_states;
+  }
+  std::vector<std::vector<uint32_t>> packs(1);
+  int sum = 0;
+  for (uint32_t r = 0; r < t.n_regex; ++r) {
+    if (!packs.back().empty() && sum + est[r] > (max_states * 3) / 4) { packs.emplace_back(); sum = 0; }
+    packs.back().push_back(r);
+    sum += est[r];
+  }
+  std::vector<GroupBuild> gbs;
+  for (auto& pk : packs) build_groups(trees, pk, max_states, gbs);
+
+  // device layout
+  P.n_groups = (uint32_t)gbs.size();
+  P.groups.clear();
+  P.fwd.clear(); P.rev.clear(); P.lf.clear(); P.mptr.clear(); P.mlist.clear();
+  P.rmptr.clear(); P.rmlist.clear(); P.cls.clear();
+  P.lfinfo.assign(4 * (size_t)t.n_regex, 0);
+  P.pid.assign(t.regex_pattern_ids, t.regex_pattern_ids + t.n_regex);
+  P.regex_group.assign(t.n_regex, 0);
+  P.total_states = 0;
+  P.max_classes = 0;
+  auto encode = [](const Dfa& d, std::vector<uint32_t>& dst) {
+    size_t base = dst.size();
+    dst.resize(base + d.trans.size());
+    for (size_t k = 0; k < d.trans.size(); ++k) {
+      uint32_t w = d.trans[k];
+      dst[base + k] = (w & DFA_MASK_STATE) * (uint32_t)d.n_classes | (w & ~DFA_MASK_STATE);
+    }
+    return (uint32_t)base;
+  };
+  for (uint32_t g = 0; g < P.n_groups; ++g) {
+    GroupBuild& gb = gbs[g];
+    GroupDev gd{};
+    const uint32_t C = (uint32_t)gb.cls.count;
+    gd.n_states = (uint32_t)gb.fwd.n_states;
+    gd.n_classes = C;
+    gd.fwd_off = encode(gb.fwd, P.fwd);
+    gd.start_anchored = gb.fwd.start_anchored * C;
+    gd.start_unanchored = gb.fwd.start_unanchored * C;
+    gd.rev_off = encode(gb.rev, P.rev);
+    gd.rev_start = gb.rev.start_anchored * C;
+    gd.cls_off = g * 256;
+    gd.mptr_off = (uint32_t)P.mptr.size();
+    for (int s = 0; s < gb.fwd.n_states; ++s) {
+      P.mptr.push_back((uint32_t)P.mlist.size());
+      for (uint32_t j = gb.fwd.match_ptr[(size_t)s]; j < gb.fwd.match_ptr[(size_t)s + 1]; ++j)
+        P.mlist.push_back(gb.regexes[gb.fwd.match_list[j]]);
+    }
+    P.mptr.push_back((uint32_t)P.mlist.size());
+    gd.rmptr_off = (uint32_t)P.rmptr.size();
+    for (int s = 0; s < gb.rev.n_states; ++s) {
+      P.rmptr.push_back((uint32_t)P.rmlist.size());
+      for (uint32_t j = gb.rev.match_ptr[(size_t)s]; j < gb.rev.match_ptr[(size_t)s + 1]; ++j)
+        P.rmlist.push_back(gb.regexes[gb.rev.match_list[j]]);
+    }
+    P.rmptr.push_back((uint32_t)P.rmlist.size());
+    for (int b = 0; b < 256; ++b) P.cls.push_back(gb.cls.map[b]);
+    for (size_t k = 0; k < gb.regexes.size(); ++k) {
+      uint32_t r = gb.regexes[k];
+      const Dfa& lf = gb.lf[k];
+      uint32_t off = encode(lf, P.lf);
+      P.lfinfo[4 * r + 0] = off;
+      P.lfinfo[4 * r + 1] = lf.start_anchored * C;
+      P.lfinfo[4 * r + 2] = g;
+      P.regex_group[r] = g;
+    }
+    gd.hot_words = 0;
+    P.groups.push_back(gd);
+    P.total_states += gd.n_states;
+    P.max_classes = std::max(P.max_classes, C);
+  }
+  if (P.fwd.size() > F_MASK || P.lf.size() > F_MASK) raise(WS_ERR_COMPILE, "regex tables exceed 2^30 words");
+  P.d_groups.upload(P.groups.data(), P.groups.size() * sizeof(GroupDev));
+  P.d_fwd.upload(P.fwd.data(), P.fwd.size() * 4);
+  P.d_rev.upload(P.rev.data(), P.rev.size() * 4);
+  P.d_lf.upload(P.lf.data(), P.lf.size() * 4);
+  P.d_cls.upload(P.cls.data(), P.cls.size());
+  P.d_mptr.upload(P.mptr.data(), P.mptr.size() * 4);
+  P.d_mlist.upload(P.mlist.data(), std::max<size_t>(P.mlist.size(), 1) * 4);
+  P.d_rmptr.upload(P.rmptr.data(), P.rmptr.size() * 4);
+  P.d_rmlist.upload(P.rmlist.data(), std::max<size_t>(P.rmlist.size(), 1) * 4);
+  P.d_lfinfo.upload(P.lfinfo.data(), P.lfinfo.size() * 4);
+  P.d_pid.upload(P.pid.data(), P.pid.size() * 4);
+
+  if (cfg.proposer == WS_PROPOSER_MLP) P.proposer = proposer_train(P, cfg);
+}
+
+void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
+  info.n_groups = P.n_groups;
+  info.total_states = P.total_states;
+  info.max_classes = P.max_classes;
+  info.proposer_top1 = P.top1;
+  info.proposer_top4 = P.top4;
+}
+
+static uint32_t walk_chunk_of(uint64_t len) {
+  (void)len;
+  return 4096;
+}
+
+uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch, int sm_count,
+                        cudaEvent_t* ev) {
+  if (!P.n_regex || l.len == 0) return 0;
+  uint32_t chunk = P.walk_chunk ? P.walk_chunk : walk_chunk_of(l.len);
+  RxLayout L = layout(P, l.len, chunk, l.cap);
+  if (scratch.bytes < L.total) {
+    size_t n = 1;
+    while (n < L.total) n <<= 1;
+    scratch.alloc(n);
+  }
+  ScanPtrs p = make_ptrs(L, scratch.ptr, l);
+  DevTables t = dev_tables(P);
+  uint32_t launches = 0;
+  check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");
+  check_cuda(cudaMemsetAsync(p.count, 0, (size_t)P.n_regex * 4, st), "memset");
+  if (ev) check_cuda(cudaEventRecord(ev[0], st), "event");
+  launches += candidates_phase(P, t, p, l.mode, st, sm_count, ev);
+  int hg = (int)std::min<uint64_t>((uint64_t)sm_count * 8, (L.k_cap + 255) / 256);
+  k_hist_kernel<<<hg, 256, 0, st>>>(p);
+  k_scan_kernel<<<1, 1024, 0, st>>>(p, P.n_regex);
+  k_scatter_kernel<<<hg, 256, 0, st>>>(p);
+  k_sort_kernel<<<(unsigned)std::min<uint32_t>(P.n_regex, 4096), 512, 0, st>>>(p, P.n_regex);
+  k_chain_kernel<<<(P.n_regex + 127) / 128, 128, 0, st>>>(t, p);
+  check_cuda(cudaGetLastError(), "resolution kernels");
+  launches += 5;
+  if (ev) check_cuda(cudaEventRecord(ev[5], st), "event");
+  finalize_kernel<<<1, 1, 0, st>>>(p);
+  check_cuda(cudaGetLastError(), "finalize_kernel");
+  launches += 1;
+  P.last_chunks = L.n_q;
+  P.last_launches = launches;
+  return launches;
+}
+
+void regex_collect_timing(const RegexPlan& P, cudaEvent_t* ev, ws_matcher_info& info) {
+  (void)P;
+  float ms = 0;
+  // [1] proposer, [2] walk or plain, [3] fix-up, [4] reverse, [5] resolution
+  if (cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) info.last_kernel_ms[2] = ms;
+  if (cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess) info.last_kernel_ms[1] = ms;
+  if (cudaEventElapsedTime(&ms, ev[2], ev[3]) == cudaSuccess) info.last_kernel_ms[3] = ms;
+  if (cudaEventElapsedTime(&ms, ev[3], ev[4]) == cudaSuccess) info.last_kernel_ms[4] = ms;
+  if (cudaEventElapsedTime(&ms, ev[4], ev[5]) == cudaSuccess) info.last_kernel_ms[5] = ms;
+  if (cudaEventElapsedTime(&ms, ev[0], ev[5]) == cudaSuccess) info.last_kernel_ms[6] = ms;
+}
+
+uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uint32_t mode, cudaStream_t st,
+                          DeviceBuffer& scratch, int sm_count, ws_match* host_out, uint64_t cap) {
+  if (!P.n_regex || len == 0) return 0;
+  RegexLaunch l{d_data, len, nullptr, cap, nullptr, mode};
+  uint32_t chunk = P.walk_chunk ? P.walk_chunk : walk_chunk_of(len);
+  RxLayout L = layout(P, len, chunk, std::max<uint64_t>(cap, 1));
+  if (scratch.bytes < L.total) {
+    size_t n = 1;
+    while (n < L.total) n <<= 1;
+    scratch.alloc(n);
+  }
+  ScanPtrs p = make_ptrs(L, scratch.ptr, l);
+  DevTables t = dev_tables(P);
+  check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");
+  candidates_phase(P, t, p, mode, st, sm_count, nullptr);
+  unsigned long long ctr[16];
+  check_cuda(cudaMemcpyAsync(ctr, p.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st), "D2H");
+  check_cuda(cudaStreamSynchronize(st), "sync");
+  if (ctr[C_ERR]) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow", 0, ctr[C_K], L.k_cap);
+  uint64_t n = std::min<uint64_t>(ctr[C_K], L.k_cap);
+  if (n > cap) raise(WS_ERR_OVERFLOW, "too many regex candidates", 0, n, cap);
+  if (n) {
+    DeviceBuffer tmp;
+    tmp.alloc(n * sizeof(ws_match));
+    k_export_kernel<<<sm_count * 4, 256, 0, st>>>(t, p, tmp.as<ws_match>(), n);
+    check_cuda(cudaMemcpyAsync(host_out, tmp.ptr, n * sizeof(ws_match), cudaMemcpyDeviceToHost, st), "D2H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+  }
+  return n;
 }
 
 }  // namespace ws
