@@ -176,6 +176,22 @@ ws_status ws_scan_device(ws_matcher* m, const uint8_t* d_data, uint64_t len,
                          ws_match* d_out, uint64_t cap, uint64_t* d_count,
                          void* stream, ws_error_info* err);
 
+/* Allocation-free literal scan.  No counterpart in the reference.  For callers
+ * that cannot call cudaMalloc while scanning (a framework whose memory manager
+ * owns all device memory, or a latency-bound loop that cannot afford
+ * cudaMalloc's implicit synchronisation): same inputs, outputs and semantics as
+ * ws_scan_device, for matchers whose pattern set has literals only, with the
+ * scratch in a static device array inside the library (about 8 MiB, held on
+ * every GPU that loads the library until the process exits) instead of an
+ * allocation.  Accepts at most 128 MiB per call (WS_ERR_INPUT_TOO_LARGE
+ * beyond).  The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array: calls whose work overlaps on the GPU race,
+ * so serialise them (one stream, or events). */
+ws_status ws_scan_literals_noalloc(ws_matcher* m, const uint8_t* d_data, uint64_t len,
+                                   ws_match* d_out, uint64_t cap, uint64_t* d_count,
+                                   void* stream, ws_error_info* err);
+
 /* scan_batch / scan_batch_gpu (core/src/batch.rs:170-363): every item scanned
  * independently in one launch sequence, matches tagged with the item id and
  * sorted by (source_id, start, pattern_id, end); no cross-item matches. */

@@ -91,6 +91,9 @@ SIGNATURES = {
                                ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),
     "ws_scan_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                       ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(WsErrorInfo)]),
+    "ws_scan_literals_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                                ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.POINTER(WsErrorInfo)]),
     "ws_scan_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsItem), ctypes.c_uint64,
                                      ctypes.POINTER(WsTaggedMatch), ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),

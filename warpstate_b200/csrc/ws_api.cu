@@ -403,3 +403,14 @@ extern "C" ws_status ws_regex_candidates(ws_matcher* m, const uint8_t* data, uin
     check_cuda(cudaEventRecord(s->busy, s->stream), "event");
   });
 }
+
+namespace ws {
+// Used by the allocation-free scan (ws_noalloc.cu), which sees ws_matcher only
+// as an opaque type.
+const LiteralPlan* matcher_literal_plan(const ws_matcher* m, uint32_t* n_regex, int* device, int* sm_count) {
+  *n_regex = m->rx.n_regex;
+  *device = m->ctx->device;
+  *sm_count = m->ctx->sm_count;
+  return &m->lit;
+}
+}  // namespace ws
