@@ -214,6 +214,14 @@ def main():
         pcfg = ws.AutoMatcherConfig().max_matches(8 << 20).profile(True).regex_mode(ws.REGEX_PLAIN)
         plain = ws.GpuMatcher.with_config(ps, pcfg)
     m = ws.GpuMatcher.with_config(ps, cfg)
+    train_s = None
+    if args.config == "regex":
+        # the proposer learns from a separately seeded 256 MiB corpus of the same distribution
+        t0 = time.perf_counter()
+        corpus = W.regex_training_corpus(256 * W.MiB)
+        m.train_proposer(corpus)
+        train_s = time.perf_counter() - t0
+        del corpus
 
     d_in = torch.from_numpy(wl.data).to(f"cuda:{local}")
     cap = 8 << 20
@@ -345,6 +353,7 @@ def main():
         line["regex"] = {"speculative_gbs": round(value, 3), "plain_gbs": round(plain_gbs, 3),
                          "speedup_vs_plain": round(value / plain_gbs, 3), "plain_ms_per_step": round(plain_ms, 4),
                          "proposer_top1": last["proposer_top1"], "proposer_top4": last["proposer_top4"],
+                         "proposer_train_s": round(train_s, 2) if train_s else None,
                          "fixup_chunks": last["last_fixup_chunks"], "chunks": last["last_chunks"],
                          "groups": last["n_groups"], "states": last["total_states"],
                          "phase_ms": [round(x, 4) for x in last["last_kernel_ms"]]}

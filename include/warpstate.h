@@ -210,6 +210,15 @@ ws_status ws_stream_end(ws_stream* s, ws_match64* out, uint64_t cap, uint64_t* n
                         ws_error_info* err);
 void ws_stream_destroy(ws_stream* s);
 
+/* Trains the learned boundary-state proposer of the speculative regex walk on
+ * a corpus drawn from the same distribution as the inputs to be scanned (host
+ * memory, at least 64 KiB; 256 MiB is the intended size).  No counterpart in
+ * the reference (its GPU regex path has no chunked walk).  Until it is called,
+ * the walk guesses the unanchored start state at every chunk boundary; results
+ * are exact either way (mispredicted chunks are re-walked). */
+ws_status ws_matcher_train_proposer(ws_matcher* m, const uint8_t* corpus, uint64_t len, uint64_t seed,
+                                    ws_error_info* err);
+
 /* Introspection for tests and the benchmark. */
 typedef struct {
   uint32_t n_literals, n_regex, n_groups;

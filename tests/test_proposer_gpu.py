@@ -1,0 +1,51 @@
+"""Learned proposer: BF16 GEMM numerics against torch fp32, training, and scan
+parity with the proposer driving the speculative walk."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+import workloads as w
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mnk", [(64, 64, 64), (512, 576, 256), (100, 37, 300), (256, 256, 512)])
+def test_bf16_gemm_matches_torch_fp32(mnk):
+    import torch
+    from warpstate_b200 import _native as N
+    M, Nn, K = mnk
+    g = torch.Generator().manual_seed(M * 7 + Nn)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).cuda()
+    B = torch.randn(K, Nn, generator=g).to(torch.bfloat16).cuda()
+    C = torch.empty(M, Nn, dtype=torch.float32, device="cuda")
+    fn = N.lib().ws_testing_gemm_bf16
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    assert fn(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, Nn, K) == 0
+    ref = A.float() @ B.float()  # fp32 reference of the same bf16 operands
+    # fp32 accumulation in a different order: relative tolerance 1e-4 of the row scale
+    tol = 1e-4 * ref.abs().amax().item() + 1e-3
+    assert (C - ref).abs().max().item() <= tol
+
+
+def test_proposer_training_and_exact_scan():
+    import warpstate_b200 as ws
+    wl = w.regex(size=8 << 20, n=150, seed=13)
+    corpus = w.fill_markov(16 << 20, w.PRINTABLE, 13 * 1000 + 77, 13 * 1000 + 4)
+    b = ws.PatternSet.builder()
+    for _, p in wl.patterns:
+        b = b.regex(p.decode())
+    ps = b.build()
+    m = ws.GpuMatcher.with_config(ps, ws.AutoMatcherConfig().regex_mode(ws.REGEX_SPECULATIVE))
+    stats = m.train_proposer(corpus)
+    assert 0.0 <= stats["top1"] <= stats["top4"] <= 1.0
+    assert stats["top1"] > 0.5, stats
+    got = m.scan_array(wl.data)
+    exp = oracle.scan_patterns(wl.patterns, wl.data)
+    assert len(exp) > 100
+    assert np.array_equal(got, exp)
+    # the plain kernel agrees as well
+    pm = ws.GpuMatcher.with_config(ps, ws.AutoMatcherConfig().regex_mode(ws.REGEX_PLAIN))
+    assert np.array_equal(pm.scan_array(wl.data), exp)

@@ -458,6 +458,15 @@ class GpuMatcher:
         """Device-resident scan (pointers are CUDA device addresses)."""
         _call(N.lib().ws_scan_device, self._h, d_data, length, d_out, cap, d_count, stream)
 
+    def train_proposer(self, corpus, seed: int = 0x5EED) -> dict:
+        """Trains the learned boundary-state proposer of the speculative regex
+        walk on `corpus` (same distribution as the inputs to be scanned)."""
+        ptr, n, keep = _buffer(corpus)
+        _call(N.lib().ws_matcher_train_proposer, self._h, ptr, n, seed)
+        del keep
+        i = self.info()
+        return {"top1": i["proposer_top1"], "top4": i["proposer_top4"]}
+
     def regex_candidates(self, data, mode: int) -> np.ndarray:
         ptr, n, keep = _buffer(data)
         cap = max(int(self.config.c.max_matches), 1) * 4

@@ -102,6 +102,8 @@ SIGNATURES = {
     "ws_stream_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatch64), ctypes.c_uint64, c_u64p,
                                      ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_destroy": (None, [ctypes.c_void_p]),
+    "ws_matcher_train_proposer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.POINTER(WsErrorInfo)]),
     "ws_matcher_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatcherInfo)]),
     "ws_regex_candidates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
                                            ctypes.POINTER(WsMatch), ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),

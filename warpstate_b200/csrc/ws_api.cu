@@ -16,6 +16,7 @@
 
 #include "ws_internal.h"
 #include "ws_dfa.h"
+#include "ws_proposer.h"
 
 using namespace ws;
 
@@ -414,3 +415,24 @@ const LiteralPlan* matcher_literal_plan(const ws_matcher* m, uint32_t* n_regex, 
   return &m->lit;
 }
 }  // namespace ws
+
+extern "C" ws_status ws_matcher_train_proposer(ws_matcher* m, const uint8_t* corpus, uint64_t len, uint64_t seed,
+                                               ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || (len && !corpus)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    if (!m->rx.n_regex) return;
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    DeviceBuffer d;
+    d.alloc(len + 64);
+    check_cuda(cudaMemcpy(d.ptr, corpus, len, cudaMemcpyHostToDevice), "H2D corpus");
+    // first place the hottest DFA rows of this workload in shared memory, then
+    // learn the boundary states in the resulting numbering
+    regex_rerank_from_corpus(m->rx, d.as<uint8_t>(), len);
+    ProposerStats st;
+    proposer_train(m->rx, d.as<uint8_t>(), len, seed, m->ctx->sm_count, &st);
+    m->rx.start_rate = st.start_rate;
+    std::lock_guard<std::mutex> g(m->info_mu);
+    m->info.proposer_top1 = st.top1;
+    m->info.proposer_top4 = st.top4;
+  });
+}

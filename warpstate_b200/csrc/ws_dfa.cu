@@ -5,7 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <deque>
-#include <functional>
+#include <numeric>
 
 #include "ws_dfa.h"
 #include "ws_proposer.h"
@@ -21,13 +21,14 @@ constexpr uint32_t F_DEAD = 0x40000000u;
 constexpr uint32_t F_MASK = 0x3FFFFFFFu;
 constexpr uint32_t kCkpt = 256;       // bytes between recorded walk states
 constexpr int kFixRounds = 3;         // parallel fix-up rounds before the serial sweep
+constexpr int kWalkThreads = 1024;    // threads (= chunks) per walk block
 
 // ------------------------------------------------------------ scratch layout
 struct RxLayout {
   uint64_t n_chunks = 0, chunk = 0, nck = 0, n_q = 0;
   uint64_t k_cap = 0, ev_cap = 0;
   size_t off_ctr, off_k, off_ev, off_guess, off_used, off_end, off_spec, off_conv, off_round, off_ckpt,
-      off_count, off_offs, off_cursor, off_starts, total;
+      off_count, off_offs, off_cursor, off_starts, off_lfend, total;
 };
 
 struct KCand { uint32_t r, s, e; };
@@ -61,6 +62,7 @@ RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_m
   L.off_offs = take(((size_t)p.n_regex + 1) * 4);
   L.off_cursor = take((size_t)p.n_regex * 4);
   L.off_starts = take(L.k_cap * 4);
+  L.off_lfend = take(L.k_cap * 4);
   L.total = o;
   return L;
 }
@@ -68,6 +70,7 @@ RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_m
 struct DevTables {
   const GroupDev* groups;
   const uint32_t* fwd;
+  const uint32_t* hot;
   const uint32_t* rev;
   const uint32_t* lf;
   const uint8_t* cls;
@@ -75,7 +78,7 @@ struct DevTables {
   const uint32_t* mlist;
   const uint32_t* rmptr;
   const uint32_t* rmlist;
-  const uint4* lfinfo;   // per regex: {lf_off, lf_start (premultiplied), group, 0}
+  const uint4* lfinfo;   // per regex: {lf_off, lf_start row, group, classes}
   const uint32_t* pid;
   uint32_t n_groups, n_regex;
 };
@@ -99,6 +102,7 @@ struct ScanPtrs {
   uint32_t* offs;
   uint32_t* cursor;
   uint32_t* starts;
+  uint32_t* lfend;
   uint64_t n_chunks, chunk, nck;
   ws_match* out;
   uint64_t out_cap;
@@ -126,6 +130,7 @@ ScanPtrs make_ptrs(const RxLayout& L, void* base, const RegexLaunch& l) {
   p.offs = reinterpret_cast<uint32_t*>(b + L.off_offs);
   p.cursor = reinterpret_cast<uint32_t*>(b + L.off_cursor);
   p.starts = reinterpret_cast<uint32_t*>(b + L.off_starts);
+  p.lfend = reinterpret_cast<uint32_t*>(b + L.off_lfend);
   p.n_chunks = L.n_chunks;
   p.chunk = L.chunk;
   p.nck = L.nck;
@@ -156,33 +161,147 @@ __device__ __forceinline__ void emit_event(const ScanPtrs& p, uint32_t e, uint32
   else atomicOr(&p.ctr[C_ERR], 2ull);
 }
 
-// ------------------------------------------------------------- plain kernel
-// One thread per start position; per group an anchored walk until the dead
-// state, every match state reached yields K candidates (the reference's
-// per-start walk, core/src/gpu/ensemble_shader.wgsl:92-124, over the merged
-// group DFA and reporting every match instead of stopping at the first).
-__global__ void __launch_bounds__(256) dfa_plain_kernel(DevTables t, ScanPtrs p) {
-  extern __shared__ uint8_t cls_s[];  // n_groups * 256
-  for (uint32_t k = threadIdx.x; k < t.n_groups * 256; k += blockDim.x) cls_s[k] = t.cls[k];
+// Shared-memory image of a group's hot rows (32-bit words, 7 blocks of 8192):
+//   block 0     the first hot row, replicated per lane: word b * 32 + lane;
+//   blocks 1..6 hot rows 1..191 column-interleaved: row r, byte b at word
+//               (1 + r / 32) * 8192 + b * 32 + r % 32 (column 0 of block 1 is
+//               the trap column, see below).
+// A thread's state is the byte offset of its row's column (lane * 4 for the
+// first row), so the entry for byte b is at state + b * 128 and every row sits
+// in one bank: lanes in the first row never conflict, lanes in other rows only
+// when their rows share a column.  An entry is either the next row's byte
+// offset (0 for the first row, made lane-specific by max(entry, lane * 4)), or
+// a slow word (bit 31) for transitions into match, cold or dead states.  Cold
+// states run through the trap column, whose entries are all slow, and take
+// their transitions from the class-indexed table through L2.
+constexpr uint32_t kImgBlock = 8192;
+constexpr uint32_t kImgWords = 7 * kImgBlock;
+constexpr uint32_t kTrapByte = kImgBlock * 4;
+constexpr uint32_t S_SLOW = 0x80000000u, S_MATCH = 0x40000000u, S_COLD = 0x20000000u, S_TRAP = 0x10000000u,
+                   S_DEAD = 0x08000000u, S_ROW = 0x07FFFFFFu;
+
+__host__ __device__ constexpr size_t hot_smem_bytes(uint32_t rows) {
+  return rows ? (size_t)kImgWords * 4 + 256 : 256;
+}
+
+__host__ __device__ __forceinline__ uint32_t slot_word(uint32_t r) { return (1 + (r >> 5)) * kImgBlock + (r & 31); }
+
+__device__ __forceinline__ uint32_t slot_byte(uint32_t r, uint32_t lane4) { return r == 0 ? lane4 : slot_word(r) * 4; }
+
+// Global row of a walk state (rows of this image start at `first`).
+__device__ __forceinline__ uint32_t row_of(uint32_t st, uint32_t cold_row, uint32_t first) {
+  if (st < 128) return first;
+  if (st == kTrapByte) return cold_row;
+  uint32_t w = st >> 2;
+  return first + ((w >> 13) - 1) * 32 + (w & 31);
+}
+
+// Walk state of a global row.
+__device__ __forceinline__ uint32_t state_of(uint32_t row, uint32_t first, uint32_t rows, uint32_t lane4,
+                                             uint32_t* cold_row) {
+  uint32_t r = row - first;
+  if (r < rows) return slot_byte(r, lane4);
+  *cold_row = row;
+  return kTrapByte;
+}
+
+// Stages the image (when the group has one) and the class map.
+__device__ __forceinline__ void stage_hot(const DevTables& t, uint32_t g, uint32_t off, uint32_t rows,
+                                          uint32_t* img, uint8_t* cls_s) {
+  if (rows) {
+    const uint4* src = reinterpret_cast<const uint4*>(t.hot + off);
+    uint4* dst = reinterpret_cast<uint4*>(img);
+    for (uint32_t k = threadIdx.x; k < kImgWords / 4; k += blockDim.x) dst[k] = __ldg(src + k);
+  }
+  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cls_s[k] = t.cls[g * 256 + k];
   __syncthreads();
+}
+
+// Slow path of one transition: handles match / cold / dead and returns false
+// when the walk reached the dead state.  `m_row` receives the row of a match
+// state (0xFFFFFFFF when none).
+__device__ __forceinline__ bool slow_step(uint32_t w, uint32_t b, uint32_t& st, uint32_t& cold_row, uint32_t first,
+                                          uint32_t rows, uint32_t lane4, const uint8_t* cls_s, const uint32_t* tab,
+                                          uint32_t C, uint32_t& m_row) {
+  uint32_t n;
+  bool match, cold, dead;
+  if (w & S_TRAP) {
+    uint32_t t = __ldg(tab + cold_row * C + cls_s[b]);
+    n = t & F_MASK;
+    match = t & F_MATCH;
+    dead = t & F_DEAD;
+    cold = (n - first) >= rows;
+  } else {
+    n = w & S_ROW;
+    match = w & S_MATCH;
+    dead = w & S_DEAD;
+    cold = w & S_COLD;
+  }
+  m_row = match ? n : 0xFFFFFFFFu;
+  if (dead) return false;
+  if (cold) { st = kTrapByte; cold_row = n; }
+  else st = slot_byte(n - first, lane4);
+  return true;
+}
+
+// Out-of-line slow path of the unanchored walk (keeps the unrolled fast loop
+// small); returns the row of a match state entered, or 0xFFFFFFFF.
+struct SlowOut {
+  uint32_t st, cold_row, m_row;
+};
+
+__device__ __noinline__ SlowOut walk_slow(uint32_t w, uint32_t b, uint32_t st, uint32_t cold_row, uint32_t rows,
+                                          uint32_t lane4, const uint8_t* cls_s, const uint32_t* tab, uint32_t C) {
+  SlowOut o;
+  slow_step(w, b, st, cold_row, 0, rows, lane4, cls_s, tab, C, o.m_row);
+  o.st = st;
+  o.cold_row = cold_row;
+  return o;
+}
+
+#define WS_STEP_FAST(img, st, b) (*reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(img) + (st) + ((b) << 7)))
+
+// One transition through L2 only (fix-up walks, which are short and rare).
+__device__ __forceinline__ uint32_t step_l2(uint32_t st, uint32_t b, const uint8_t* cls_g, const uint32_t* tab,
+                                            uint32_t C) {
+  return __ldg(tab + st * C + __ldg(cls_g + b));
+}
+
+// ------------------------------------------------------------- plain kernel
+// One thread per start position; an anchored walk of the group's DFA until the
+// dead state, every match state reached yields K candidates (the reference's
+// per-start walk, core/src/gpu/ensemble_shader.wgsl:92-124, over the merged
+// group DFA, reporting every match instead of stopping at the first).
+// blockIdx.y = group; the group's hottest anchored rows sit in shared memory.
+__global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t, ScanPtrs p) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const uint32_t g = blockIdx.y;
+  const GroupDev gd = t.groups[g];
+  uint32_t* img = smem;
+  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + hot_smem_bytes(gd.ahot_rows) - 256;
+  stage_hot(t, g, gd.ahot_off, gd.ahot_rows, img, cls_s);
+  const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint32_t* mp = t.mptr + gd.mptr_off;
+  const uint32_t C = gd.n_classes, first = gd.ahot_base, rows = gd.ahot_rows;
+  const uint32_t lane4 = (threadIdx.x & 31) * 4;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < p.len; s += stride) {
-    for (uint32_t g = 0; g < t.n_groups; ++g) {
-      const GroupDev gd = t.groups[g];
-      const uint8_t* cm = cls_s + g * 256;
-      const uint32_t* tab = t.fwd + gd.fwd_off;
-      uint32_t st = gd.start_anchored;
-      for (uint64_t e = s; e < p.len; ++e) {
-        uint32_t w = __ldg(tab + st + cm[__ldg(p.data + e)]);
-        if (w & F_DEAD) break;
-        st = w & F_MASK;
-        if (w & F_MATCH) {
-          uint32_t state = st / gd.n_classes;
-          const uint32_t* mp = t.mptr + gd.mptr_off;
-          for (uint32_t j = __ldg(mp + state); j < __ldg(mp + state + 1); ++j)
-            emit_k(p, __ldg(t.mlist + j), (uint32_t)s, (uint32_t)(e + 1));
-        }
+    uint32_t cold_row = 0;
+    uint32_t st = state_of(gd.start_anchored, first, rows, lane4, &cold_row);
+    for (uint64_t e = s; e < p.len; ++e) {
+      uint32_t b = __ldg(p.data + e);
+      uint32_t w = WS_STEP_FAST(img, st, b);
+      if ((int32_t)w >= 0) {
+        st = max(w, lane4);
+        continue;
       }
+      uint32_t m_row;
+      bool alive = slow_step(w, b, st, cold_row, first, rows, lane4, cls_s, tab, C, m_row);
+      if (m_row != 0xFFFFFFFFu) {
+        for (uint32_t j = __ldg(mp + m_row); j < __ldg(mp + m_row + 1); ++j)
+          emit_k(p, __ldg(t.mlist + j), (uint32_t)s, (uint32_t)(e + 1));
+      }
+      if (!alive) break;
     }
   }
 }
@@ -190,57 +309,75 @@ __global__ void __launch_bounds__(256) dfa_plain_kernel(DevTables t, ScanPtrs p)
 // ------------------------------------------------------- speculative walk
 // Thread per (group, chunk): unanchored walk from the proposed start state,
 // recording the state every kCkpt bytes, the end state and every match event.
-__global__ void __launch_bounds__(128) dfa_walk_kernel(DevTables t, ScanPtrs p) {
-  __shared__ uint8_t cm[256];
+// blockIdx.y = group; the group's hottest rows sit in shared memory.
+__global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, ScanPtrs p) {
+  extern __shared__ __align__(16) uint32_t smem[];
   const uint32_t g = blockIdx.y;
-  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cm[k] = t.cls[g * 256 + k];
-  __syncthreads();
+  const GroupDev gd = t.groups[g];
+  uint32_t* img = smem;
+  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + hot_smem_bytes(gd.hot_rows) - 256;
+  stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s);
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.n_chunks) return;
-  const GroupDev gd = t.groups[g];
   const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint32_t C = gd.n_classes, H = gd.hot_rows;
+  const uint32_t lane4 = (threadIdx.x & 31) * 4;
   const uint64_t q = (uint64_t)g * p.n_chunks + i;
   const uint64_t c0 = i * p.chunk;
   const uint64_t c1 = min(p.len, c0 + p.chunk);
-  uint32_t st = (i == 0) ? gd.start_unanchored : p.guess[q];
-  p.used[q] = st;
+  const uint32_t start = (i == 0) ? gd.start_unanchored : p.guess[q];
+  p.used[q] = start;
   p.conv[q] = (uint32_t)c0;
   p.round[q] = 0;
   uint32_t* ck = p.ckpt + q * p.nck;
+  uint32_t cold_row = 0;
+  uint32_t st = state_of(start, 0, H, lane4, &cold_row);
   uint64_t pos = c0;
-  // full 16-byte vectors
   for (; pos + 16 <= c1; pos += 16) {
     uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + pos));
     uint32_t words[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      uint32_t b = (words[k >> 2] >> ((k & 3) * 8)) & 0xFFu;
-      uint32_t w = __ldg(tab + st + cm[b]);
-      st = w & F_MASK;
-      if (w & F_MATCH) emit_event(p, (uint32_t)(pos + k + 1), st, (uint32_t)q, 0);
+      uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
+      uint32_t w = WS_STEP_FAST(img, st, b);
+      if ((int32_t)w >= 0) {
+        st = max(w, lane4);
+      } else {
+        uint32_t m_row;
+        slow_step(w, b, st, cold_row, 0, H, lane4, cls_s, tab, C, m_row);
+        if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + k + 1), m_row, (uint32_t)q, 0);
+      }
     }
-    if (((pos + 16 - c0) % kCkpt) == 0) ck[(pos + 16 - c0) / kCkpt - 1] = st;
+    if (((pos + 16 - c0) % kCkpt) == 0) ck[(pos + 16 - c0) / kCkpt - 1] = row_of(st, cold_row, 0);
   }
   for (; pos < c1; ++pos) {
-    uint32_t w = __ldg(tab + st + cm[__ldg(p.data + pos)]);
-    st = w & F_MASK;
-    if (w & F_MATCH) emit_event(p, (uint32_t)(pos + 1), st, (uint32_t)q, 0);
+    uint32_t b = __ldg(p.data + pos);
+    uint32_t w = WS_STEP_FAST(img, st, b);
+    if ((int32_t)w >= 0) {
+      st = max(w, lane4);
+    } else {
+      uint32_t m_row;
+      slow_step(w, b, st, cold_row, 0, H, lane4, cls_s, tab, C, m_row);
+      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
+    }
   }
-  p.end[q] = st;
-  p.spec[q] = st;
+  const uint32_t end_row = row_of(st, cold_row, 0);
+  p.end[q] = end_row;
+  p.spec[q] = end_row;
 }
 
 // One chunk of a fix-up round: re-walk from the predecessor's end state until
-// the walk meets a recorded state of the speculative walk (after that the two
-// walks are identical), or to the end of the chunk.
+// the walk meets a recorded state of the speculative walk (from there on the
+// two walks are identical), or to the end of the chunk.
 __device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uint64_t i, uint32_t tag,
-                          const uint8_t* cm, unsigned long long* changed) {
+                          unsigned long long* changed) {
   const uint64_t q = (uint64_t)g * p.n_chunks + i;
   volatile uint32_t* endv = p.end;
   const uint32_t S = endv[q - 1];
   if (S == p.used[q]) return;
   const GroupDev gd = t.groups[g];
   const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint8_t* cls_g = t.cls + g * 256;
   const uint64_t c0 = i * p.chunk;
   const uint64_t c1 = min(p.len, c0 + p.chunk);
   const uint32_t* ck = p.ckpt + q * p.nck;
@@ -251,7 +388,7 @@ __device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uin
   for (uint64_t k = 0; pos < c1; ++k) {
     uint64_t stop = min(c1, c0 + (k + 1) * kCkpt);
     for (; pos < stop; ++pos) {
-      uint32_t w = __ldg(tab + st + cm[__ldg(p.data + pos)]);
+      uint32_t w = step_l2(st, __ldg(p.data + pos), cls_g, tab, gd.n_classes);
       st = w & F_MASK;
       if (w & F_MATCH) emit_event(p, (uint32_t)(pos + 1), st, (uint32_t)q, tag);
     }
@@ -271,28 +408,21 @@ __device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uin
   }
 }
 
-__global__ void __launch_bounds__(128) dfa_fixup_kernel(DevTables t, ScanPtrs p, int round) {
+__global__ void __launch_bounds__(256) dfa_fixup_kernel(DevTables t, ScanPtrs p, int round) {
   if (round > 0 && p.ctr[C_ROUND + round - 1] == 0) return;  // nothing changed last round
-  __shared__ uint8_t cm[256];
   const uint32_t g = blockIdx.y;
-  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cm[k] = t.cls[g * 256 + k];
-  __syncthreads();
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i >= p.n_chunks) return;
-  fix_chunk(t, p, g, i, (uint32_t)round + 1, cm, &p.ctr[C_ROUND + round]);
+  fix_chunk(t, p, g, i, (uint32_t)round + 1, &p.ctr[C_ROUND + round]);
 }
 
 // Final sweep, one thread per group, in chunk order: exact whatever happened
 // in the parallel rounds (runs only if the last round still changed something).
 __global__ void dfa_fixup_serial_kernel(DevTables t, ScanPtrs p) {
   if (p.ctr[C_ROUND + kFixRounds - 1] == 0) return;
-  __shared__ uint8_t cm[256];
   const uint32_t g = blockIdx.x;
-  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cm[k] = t.cls[g * 256 + k];
-  __syncthreads();
-  if (threadIdx.x != 0) return;
   for (uint64_t i = 1; i < p.n_chunks; ++i)
-    fix_chunk(t, p, g, i, (uint32_t)kFixRounds + 1, cm, &p.ctr[C_ROUND + kFixRounds]);
+    fix_chunk(t, p, g, i, (uint32_t)kFixRounds + 1, &p.ctr[C_ROUND + kFixRounds]);
 }
 
 // Valid match events -> reverse walk -> K candidates.
@@ -310,14 +440,14 @@ __global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs 
     const uint8_t* cm = t.cls + g * 256;
     const uint32_t* tab = t.rev + gd.rev_off;
     const uint32_t* rmp = t.rmptr + gd.rmptr_off;
+    const uint32_t C = gd.n_classes;
     uint32_t st = gd.rev_start;
     for (uint64_t pos = ev.e; pos > 0; --pos) {
-      uint32_t w = __ldg(tab + st + __ldg(cm + __ldg(p.data + pos - 1)));
+      uint32_t w = __ldg(tab + st * C + __ldg(cm + __ldg(p.data + pos - 1)));
       if (w & F_DEAD) break;
       st = w & F_MASK;
       if (w & F_MATCH) {
-        uint32_t state = st / gd.n_classes;
-        for (uint32_t j = __ldg(rmp + state); j < __ldg(rmp + state + 1); ++j)
+        for (uint32_t j = __ldg(rmp + st); j < __ldg(rmp + st + 1); ++j)
           emit_k(p, __ldg(t.rmlist + j), (uint32_t)(pos - 1), ev.e);
       }
     }
@@ -400,36 +530,51 @@ __global__ void __launch_bounds__(512) k_sort_kernel(ScanPtrs p, uint32_t n_rege
   }
 }
 
-// find_iter chain per regex: leftmost candidate start, its leftmost-first end
-// (the last match position of the regex's priority DFA walked from it), then
-// the next candidate at or after that end.
-__global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= t.n_regex) return;
-  const uint4 info = t.lfinfo[r];
-  const uint8_t* cm = t.cls + info.z * 256;
-  const uint32_t* tab = t.lf + info.x;
-  const uint32_t a = p.offs[r], b = p.offs[r + 1];
-  const uint32_t pid = t.pid[r];
-  uint64_t last_end = 0;
-  uint32_t prev = 0xFFFFFFFFu;
-  for (uint32_t j = a; j < b; ++j) {
-    uint32_t s = p.starts[j];
-    if (s == prev) continue;
-    prev = s;
-    if (s < last_end) continue;
+// Leftmost-first end of every distinct candidate start (in parallel): walk the
+// regex's priority DFA from the start, remembering the last match position.
+__global__ void k_lf_kernel(DevTables t, ScanPtrs p, uint32_t n_regex) {
+  const uint32_t total = p.offs[n_regex];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+    // owning regex: binary search in offs
+    uint32_t lo = 0, hi = n_regex;
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (p.offs[mid] <= j) lo = mid; else hi = mid;
+    }
+    const uint32_t r = lo;
+    const uint32_t s = p.starts[j];
+    if (j > p.offs[r] && p.starts[j - 1] == s) { p.lfend[j] = 0xFFFFFFFFu; continue; }  // duplicate
+    const uint4 info = t.lfinfo[r];
+    const uint8_t* cm = t.cls + info.z * 256;
+    const uint32_t* tab = t.lf + info.x;
     uint32_t st = info.y;
     int64_t last = -1;
     for (uint64_t pos = s; pos < p.len; ++pos) {
-      uint32_t w = __ldg(tab + st + __ldg(cm + __ldg(p.data + pos)));
+      uint32_t w = __ldg(tab + st * info.w + __ldg(cm + __ldg(p.data + pos)));
       if (w & F_DEAD) break;
       st = w & F_MASK;
       if (w & F_MATCH) last = (int64_t)pos + 1;
     }
-    if (last < 0) continue;  // cannot happen for a true candidate
+    p.lfend[j] = last < 0 ? 0xFFFFFFFFu : (uint32_t)last;
+  }
+}
+
+// find_iter chain per regex: leftmost candidate start with its leftmost-first
+// end, then the next candidate at or after that end.
+__global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= t.n_regex) return;
+  const uint32_t a = p.offs[r], b = p.offs[r + 1];
+  const uint32_t pid = t.pid[r];
+  uint64_t last_end = 0;
+  for (uint32_t j = a; j < b; ++j) {
+    uint32_t e = p.lfend[j];
+    if (e == 0xFFFFFFFFu) continue;
+    uint32_t s = p.starts[j];
+    if (s < last_end) continue;
     unsigned long long idx = atomicAdd(p.out_counter, 1ull);
-    if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, (uint32_t)last};
-    last_end = (uint64_t)last;
+    if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, e};
+    last_end = e;
   }
 }
 
@@ -463,6 +608,7 @@ DevTables dev_tables(const RegexPlan& P) {
   DevTables t;
   t.groups = P.d_groups.as<GroupDev>();
   t.fwd = P.d_fwd.as<uint32_t>();
+  t.hot = P.d_hot.as<uint32_t>();
   t.rev = P.d_rev.as<uint32_t>();
   t.lf = P.d_lf.as<uint32_t>();
   t.cls = P.d_cls.as<uint8_t>();
@@ -477,44 +623,60 @@ DevTables dev_tables(const RegexPlan& P) {
   return t;
 }
 
+
+uint32_t max_rows(const RegexPlan& P, bool anchored) {
+  uint32_t m = 0;
+  for (const auto& g : P.groups) m = std::max(m, anchored ? g.ahot_rows : g.hot_rows);
+  return m;
+}
+
+template <class K>
+void set_smem(K kernel, size_t bytes, const char* what) {
+  check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), what);
+}
+
 // Runs the candidate phase (plain or speculative) and leaves K in scratch.
 uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, uint32_t mode, cudaStream_t st,
                           int sm_count, cudaEvent_t* ev) {
   uint32_t launches = 0;
   auto mark = [&](int k) { if (ev) check_cuda(cudaEventRecord(ev[k], st), "event"); };
   if (mode == WS_REGEX_PLAIN) {
-    size_t smem = (size_t)P.n_groups * 256;
-    uint64_t want = (p.len + 255) / 256;
-    int grid = (int)std::min<uint64_t>(want, (uint64_t)sm_count * 16);
-    dfa_plain_kernel<<<std::max(grid, 1), 256, smem, st>>>(t, p);
+    size_t smem = hot_smem_bytes(max_rows(P, true));
+    set_smem(dfa_plain_kernel, smem, "smem(plain)");
+    uint64_t per_group = std::max<uint64_t>(1, (uint64_t)sm_count / P.n_groups);
+    uint64_t want = (p.len + kWalkThreads - 1) / kWalkThreads;
+    dim3 grid((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, per_group * 2)), P.n_groups);
+    mark(1);
+    dfa_plain_kernel<<<grid, kWalkThreads, smem, st>>>(t, p);
     check_cuda(cudaGetLastError(), "dfa_plain_kernel");
     launches++;
-    mark(1);
     mark(2);
     mark(3);
     mark(4);
     return launches;
   }
-  dim3 cgrid((unsigned)((p.n_chunks + 127) / 128), P.n_groups);
-  if (P.proposer) {
-    launches += proposer_predict(*P.proposer, t.cls, p.data, p.len, p.chunk, p.n_chunks, p.guess, st);
+  dim3 cgrid((unsigned)((p.n_chunks + kWalkThreads - 1) / kWalkThreads), P.n_groups);
+  if (P.proposer && P.use_proposer) {
+    launches += proposer_predict(*P.proposer, p.data, p.len, p.chunk, p.n_chunks, p.guess, st);
   } else {
-    fill_guess_kernel<<<dim3(std::min<unsigned>(cgrid.x, 1024), P.n_groups), 128, 0, st>>>(t, p);
+    fill_guess_kernel<<<dim3(std::min<unsigned>((unsigned)((p.n_chunks + 255) / 256), 1024), P.n_groups), 256, 0, st>>>(t, p);
     check_cuda(cudaGetLastError(), "fill_guess_kernel");
     launches++;
   }
   mark(1);
-  dfa_walk_kernel<<<cgrid, 128, 0, st>>>(t, p);
+  size_t smem = hot_smem_bytes(max_rows(P, false));
+  set_smem(dfa_walk_kernel, smem, "smem(walk)");
+  dfa_walk_kernel<<<cgrid, kWalkThreads, smem, st>>>(t, p);
   check_cuda(cudaGetLastError(), "dfa_walk_kernel");
   launches++;
   mark(2);
-  dim3 fgrid((unsigned)((p.n_chunks + 127) / 128), P.n_groups);
+  dim3 fgrid((unsigned)((p.n_chunks + 255) / 256), P.n_groups);
   for (int r = 0; r < kFixRounds; ++r) {
-    dfa_fixup_kernel<<<fgrid, 128, 0, st>>>(t, p, r);
+    dfa_fixup_kernel<<<fgrid, 256, 0, st>>>(t, p, r);
     check_cuda(cudaGetLastError(), "dfa_fixup_kernel");
     launches++;
   }
-  dfa_fixup_serial_kernel<<<P.n_groups, 32, 0, st>>>(t, p);
+  dfa_fixup_serial_kernel<<<P.n_groups, 1, 0, st>>>(t, p);
   check_cuda(cudaGetLastError(), "dfa_fixup_serial_kernel");
   launches++;
   mark(3);
@@ -537,7 +699,80 @@ struct GroupBuild {
   ByteClasses cls;
   Dfa fwd, rev;
   std::vector<Dfa> lf;
+  uint32_t n_hot_u = 0, n_hot_a = 0;
 };
+
+// Byte distribution assumed when ranking states: text-like input (printable
+// ASCII and common whitespace most likely, every byte possible).
+std::vector<double> class_probabilities(const ByteClasses& bc) {
+  std::vector<double> pb(256, 0.02 / 156);
+  for (int b = 0x20; b < 0x7F; ++b) pb[b] = 0.97 / 95;
+  pb['\n'] = pb['\t'] = pb['\r'] = 0.01 / 3;
+  std::vector<double> pc((size_t)bc.count, 0);
+  for (int b = 0; b < 256; ++b) pc[bc.map[b]] += pb[b];
+  return pc;
+}
+
+// Ranks states by estimated visit frequency: the unanchored part by the
+// average of the first 64 iterates of the walk's state distribution from the
+// unanchored start, the anchored part by the expected number of visits of a
+// walk from the anchored start.  New order: hot unanchored rows, hot anchored
+// rows, the remaining unanchored rows, the remaining anchored rows, dead.
+void rank_states(GroupBuild& gb) {
+  Dfa& d = gb.fwd;
+  const int n = d.n_states, C = d.n_classes;
+  auto pc = class_probabilities(gb.cls);
+  auto propagate = [&](const std::vector<double>& cur, std::vector<double>& nxt) {
+    std::fill(nxt.begin(), nxt.end(), 0.0);
+    for (int s = 0; s < n; ++s) {
+      if (cur[(size_t)s] == 0) continue;
+      for (int c = 0; c < C; ++c) {
+        uint32_t w = d.trans[(size_t)s * C + c];
+        if (w & DFA_FLAG_DEAD) continue;
+        nxt[w & DFA_MASK_STATE] += cur[(size_t)s] * pc[(size_t)c];
+      }
+    }
+  };
+  std::vector<double> pu((size_t)n, 0), pa((size_t)n, 0), cur((size_t)n, 0), nxt((size_t)n, 0);
+  cur[d.start_unanchored] = 1;
+  for (int it = 0; it < 64; ++it) {
+    for (int s = 0; s < n; ++s) pu[(size_t)s] += cur[(size_t)s];
+    propagate(cur, nxt);
+    cur.swap(nxt);
+  }
+  std::fill(cur.begin(), cur.end(), 0.0);
+  cur[d.start_anchored] = 1;
+  for (int it = 0; it < 64; ++it) {
+    for (int s = 0; s < n; ++s) pa[(size_t)s] += cur[(size_t)s];
+    propagate(cur, nxt);
+    cur.swap(nxt);
+  }
+  // which part each state belongs to: reachable from the unanchored start?
+  std::vector<uint8_t> in_u((size_t)n, 0);
+  std::deque<uint32_t> dq{d.start_unanchored};
+  in_u[d.start_unanchored] = 1;
+  while (!dq.empty()) {
+    uint32_t s = dq.front();
+    dq.pop_front();
+    for (int c = 0; c < C; ++c) {
+      uint32_t t = d.trans[(size_t)s * C + c] & DFA_MASK_STATE;
+      if (!in_u[t]) { in_u[t] = 1; dq.push_back(t); }
+    }
+  }
+  std::vector<uint32_t> us, as;
+  for (int s = 1; s < n; ++s) (in_u[(size_t)s] ? us : as).push_back((uint32_t)s);
+  std::stable_sort(us.begin(), us.end(), [&](uint32_t a, uint32_t b) { return pu[a] > pu[b]; });
+  std::stable_sort(as.begin(), as.end(), [&](uint32_t a, uint32_t b) { return pa[a] > pa[b]; });
+  gb.n_hot_u = (uint32_t)std::min<size_t>(us.size(), kHotRows);
+  gb.n_hot_a = (uint32_t)std::min<size_t>(as.size(), kHotRows);
+  std::vector<uint32_t> order;
+  order.insert(order.end(), us.begin(), us.begin() + gb.n_hot_u);
+  order.insert(order.end(), as.begin(), as.begin() + gb.n_hot_a);
+  order.insert(order.end(), us.begin() + gb.n_hot_u, us.end());
+  order.insert(order.end(), as.begin() + gb.n_hot_a, as.end());
+  order.push_back(0);  // dead
+  renumber_dfa(d, order);
+}
 
 bool try_group(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
                GroupBuild& out) {
@@ -550,33 +785,11 @@ bool try_group(const std::vector<ReTree>& trees, const std::vector<uint32_t>& me
   Nfa rn = build_nfa(tp, true);
   Dfa rev = build_all_dfa(rn, bc, false, 1 << 22);
   if (rev.too_big) return false;
-  // order: dead first, then breadth-first from the unanchored start (the states
-  // a scan visits most), then whatever only the anchored start reaches
-  std::vector<uint32_t> order{0};
-  std::vector<uint8_t> seen((size_t)fwd.n_states, 0);
-  seen[0] = 1;
-  auto bfs = [&](uint32_t root) {
-    if (seen[root]) return;
-    std::deque<uint32_t> dq{root};
-    seen[root] = 1;
-    while (!dq.empty()) {
-      uint32_t s = dq.front();
-      dq.pop_front();
-      order.push_back(s);
-      for (int c = 0; c < fwd.n_classes; ++c) {
-        uint32_t n = fwd.trans[(size_t)s * fwd.n_classes + c] & DFA_MASK_STATE;
-        if (!seen[n]) { seen[n] = 1; dq.push_back(n); }
-      }
-    }
-  };
-  bfs(fwd.start_unanchored);
-  bfs(fwd.start_anchored);
-  for (uint32_t s = 0; s < (uint32_t)fwd.n_states; ++s) if (!seen[s]) order.push_back(s);
-  renumber_dfa(fwd, order);
   out.regexes = members;
   out.cls = bc;
   out.fwd = std::move(fwd);
   out.rev = std::move(rev);
+  rank_states(out);
   out.lf.clear();
   for (uint32_t r : members) {
     Nfa one = build_nfa({&trees[r]}, false);
@@ -585,6 +798,72 @@ bool try_group(const std::vector<ReTree>& trees, const std::vector<uint32_t>& me
     out.lf.push_back(std::move(lf));
   }
   return true;
+}
+
+uint32_t append_trans(const Dfa& d, std::vector<uint32_t>& dst) {
+  size_t base = dst.size();
+  dst.insert(dst.end(), d.trans.begin(), d.trans.end());
+  return (uint32_t)base;
+}
+
+// Builds the forward tables of every group from P.fdfa (class-indexed words,
+// 16-bit byte-indexed hot rows, match lists) and uploads them.
+void layout_forward(RegexPlan& P) {
+  P.fwd.clear(); P.hot.clear(); P.mptr.clear(); P.mlist.clear();
+  P.total_states = 0;
+  P.max_classes = 0;
+  for (uint32_t g = 0; g < P.n_groups; ++g) {
+    const Dfa& d = P.fdfa[g];
+    const ByteClasses& bc = P.fcls[g];
+    GroupDev& gd = P.groups[g];
+    const uint32_t C = (uint32_t)bc.count;
+    gd.n_states = (uint32_t)d.n_states;
+    gd.n_classes = C;
+    gd.fwd_off = append_trans(d, P.fwd);
+    gd.start_anchored = d.start_anchored;
+    gd.start_unanchored = d.start_unanchored;
+    // slow words carry the next row in 27 bits; larger DFAs walk through L2 only
+    const bool fits = d.n_states < (1 << 27);
+    auto image = [&](uint32_t first, uint32_t rows) {
+      uint32_t off = (uint32_t)P.hot.size();
+      if (!rows) return off;
+      P.hot.resize(P.hot.size() + kImgWords, S_SLOW | S_TRAP);
+      uint32_t* img = P.hot.data() + off;
+      auto entry = [&](uint32_t w) -> uint32_t {
+        uint32_t n = w & DFA_MASK_STATE, nl = n - first;
+        bool match = w & DFA_FLAG_MATCH, dead = w & DFA_FLAG_DEAD, hot = nl < rows;
+        if (!match && !dead && hot) return nl == 0 ? 0u : slot_word(nl) * 4;
+        return S_SLOW | (match ? S_MATCH : 0u) | (hot ? 0u : S_COLD) | (dead ? S_DEAD : 0u) | n;
+      };
+      for (uint32_t r = 0; r < rows; ++r)
+        for (int b = 0; b < 256; ++b) {
+          uint32_t e = entry(d.trans[(size_t)(first + r) * C + bc.map[b]]);
+          if (r == 0) for (int l = 0; l < 32; ++l) img[b * 32 + l] = e;
+          else img[slot_word(r) + b * 32] = e;
+        }
+      return off;
+    };
+    gd.hot_rows = fits ? P.nhot_u[g] : 0;
+    gd.hot_off = image(0, gd.hot_rows);
+    gd.ahot_base = P.nhot_u[g];
+    gd.ahot_rows = fits ? P.nhot_a[g] : 0;
+    gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows);
+    gd.mptr_off = (uint32_t)P.mptr.size();
+    for (int s = 0; s < d.n_states; ++s) {
+      P.mptr.push_back((uint32_t)P.mlist.size());
+      for (uint32_t j = d.match_ptr[(size_t)s]; j < d.match_ptr[(size_t)s + 1]; ++j)
+        P.mlist.push_back(P.gregex[g][d.match_list[j]]);
+    }
+    P.mptr.push_back((uint32_t)P.mlist.size());
+    P.total_states += gd.n_states;
+    P.max_classes = std::max(P.max_classes, C);
+  }
+  if (P.fwd.size() > DFA_MASK_STATE) raise(WS_ERR_COMPILE, "regex tables exceed 2^30 words");
+  P.d_groups.upload(P.groups.data(), P.groups.size() * sizeof(GroupDev));
+  P.d_fwd.upload(P.fwd.data(), P.fwd.size() * 4);
+  P.d_hot.upload(P.hot.data(), std::max<size_t>(P.hot.size(), 4) * 4);
+  P.d_mptr.upload(P.mptr.data(), P.mptr.size() * 4);
+  P.d_mlist.upload(P.mlist.data(), std::max<size_t>(P.mlist.size(), 1) * 4);
 }
 
 void build_groups(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
@@ -648,51 +927,28 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
   std::vector<std::vector<uint32_t>> packs(1);
   int sum = 0;
   for (uint32_t r = 0; r < t.n_regex; ++r) {
-    if (!packs.back().empty() && sum + est[r] > (max_states * 3) / 4) { packs.emplace_back(); sum = 0; }
+    if (!packs.back().empty() && 4 * (sum + est[r]) > 3 * max_states) { packs.emplace_back(); sum = 0; }
     packs.back().push_back(r);
     sum += est[r];
   }
   std::vector<GroupBuild> gbs;
   for (auto& pk : packs) build_groups(trees, pk, max_states, gbs);
 
-  // device layout
+  // device layout: reverse and leftmost-first tables, then the forward layout
   P.n_groups = (uint32_t)gbs.size();
-  P.groups.clear();
-  P.fwd.clear(); P.rev.clear(); P.lf.clear(); P.mptr.clear(); P.mlist.clear();
-  P.rmptr.clear(); P.rmlist.clear(); P.cls.clear();
+  P.groups.assign(P.n_groups, GroupDev{});
+  P.rev.clear(); P.lf.clear(); P.rmptr.clear(); P.rmlist.clear(); P.cls.clear();
+  P.fdfa.clear(); P.fcls.clear(); P.gregex.clear(); P.nhot_u.clear(); P.nhot_a.clear();
   P.lfinfo.assign(4 * (size_t)t.n_regex, 0);
   P.pid.assign(t.regex_pattern_ids, t.regex_pattern_ids + t.n_regex);
   P.regex_group.assign(t.n_regex, 0);
-  P.total_states = 0;
-  P.max_classes = 0;
-  auto encode = [](const Dfa& d, std::vector<uint32_t>& dst) {
-    size_t base = dst.size();
-    dst.resize(base + d.trans.size());
-    for (size_t k = 0; k < d.trans.size(); ++k) {
-      uint32_t w = d.trans[k];
-      dst[base + k] = (w & DFA_MASK_STATE) * (uint32_t)d.n_classes | (w & ~DFA_MASK_STATE);
-    }
-    return (uint32_t)base;
-  };
   for (uint32_t g = 0; g < P.n_groups; ++g) {
     GroupBuild& gb = gbs[g];
-    GroupDev gd{};
+    GroupDev& gd = P.groups[g];
     const uint32_t C = (uint32_t)gb.cls.count;
-    gd.n_states = (uint32_t)gb.fwd.n_states;
-    gd.n_classes = C;
-    gd.fwd_off = encode(gb.fwd, P.fwd);
-    gd.start_anchored = gb.fwd.start_anchored * C;
-    gd.start_unanchored = gb.fwd.start_unanchored * C;
-    gd.rev_off = encode(gb.rev, P.rev);
-    gd.rev_start = gb.rev.start_anchored * C;
+    gd.rev_off = append_trans(gb.rev, P.rev);
+    gd.rev_start = gb.rev.start_anchored;
     gd.cls_off = g * 256;
-    gd.mptr_off = (uint32_t)P.mptr.size();
-    for (int s = 0; s < gb.fwd.n_states; ++s) {
-      P.mptr.push_back((uint32_t)P.mlist.size());
-      for (uint32_t j = gb.fwd.match_ptr[(size_t)s]; j < gb.fwd.match_ptr[(size_t)s + 1]; ++j)
-        P.mlist.push_back(gb.regexes[gb.fwd.match_list[j]]);
-    }
-    P.mptr.push_back((uint32_t)P.mlist.size());
     gd.rmptr_off = (uint32_t)P.rmptr.size();
     for (int s = 0; s < gb.rev.n_states; ++s) {
       P.rmptr.push_back((uint32_t)P.rmlist.size());
@@ -704,31 +960,108 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
     for (size_t k = 0; k < gb.regexes.size(); ++k) {
       uint32_t r = gb.regexes[k];
       const Dfa& lf = gb.lf[k];
-      uint32_t off = encode(lf, P.lf);
-      P.lfinfo[4 * r + 0] = off;
-      P.lfinfo[4 * r + 1] = lf.start_anchored * C;
+      P.lfinfo[4 * r + 0] = append_trans(lf, P.lf);
+      P.lfinfo[4 * r + 1] = lf.start_anchored;
       P.lfinfo[4 * r + 2] = g;
+      P.lfinfo[4 * r + 3] = C;
       P.regex_group[r] = g;
     }
-    gd.hot_words = 0;
-    P.groups.push_back(gd);
-    P.total_states += gd.n_states;
-    P.max_classes = std::max(P.max_classes, C);
+    P.fdfa.push_back(std::move(gb.fwd));
+    P.fcls.push_back(gb.cls);
+    P.gregex.push_back(gb.regexes);
+    P.nhot_u.push_back(gb.n_hot_u);
+    P.nhot_a.push_back(gb.n_hot_a);
   }
-  if (P.fwd.size() > F_MASK || P.lf.size() > F_MASK) raise(WS_ERR_COMPILE, "regex tables exceed 2^30 words");
-  P.d_groups.upload(P.groups.data(), P.groups.size() * sizeof(GroupDev));
-  P.d_fwd.upload(P.fwd.data(), P.fwd.size() * 4);
+  layout_forward(P);
   P.d_rev.upload(P.rev.data(), P.rev.size() * 4);
   P.d_lf.upload(P.lf.data(), P.lf.size() * 4);
   P.d_cls.upload(P.cls.data(), P.cls.size());
-  P.d_mptr.upload(P.mptr.data(), P.mptr.size() * 4);
-  P.d_mlist.upload(P.mlist.data(), std::max<size_t>(P.mlist.size(), 1) * 4);
   P.d_rmptr.upload(P.rmptr.data(), P.rmptr.size() * 4);
   P.d_rmlist.upload(P.rmlist.data(), std::max<size_t>(P.rmlist.size(), 1) * 4);
   P.d_lfinfo.upload(P.lfinfo.data(), P.lfinfo.size() * 4);
   P.d_pid.upload(P.pid.data(), P.pid.size() * 4);
+  P.use_proposer = cfg.proposer == WS_PROPOSER_MLP;
+}
 
-  if (cfg.proposer == WS_PROPOSER_MLP) P.proposer = proposer_train(P, cfg);
+namespace {
+
+// Visit counts of the forward states of one group over a corpus: thread per
+// 4 KiB chunk walking from the unanchored start, shared-memory histogram.
+__global__ void visit_hist_kernel(const uint32_t* tab, uint32_t C, uint32_t start, const uint8_t* cls,
+                                  const uint8_t* data, uint64_t len, uint32_t n_states, unsigned int* hist) {
+  extern __shared__ unsigned int h[];
+  for (uint32_t k = threadIdx.x; k < n_states; k += blockDim.x) h[k] = 0;
+  __syncthreads();
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t c0 = i * 4096;
+  if (c0 < len) {
+    const uint64_t c1 = min(len, c0 + 4096);
+    uint32_t st = start;
+    for (uint64_t pos = c0; pos < c1; ++pos) {
+      st = __ldg(tab + st * C + cls[data[pos]]) & F_MASK;
+      atomicAdd(&h[st], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < n_states; k += blockDim.x)
+    if (h[k]) atomicAdd(&hist[k], h[k]);
+}
+
+}  // namespace
+
+void regex_rerank_from_corpus(RegexPlan& P, const uint8_t* d_corpus, uint64_t len) {
+  if (!P.n_regex) return;
+  const uint64_t use = std::min<uint64_t>(len, 64ull << 20);
+  for (uint32_t g = 0; g < P.n_groups; ++g) {
+    Dfa& d = P.fdfa[g];
+    const uint32_t n = (uint32_t)d.n_states, C = (uint32_t)d.n_classes;
+    if (n > (1u << 14)) continue;  // L2-only group: nothing to place
+    DeviceBuffer hist;
+    hist.alloc((size_t)n * 4);
+    check_cuda(cudaMemset(hist.ptr, 0, (size_t)n * 4), "memset");
+    size_t smem = (size_t)n * 4;
+    check_cuda(cudaFuncSetAttribute(visit_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "smem(visit)");
+    uint64_t chunks = (use + 4095) / 4096;
+    visit_hist_kernel<<<(unsigned)((chunks + 255) / 256), 256, smem>>>(
+        P.d_fwd.as<uint32_t>() + P.groups[g].fwd_off, C, d.start_unanchored, P.d_cls.as<uint8_t>() + g * 256,
+        d_corpus, use, n, hist.as<unsigned int>());
+    check_cuda(cudaGetLastError(), "visit_hist_kernel");
+    std::vector<unsigned int> cnt(n);
+    check_cuda(cudaMemcpy(cnt.data(), hist.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost), "D2H hist");
+    // current layout: [hot u][hot a][rest u][rest a][dead]; keep the anchored
+    // part's order, sort the unanchored part by visits
+    const uint32_t hu = P.nhot_u[g], ha = P.nhot_a[g];
+    std::vector<uint8_t> in_u(n, 0);
+    std::deque<uint32_t> dq{d.start_unanchored};
+    in_u[d.start_unanchored] = 1;
+    while (!dq.empty()) {
+      uint32_t s = dq.front();
+      dq.pop_front();
+      for (uint32_t c = 0; c < C; ++c) {
+        uint32_t t2 = d.trans[(size_t)s * C + c] & DFA_MASK_STATE;
+        if (!in_u[t2]) { in_u[t2] = 1; dq.push_back(t2); }
+      }
+    }
+    std::vector<uint32_t> us, as;
+    uint32_t dead = n - 1;
+    for (uint32_t s = 0; s < n; ++s) {
+      if (s == dead) continue;
+      (in_u[s] ? us : as).push_back(s);
+    }
+    std::stable_sort(us.begin(), us.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
+    (void)hu;
+    std::vector<uint32_t> order;
+    uint32_t nu = (uint32_t)std::min<size_t>(us.size(), kHotRows);
+    order.insert(order.end(), us.begin(), us.begin() + nu);
+    order.insert(order.end(), as.begin(), as.begin() + std::min<size_t>(as.size(), ha));
+    order.insert(order.end(), us.begin() + nu, us.end());
+    if (as.size() > ha) order.insert(order.end(), as.begin() + ha, as.end());
+    order.push_back(dead);
+    renumber_dfa(d, order);
+    P.nhot_u[g] = nu;
+  }
+  layout_forward(P);
 }
 
 void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
@@ -739,21 +1072,22 @@ void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
   info.proposer_top4 = P.top4;
 }
 
-static uint32_t walk_chunk_of(uint64_t len) {
-  (void)len;
-  return 4096;
+namespace {
+
+void ensure_scratch(DeviceBuffer& scratch, size_t need) {
+  if (scratch.bytes >= need) return;
+  size_t n = 1;
+  while (n < need) n <<= 1;
+  scratch.alloc(n);
 }
+
+}  // namespace
 
 uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch, int sm_count,
                         cudaEvent_t* ev) {
   if (!P.n_regex || l.len == 0) return 0;
-  uint32_t chunk = P.walk_chunk ? P.walk_chunk : walk_chunk_of(l.len);
-  RxLayout L = layout(P, l.len, chunk, l.cap);
-  if (scratch.bytes < L.total) {
-    size_t n = 1;
-    while (n < L.total) n <<= 1;
-    scratch.alloc(n);
-  }
+  RxLayout L = layout(P, l.len, P.walk_chunk, l.cap);
+  ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   DevTables t = dev_tables(P);
   uint32_t launches = 0;
@@ -766,13 +1100,14 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   k_scan_kernel<<<1, 1024, 0, st>>>(p, P.n_regex);
   k_scatter_kernel<<<hg, 256, 0, st>>>(p);
   k_sort_kernel<<<(unsigned)std::min<uint32_t>(P.n_regex, 4096), 512, 0, st>>>(p, P.n_regex);
+  k_lf_kernel<<<sm_count * 8, 128, 0, st>>>(t, p, P.n_regex);
   k_chain_kernel<<<(P.n_regex + 127) / 128, 128, 0, st>>>(t, p);
   check_cuda(cudaGetLastError(), "resolution kernels");
-  launches += 5;
-  if (ev) check_cuda(cudaEventRecord(ev[5], st), "event");
+  launches += 6;
   finalize_kernel<<<1, 1, 0, st>>>(p);
   check_cuda(cudaGetLastError(), "finalize_kernel");
   launches += 1;
+  if (ev) check_cuda(cudaEventRecord(ev[5], st), "event");
   P.last_chunks = L.n_q;
   P.last_launches = launches;
   return launches;
@@ -781,7 +1116,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
 void regex_collect_timing(const RegexPlan& P, cudaEvent_t* ev, ws_matcher_info& info) {
   (void)P;
   float ms = 0;
-  // [1] proposer, [2] walk or plain, [3] fix-up, [4] reverse, [5] resolution
+  // [2] proposer, [1] walk or plain, [3] fix-up, [4] reverse, [5] resolution, [6] regex total
   if (cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) info.last_kernel_ms[2] = ms;
   if (cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess) info.last_kernel_ms[1] = ms;
   if (cudaEventElapsedTime(&ms, ev[2], ev[3]) == cudaSuccess) info.last_kernel_ms[3] = ms;
@@ -794,13 +1129,8 @@ uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uin
                           DeviceBuffer& scratch, int sm_count, ws_match* host_out, uint64_t cap) {
   if (!P.n_regex || len == 0) return 0;
   RegexLaunch l{d_data, len, nullptr, cap, nullptr, mode};
-  uint32_t chunk = P.walk_chunk ? P.walk_chunk : walk_chunk_of(len);
-  RxLayout L = layout(P, len, chunk, std::max<uint64_t>(cap, 1));
-  if (scratch.bytes < L.total) {
-    size_t n = 1;
-    while (n < L.total) n <<= 1;
-    scratch.alloc(n);
-  }
+  RxLayout L = layout(P, len, P.walk_chunk, std::max<uint64_t>(cap, 1));
+  ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   DevTables t = dev_tables(P);
   check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");

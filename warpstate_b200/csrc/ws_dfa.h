@@ -18,20 +18,29 @@
 //   2. resolution: per regex, starts sorted, and the regex crate's find_iter
 //      chain rebuilt: take the leftmost start, end it where the regex's
 //      leftmost-first DFA last matched, continue from that end.
+//
+// Transition words follow the reference's packing (core/src/dfa/mod.rs:19-22):
+// bits 0..29 the next state's row, bit 31 match, bit 30 dead.  Rows are
+// ordered by estimated visit frequency, so that the hottest rows of each group
+// can be staged in shared memory as byte-indexed rows (256 words each: the
+// hot path of a walk is one shared-memory load per input byte).
 #pragma once
 #include "ws_internal.h"
 
 namespace ws {
 
+// Hot rows staged per group in shared memory (a 224 KiB image: the first row
+// replicated per lane, 191 more rows column-interleaved; see ws_dfa.cu).
+constexpr uint32_t kHotRows = 192;
+
 struct GroupDev {
-  uint32_t fwd_off;        // offset of the forward table (u32 words)
+  uint32_t fwd_off;          // class-indexed forward table (u32 words)
   uint32_t n_states, n_classes;
-  uint32_t start_anchored, start_unanchored;  // premultiplied (state * classes)
-  uint32_t rev_off, rev_start;                // reverse table, premultiplied start
-  uint32_t mptr_off;       // forward match pointers (n_states + 1)
-  uint32_t rmptr_off;      // reverse match pointers
-  uint32_t cls_off;        // 256-byte class map
-  uint32_t hot_words;      // leading table words staged in shared memory
+  uint32_t start_anchored, start_unanchored;  // rows
+  uint32_t rev_off, rev_start;                // reverse table and its start row
+  uint32_t mptr_off, rmptr_off, cls_off;
+  uint32_t hot_off, hot_rows;                 // unanchored hot rows [0, hot_rows), byte-indexed
+  uint32_t ahot_off, ahot_base, ahot_rows;    // anchored hot rows [ahot_base, +ahot_rows)
   uint32_t pad;
 };
 
@@ -44,15 +53,22 @@ struct RegexPlan {
   std::vector<GroupDev> groups;
   std::vector<uint32_t> regex_group;     // regex index -> group
   // device tables
-  DeviceBuffer d_groups, d_fwd, d_rev, d_lf, d_cls, d_mptr, d_mlist, d_rmptr, d_rmlist, d_lfinfo, d_pid;
-  // host copies (for the proposer's training walk and diagnostics)
+  DeviceBuffer d_groups, d_fwd, d_hot, d_rev, d_lf, d_cls, d_mptr, d_mlist, d_rmptr, d_rmlist, d_lfinfo, d_pid;
+  // host copies
   std::vector<uint32_t> fwd, rev, lf, mptr, mlist, rmptr, rmlist, lfinfo, pid;
+  std::vector<uint32_t> hot;   // shared-memory images, one per (group, part)
   std::vector<uint8_t> cls;
+  // host forward DFAs per group (their numbering defines the layout above)
+  std::vector<Dfa> fdfa;
+  std::vector<ByteClasses> fcls;
+  std::vector<std::vector<uint32_t>> gregex;
+  std::vector<uint32_t> nhot_u, nhot_a;
   // proposer
-  struct Proposer* proposer = nullptr;
-  double top1 = 0, top4 = 0;
-  // last scan
+  struct Proposer* proposer = nullptr;   // trained by ws_matcher_train_proposer
+  bool use_proposer = true;               // config: MLP guesses (else the unanchored start)
+  double top1 = 0, top4 = 0, start_rate = 0;
   uint32_t walk_chunk = 4096;            // speculative chunk bytes (multiple of 256)
+  // last scan
   uint64_t last_chunks = 0, last_fixup = 0, last_k = 0;
   uint32_t last_launches = 0;
   ~RegexPlan();
@@ -68,6 +84,10 @@ struct RegexLaunch {
 };
 
 void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, RegexPlan& plan);
+// Re-ranks the forward DFA states of every group by how often a walk over
+// `d_corpus` visits them and rebuilds the hot-row layout: the placement of
+// rows in shared memory versus L2 is learned from the workload.
+void regex_rerank_from_corpus(RegexPlan& plan, const uint8_t* d_corpus, uint64_t len);
 void regex_fill_info(const RegexPlan& plan, ws_matcher_info& info);
 // Enqueues the regex pipeline on `st`.  `events` (8 CUDA events) is non-null
 // when phase timing is wanted.  Returns the number of kernel launches.
@@ -77,7 +97,7 @@ uint32_t run_regex_scan(RegexPlan& plan, const RegexLaunch& l, cudaStream_t st, 
 // a scan whose candidate or event buffer overflowed).
 constexpr size_t kRegexErrorFlagOffset = 16;
 void regex_collect_timing(const RegexPlan& plan, cudaEvent_t* events, ws_matcher_info& info);
-// K candidates only (diagnostic entry point); returns their device count pointer.
+// K candidates only (diagnostic entry point), copied to host_out.
 uint64_t regex_candidates(RegexPlan& plan, const uint8_t* d_data, uint64_t len, uint32_t mode, cudaStream_t st,
                           DeviceBuffer& scratch, int sm_count, ws_match* host_out, uint64_t cap);
 
