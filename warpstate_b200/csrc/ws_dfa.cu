@@ -312,16 +312,18 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
 // blockIdx.y = group; the group's hottest rows sit in shared memory.
 __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, ScanPtrs p) {
   extern __shared__ __align__(16) uint32_t smem[];
-  const uint32_t g = blockIdx.y;
+  // blockIdx.x = group (fastest), so the groups' blocks over the same chunks
+  // run together and the input is read from HBM once, then from L2
+  const uint32_t g = blockIdx.x;
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
   uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + hot_smem_bytes(gd.hot_rows) - 256;
   stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s);
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t i = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
   if (i >= p.n_chunks) return;
   const uint32_t* tab = t.fwd + gd.fwd_off;
   const uint32_t C = gd.n_classes, H = gd.hot_rows;
-  const uint32_t lane4 = (threadIdx.x & 31) * 4;
+  const int32_t lane4 = (int32_t)((threadIdx.x & 31) * 4);
   const uint64_t q = (uint64_t)g * p.n_chunks + i;
   const uint64_t c0 = i * p.chunk;
   const uint64_t c1 = min(p.len, c0 + p.chunk);
@@ -331,33 +333,59 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
   p.round[q] = 0;
   uint32_t* ck = p.ckpt + q * p.nck;
   uint32_t cold_row = 0;
-  uint32_t st = state_of(start, 0, H, lane4, &cold_row);
-  uint64_t pos = c0;
-  for (; pos + 16 <= c1; pos += 16) {
-    uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + pos));
-    uint32_t words[4] = {v.x, v.y, v.z, v.w};
+  uint32_t st = state_of(start, 0, H, (uint32_t)lane4, &cold_row);
+  const uint64_t nfull = (c1 - c0) / 16;
+  // four 16-byte vectors in flight ahead of the walk
+  constexpr int kAhead = 4;
+  uint4 ring[kAhead];
+#pragma unroll
+  for (int a = 0; a < kAhead; ++a)
+    ring[a] = (uint64_t)a < nfull ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + a * 16)) : make_uint4(0, 0, 0, 0);
+  for (uint64_t k16 = 0; k16 < nfull; ++k16) {
+    const uint4 cur = ring[0];
+    const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+    for (int a = 0; a < kAhead - 1; ++a) ring[a] = ring[a + 1];
+    ring[kAhead - 1] = (k16 + kAhead < nfull) ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + (k16 + kAhead) * 16))
+                                              : make_uint4(0, 0, 0, 0);
+    // optimistic pass: fast entries only; a slow word (negative) sends the walk
+    // to the first row (in bounds) and marks the block for the careful pass
+    const uint32_t st0 = st, cold0 = cold_row;
+    uint32_t acc = 0;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
       uint32_t w = WS_STEP_FAST(img, st, b);
-      if ((int32_t)w >= 0) {
-        st = max(w, lane4);
-      } else {
-        uint32_t m_row;
-        slow_step(w, b, st, cold_row, 0, H, lane4, cls_s, tab, C, m_row);
-        if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + k + 1), m_row, (uint32_t)q, 0);
+      acc |= w;
+      st = (uint32_t)max((int32_t)w, lane4);
+    }
+    if ((int32_t)acc < 0) {
+      // careful pass over the same 16 bytes: match events, cold rows
+      st = st0;
+      cold_row = cold0;
+      for (int k = 0; k < 16; ++k) {
+        uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+        uint32_t w = WS_STEP_FAST(img, st, b);
+        if ((int32_t)w >= 0) {
+          st = (uint32_t)max((int32_t)w, lane4);
+        } else {
+          uint32_t m_row;
+          slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
+          if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(c0 + k16 * 16 + k + 1), m_row, (uint32_t)q, 0);
+        }
       }
     }
-    if (((pos + 16 - c0) % kCkpt) == 0) ck[(pos + 16 - c0) / kCkpt - 1] = row_of(st, cold_row, 0);
+    const uint64_t done = (k16 + 1) * 16;
+    if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = row_of(st, cold_row, 0);
   }
-  for (; pos < c1; ++pos) {
+  for (uint64_t pos = c0 + nfull * 16; pos < c1; ++pos) {
     uint32_t b = __ldg(p.data + pos);
     uint32_t w = WS_STEP_FAST(img, st, b);
     if ((int32_t)w >= 0) {
-      st = max(w, lane4);
+      st = (uint32_t)max((int32_t)w, lane4);
     } else {
       uint32_t m_row;
-      slow_step(w, b, st, cold_row, 0, H, lane4, cls_s, tab, C, m_row);
+      slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
       if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
     }
   }
@@ -655,7 +683,7 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
     mark(4);
     return launches;
   }
-  dim3 cgrid((unsigned)((p.n_chunks + kWalkThreads - 1) / kWalkThreads), P.n_groups);
+  dim3 cgrid(P.n_groups, (unsigned)((p.n_chunks + kWalkThreads - 1) / kWalkThreads));
   if (P.proposer && P.use_proposer) {
     launches += proposer_predict(*P.proposer, p.data, p.len, p.chunk, p.n_chunks, p.guess, st);
   } else {
