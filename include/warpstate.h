@@ -140,7 +140,8 @@ typedef struct {
   uint64_t proposer_train_bytes;   /* default 256 MiB */
   uint64_t proposer_seed;          /* corpus seed for proposer training */
   uint32_t flags;                  /* WS_FLAG_* below */
-  uint32_t reserved[7];
+  uint32_t batch_mib;              /* ws_scan_batch: bytes per launch sequence, MiB (0: 1024) */
+  uint32_t reserved[6];
 } ws_config;
 
 enum { WS_REGEX_SPECULATIVE = 0, WS_REGEX_PLAIN = 1 };

@@ -49,6 +49,11 @@ def lib():
         L.or_regex_set_scan.restype = ctypes.c_uint64
         L.or_regex_set_scan.argtypes = [ctypes.POINTER(ctypes.c_void_p), u32p, ctypes.c_uint32, u8p,
                                         ctypes.c_uint64, ctypes.POINTER(OrMatch), ctypes.c_uint64, ctypes.c_int]
+        L.or_batch_scan.restype = ctypes.c_uint64
+        L.or_batch_scan.argtypes = [u8p, u32p, u32p, ctypes.c_uint32, ctypes.c_uint32,
+                                    ctypes.POINTER(ctypes.c_void_p), u32p, ctypes.c_uint32, u8p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                    ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]
         L.or_sort_matches.argtypes = [ctypes.POINTER(OrMatch), ctypes.c_uint64]
         L.or_hw_threads.restype = ctypes.c_int
         _L = L
@@ -204,6 +209,63 @@ def scan_patterns(patterns: list[tuple[int, bytes]], data, threads: int = 0) -> 
                 rx_ids.append(i)
     parts = [literal_scan(lits, lit_ids, data, threads), regex_scan(rxs, rx_ids, data, threads)]
     return sort_matches(np.concatenate(parts, axis=0))
+
+
+def split_patterns(patterns: list[tuple[int, bytes]]):
+    """(literals, literal ids, Regex handles, regex ids), with the reference's
+    regex -> literal demotion applied."""
+    lits, lit_ids, rxs, rx_ids = [], [], [], []
+    for i, (kind, b) in enumerate(patterns):
+        if kind == 0:
+            lits.append(bytes(b))
+            lit_ids.append(i)
+        else:
+            src = b.decode() if isinstance(b, (bytes, bytearray)) else b
+            lit = regex_literal(src)
+            if lit:
+                lits.append(lit)
+                lit_ids.append(i)
+            else:
+                rxs.append(Regex(src))
+                rx_ids.append(i)
+    return lits, lit_ids, rxs, rx_ids
+
+
+TAGGED = np.dtype([("sid", "<u8"), ("pid", "<u4"), ("start", "<u4"), ("end", "<u4"), ("res", "<u4")])
+
+
+def batch_scan(patterns: list[tuple[int, bytes]], data, items, ids=None, threads: int = 0) -> np.ndarray:
+    """Batch contract (scan_batch_cpu, core/src/batch.rs:170-195): items are
+    (offset, length) slices of ``data``, each scanned on its own; returns an
+    (n, 4) uint64 array (source_id, pattern_id, start, end) sorted by
+    (source_id, start, pattern_id, end)."""
+    lits, lit_ids, rxs, rx_ids = split_patterns(patterns)
+    packed = b"".join(lits)
+    offs, o = [], 0
+    for l in lits:
+        offs += [o, len(l)]
+        o += len(l)
+    pk, ppk = _u8(packed if packed else b"\0")
+    of, pof = _u32(offs if offs else [0, 0])
+    li, pli = _u32(lit_ids if lit_ids else [0])
+    ri, pri = _u32(rx_ids if rx_ids else [0])
+    hs = (ctypes.c_void_p * max(len(rxs), 1))(*[r.h for r in rxs])
+    d, pd = _u8(data)
+    it = np.asarray(items, dtype=np.uint64).reshape(-1, 2)
+    off = np.ascontiguousarray(it[:, 0])
+    ln = np.ascontiguousarray(it[:, 1])
+    sid = np.arange(len(it), dtype=np.uint64) if ids is None else np.ascontiguousarray(ids, dtype=np.uint64)
+    cap = 1 << 16
+    while True:
+        out = np.empty(cap, dtype=TAGGED)
+        n = lib().or_batch_scan(ppk, pof, pli, len(lits), 8, hs, pri, len(rxs), pd, off.ctypes.data,
+                                ln.ctypes.data, sid.ctypes.data, len(it), out.ctypes.data, cap, threads)
+        if n <= cap:
+            o = out[:n]
+            res = np.empty((n, 4), dtype=np.uint64)
+            res[:, 0], res[:, 1], res[:, 2], res[:, 3] = o["sid"], o["pid"], o["start"], o["end"]
+            return res
+        cap = int(n)
 
 
 def hw_threads() -> int:

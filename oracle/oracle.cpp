@@ -927,6 +927,124 @@ uint64_t or_regex_set_scan(or_regex* const* rs, const uint32_t* pattern_ids, uin
   return total;
 }
 
+// scan_batch_cpu (core/src/batch.rs:170-195): every item scanned on its own
+// (contract L + contract R inside the item), matches tagged with the item id
+// and sorted by (source_id, start, pattern_id, end).  The literal table and
+// the regexes' first-byte-pair indexes are built once; items are spread over
+// the threads.
+uint64_t or_batch_scan(const uint8_t* packed, const uint32_t* offsets, const uint32_t* literal_pattern_ids,
+                       uint32_t n_literals, uint32_t window, or_regex* const* rs, const uint32_t* regex_pattern_ids,
+                       uint32_t n_regex, const uint8_t* data, const uint64_t* item_off, const uint64_t* item_len,
+                       const uint64_t* item_id, uint64_t n_items, or_tagged_match* out, uint64_t cap,
+                       int nthreads) {
+  // literal prefilter table, as or_literal_scan builds it
+  std::vector<uint32_t> hashes(n_literals), meta(4 * window), ranges, ents;
+  if (n_literals) {
+    for (uint32_t li = 0; li < n_literals; ++li)
+      hashes[li] = or_fnv1a(packed + offsets[2 * li], offsets[2 * li + 1], window);
+    uint32_t nb = 0;
+    or_prefilter_build(offsets, hashes.data(), n_literals, window, nullptr, nullptr, &nb, nullptr);
+    ranges.resize(2 * (size_t)nb);
+    ents.resize(2 * (size_t)n_literals);
+    or_prefilter_build(offsets, hashes.data(), n_literals, window, meta.data(), ranges.data(), &nb, ents.data());
+  }
+  // regexes: general ones use find_iter_one, the rest share first-pair indexes
+  // in blocks of 32 (as or_regex_set_scan)
+  struct Block {
+    std::vector<uint32_t> members;
+    std::vector<std::vector<uint16_t>> index, last_byte;
+  };
+  std::vector<uint32_t> general;
+  std::vector<Block> blocks;
+  for (uint32_t k = 0; k < n_regex; ++k) {
+    const Program& P = rs[k]->prog;
+    if (P.nullable || P.has_assert) { general.push_back(k); continue; }
+    if (blocks.empty() || blocks.back().members.size() == 32) blocks.emplace_back();
+    blocks.back().members.push_back(k);
+  }
+  for (auto& b : blocks) {
+    b.index.assign(65536, {});
+    b.last_byte.assign(256, {});
+    for (uint16_t j = 0; j < b.members.size(); ++j) {
+      const Program& P = rs[b.members[j]]->prog;
+      for (size_t key = 0; key < 65536; ++key)
+        if ((P.pair_ok[key >> 6] >> (key & 63)) & 1) b.index[key].push_back(j);
+      for (int c = 0; c < 256; ++c) if (P.one_byte[c]) b.last_byte[c].push_back(j);
+    }
+  }
+  int T = std::max(1, std::min<int>(resolve_threads(nthreads), (int)std::max<uint64_t>(n_items, 1)));
+  std::vector<std::vector<or_tagged_match>> res(T);
+  std::atomic<uint64_t> next{0};
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; ++t) {
+    th.emplace_back([&, t] {
+      std::vector<std::unique_ptr<Backtracker>> bts;
+      for (uint32_t k = 0; k < n_regex; ++k) bts.emplace_back(new Backtracker(rs[k]->prog));
+      std::vector<std::pair<uint32_t, uint32_t>> tmp;
+      std::vector<uint64_t> cursor;
+      auto& r = res[t];
+      while (true) {
+        uint64_t it = next.fetch_add(1);
+        if (it >= n_items) break;
+        const uint8_t* d = data + item_off[it];
+        const uint64_t len = item_len[it], sid = item_id[it];
+        // contract L inside the item
+        for (uint64_t pos = 0; n_literals && pos < len; ++pos) {
+          uint32_t h = FNV_BASIS;
+          uint64_t maxp = std::min<uint64_t>(window, len - pos);
+          for (uint64_t i = 0; i < maxp; ++i) {
+            h = (h ^ d[pos + i]) * FNV_PRIME;
+            const uint32_t* m = &meta[4 * i];
+            if (m[2] == 0) continue;
+            uint32_t bi = m[0] + (h & m[1]);
+            uint32_t es = ranges[2 * bi], ec = ranges[2 * bi + 1];
+            for (uint32_t e = 0; e < ec; ++e) {
+              if (ents[2 * (es + e)] != h) continue;
+              uint32_t li = ents[2 * (es + e) + 1];
+              uint32_t lo = offsets[2 * li], ll = offsets[2 * li + 1];
+              if (pos + ll > len) continue;
+              if (std::memcmp(d + pos, packed + lo, ll) == 0)
+                r.push_back({sid, literal_pattern_ids[li], (uint32_t)pos, (uint32_t)(pos + ll), 0});
+            }
+          }
+        }
+        // contract R inside the item
+        for (uint32_t k : general) {
+          tmp.clear();
+          find_iter_one(rs[k], d, len, tmp);
+          for (auto& m : tmp) r.push_back({sid, regex_pattern_ids[k], m.first, m.second, 0});
+        }
+        for (const auto& b : blocks) {
+          cursor.assign(b.members.size(), 0);
+          for (uint64_t q = 0; q < len; ++q) {
+            const std::vector<uint16_t>& lst =
+                (q + 1 < len) ? b.index[(size_t)d[q] << 8 | d[q + 1]] : b.last_byte[d[q]];
+            for (uint16_t j : lst) {
+              if (q < cursor[j]) continue;
+              int64_t e = bts[b.members[j]]->run(d, len, q);
+              if (e >= 0) {
+                r.push_back({sid, regex_pattern_ids[b.members[j]], (uint32_t)q, (uint32_t)e, 0});
+                cursor[j] = (uint64_t)e;
+              }
+            }
+          }
+        }
+      }
+    });
+  }
+  for (auto& x : th) x.join();
+  std::vector<or_tagged_match> all;
+  for (auto& r : res) all.insert(all.end(), r.begin(), r.end());
+  std::sort(all.begin(), all.end(), [](const or_tagged_match& a, const or_tagged_match& b) {
+    if (a.source_id != b.source_id) return a.source_id < b.source_id;
+    if (a.start != b.start) return a.start < b.start;
+    if (a.pattern_id != b.pattern_id) return a.pattern_id < b.pattern_id;
+    return a.end < b.end;
+  });
+  for (uint64_t k = 0; k < all.size() && k < cap; ++k) out[k] = all[k];
+  return all.size();
+}
+
 void or_sort_matches(or_match* m, uint64_t n) {
   std::sort(m, m + n, [](const or_match& a, const or_match& b) {
     if (a.start != b.start) return a.start < b.start;

@@ -77,6 +77,17 @@ uint64_t or_regex_set_scan(or_regex* const* rs, const uint32_t* pattern_ids, uin
                            const uint8_t* data, uint64_t len,
                            or_match* out, uint64_t cap, int nthreads);
 
+/* Batch contract: every item scanned independently (L + R inside the item),
+ * tagged with its id, sorted by (source_id, start, pattern_id, end) -- the
+ * structure of scan_batch_cpu (core/src/batch.rs:170-195).  Items are
+ * (item_off[i], item_len[i]) slices of data.  Returns the true count. */
+typedef struct { uint64_t source_id; uint32_t pattern_id, start, end, reserved; } or_tagged_match;
+uint64_t or_batch_scan(const uint8_t* packed, const uint32_t* offsets, const uint32_t* literal_pattern_ids,
+                       uint32_t n_literals, uint32_t window, or_regex* const* rs, const uint32_t* regex_pattern_ids,
+                       uint32_t n_regex, const uint8_t* data, const uint64_t* item_off, const uint64_t* item_len,
+                       const uint64_t* item_id, uint64_t n_items, or_tagged_match* out, uint64_t cap,
+                       int nthreads);
+
 /* Sort matches by (start, pattern_id, end): the CPU path's order
  * (core/src/cpu/mod.rs:56-78). */
 void or_sort_matches(or_match* m, uint64_t n);

@@ -1,0 +1,243 @@
+"""Batch and stream scans on the GPU against the oracle, bit-exact.
+
+Batch (core/src/batch.rs): every item scanned on its own, matches tagged with
+the item id, sorted by (source_id, start, pattern_id, end), no cross-item
+match -- the reference's batch known answers and GPU batch tests
+(core/tests/unit/gpu_batch.rs), per-item regex chains, launch-group splits,
+and a scaled mixed literal + regex workload against the batch oracle.
+
+Stream (core/src/pipeline.rs, core/src/stream.rs): pieces fed in any sizes
+give exactly the whole-input scan -- the reference's stream known answers, and
+random piece sizes over literal + regex workloads in both regex modes.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+import workloads as w
+
+pytestmark = pytest.mark.gpu
+
+PLAIN, SPEC = 1, 0
+
+
+def _ws():
+    import warpstate_b200 as ws
+    return ws
+
+
+def matcher(patterns, mode=SPEC, **cfg):
+    ws = _ws()
+    b = ws.PatternSet.builder()
+    for kind, p in patterns:
+        b = b.literal_bytes(p) if kind == 0 else b.regex(p.decode() if isinstance(p, bytes) else p)
+    c = ws.AutoMatcherConfig().regex_mode(mode)
+    for k, v in cfg.items():
+        getattr(c, k)(v)
+    return ws.GpuMatcher.with_config(b.build(), c)
+
+
+def tagged_rows(tagged):
+    return [[t.source_id, t.matched.pattern_id, t.matched.start, t.matched.end] for t in tagged]
+
+
+# ----------------------------------------------------------------- batch
+def test_batch_golden(golden):
+    ws = _ws()
+    for case in golden["batch"]:
+        m = matcher([(0, p.encode()) for p in case["patterns"]])
+        items = [ws.ScanItem(i, s.encode()) for i, s in case["items"]]
+        assert tagged_rows(ws.scan_batch_gpu(m, items)) == case["expected"], case["src"]
+
+
+def test_batch_attributes_100_items():
+    # core/tests/unit/gpu_batch.rs:7-33
+    ws = _ws()
+    m = ws.AutoMatcher.with_config(ws.PatternSet.builder().literal("needle").build(),
+                                   ws.AutoMatcherConfig.new().gpu_threshold(0))
+    items = [ws.ScanItem(i, f"id-{i:03}-needle".encode()) for i in range(100)]
+    got = ws.scan_batch_gpu(m, items)
+    assert len(got) == 100
+    for i, t in enumerate(got):
+        assert (t.source_id, t.matched.pattern_id, t.matched.start) == (i, 0, 7)
+
+
+def test_batch_rejects_cross_item_matches():
+    # core/tests/unit/gpu_batch.rs:36-67
+    ws = _ws()
+    m = ws.AutoMatcher.with_config(ws.PatternSet.builder().literal("needle").build(),
+                                   ws.AutoMatcherConfig.new().gpu_threshold(0))
+    data = [b"nee" if i == 49 else b"dle" if i == 50 else f"item-{i:03}-needle".encode() for i in range(100)]
+    got = ws.scan_batch_gpu(m, [ws.ScanItem(i, d) for i, d in enumerate(data)])
+    assert len(got) == 98
+    assert not any(t.source_id in (49, 50) for t in got)
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_batch_regex_chains_are_per_item(mode):
+    # one find_iter chain per item: a greedy regex does not run across items,
+    # a match is not lost to a chain that started in the previous item
+    ws = _ws()
+    pats = [(1, b"a+b?"), (1, b"x[yz]{1,3}"), (0, b"ab")]
+    m = matcher(pats, mode=mode)
+    datas = [b"aaa", b"aab", b"baaa", b"xy", b"zxzz", b"", b"aaaaaaaaab", b"x"]
+    items = [ws.ScanItem(i, d) for i, d in enumerate(datas)]
+    got = tagged_rows(ws.scan_batch_gpu(m, items))
+    exp = oracle.batch_scan(pats, b"".join(datas), _offsets(datas)).tolist()
+    assert got == exp
+    assert [0, 0, 0, 3] in got and [1, 0, 0, 3] in got  # "aaa" | "aab" not merged
+
+
+def _offsets(datas):
+    out, off = [], 0
+    for d in datas:
+        out.append((off, len(d)))
+        off += len(d)
+    return out
+
+
+def test_batch_ids_unsorted_duplicated_and_empty():
+    ws = _ws()
+    pats = [(0, b"abc"), (1, b"b[cd]{2}")]
+    m = matcher(pats)
+    datas = [b"xxabcdd", b"", b"abcabc", b"bdd", b"zzz"]
+    ids = [7, 3, 7, 0, 1]
+    got = tagged_rows(ws.scan_batch_gpu(m, [ws.ScanItem(i, d) for i, d in zip(ids, datas)]))
+    exp = oracle.batch_scan(pats, b"".join(datas), _offsets(datas), ids).tolist()
+    assert got == exp
+    assert ws.scan_batch_gpu(m, []) == []
+    assert ws.scan_batch_gpu(m, [ws.ScanItem(5, b"")]) == []
+
+
+def test_batch_overflow_reports_true_count():
+    ws = _ws()
+    m = matcher([(0, b"a")], max_matches=10)
+    with pytest.raises(ws.MatchBufferOverflow) as e:
+        ws.scan_batch_gpu(m, [ws.ScanItem(0, b"a" * 8), ws.ScanItem(1, b"a" * 8)])
+    assert e.value.count == 16
+
+
+def _batch_workload(n_items=2000, seed=21):
+    return w.batch(n_items=n_items, n_lit=300, n_rx=60, seed=seed, median=2048.0, hi=64 * 1024)
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_batch_scaled_vs_oracle(mode):
+    ws = _ws()
+    wl = _batch_workload()
+    m = matcher(wl.patterns, mode=mode)
+    lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+    got = ws.scan_batch_packed(m, wl.data, lens)
+    exp = oracle.batch_scan(wl.patterns, wl.data, wl.items)
+    assert len(exp) > 200
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
+def test_batch_launch_groups_and_planner_agree():
+    # a 1 MiB launch budget splits the batch into several launch sequences;
+    # the reference planner's grouping (scan_batch) gives the same result
+    ws = _ws()
+    wl = _batch_workload(n_items=600, seed=22)
+    m1 = matcher(wl.patterns, batch_mib=1)
+    items = [ws.ScanItem(i, wl.data[o:o + ln]) for i, (o, ln) in enumerate(wl.items)]
+    one = tagged_rows(ws.scan_batch_gpu(m1, items))
+    exp = oracle.batch_scan(wl.patterns, wl.data, wl.items).tolist()
+    assert one == exp
+    nested = ws.scan_batch(m1, [it.data for it in items], ws.BatchConfig(max_inputs=37, max_bytes=200_000))
+    flat = sorted([[i, x.pattern_id, x.start, x.end] for i, ms in enumerate(nested) for x in ms],
+                  key=lambda r: (r[0], r[2], r[1], r[3]))
+    assert flat == exp
+
+
+def test_pattern_set_scan_batch_spelling():
+    # README spelling: patterns.scan_batch(items)
+    ws = _ws()
+    ps = ws.PatternSet.builder().literal("needle").build()
+    got = ps.scan_batch([ws.ScanItem(1, b"a needle"), ws.ScanItem(2, b"none")])
+    assert tagged_rows(got) == [[1, 0, 2, 8]]
+
+
+# ---------------------------------------------------------------- stream
+def test_stream_golden(golden):
+    ws = _ws()
+    for case in golden["stream"]:
+        m = matcher([(0, p.encode()) for p in case["patterns"]])
+        out = []
+        with ws.Stream(m) as s:
+            for f in case["feeds"]:
+                out += s.feed(f.encode())
+            out += s.end()
+        out.sort(key=lambda x: (x.start, x.pattern_id, x.end))
+        assert [[x.pattern_id, x.start, x.end] for x in out] == case["expected"], case["src"]
+
+
+def _pieces(n, seed, max_piece):
+    r = np.random.default_rng(seed)
+    cuts, pos = [], 0
+    while pos < n:
+        k = int(r.integers(0, max_piece + 1))
+        cuts.append((pos, min(n, pos + k)))
+        pos = min(n, pos + k)
+    return cuts
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_stream_random_pieces_equal_whole_scan(mode):
+    ws = _ws()
+    wl = w.regex(size=2 << 20, n=80, seed=31)
+    lits = w.literals_large(size=1 << 10, n=200, seed=32).patterns
+    pats = wl.patterns + lits
+    data = wl.data
+    m = matcher(pats, mode=mode)
+    whole = m.scan_array(data).astype(np.uint64)
+    exp = oracle.scan_patterns(pats, data).astype(np.uint64)
+    assert np.array_equal(whole, exp) and len(exp) > 50
+    # (seed, largest piece, bytes streamed): tiny pieces over a prefix only
+    for seed, maxp, n in ((1, 64, 96 << 10), (2, 8192, len(data)), (3, 300_000, len(data))):
+        ref = exp if n == len(data) else oracle.scan_patterns(pats, data[:n]).astype(np.uint64)
+        parts = []
+        with ws.Stream(m) as s:
+            for a, b in _pieces(n, seed, maxp):
+                parts.append(s.feed_ptr_array(data.ctypes.data + a, b - a))
+            parts.append(s.end_array())
+        got = np.concatenate(parts)
+        got = got[np.lexsort((got[:, 2], got[:, 0], got[:, 1]))]
+        assert np.array_equal(got, ref), (seed, maxp)
+
+
+def test_stream_pipeline_scan_and_unbounded_regex():
+    ws = _ws()
+    r = np.random.default_rng(5)
+    data = r.choice(np.frombuffer(b"abcx", np.uint8), size=1 << 20).astype(np.uint8)
+    pats = [(1, b"ab+c"), (1, b"x[ab]*x"), (0, b"cab"), (0, b"xx")]
+    m = matcher(pats)
+    exp = oracle.scan_patterns(pats, data).astype(np.uint64)
+    got = ws.StreamPipeline(m, 4096).scan_array(data, block=100_000)
+    assert np.array_equal(got, exp)
+    assert len(exp) > 1000
+
+
+def test_stream_drains_when_the_output_is_small():
+    ws = _ws()
+    import warpstate_b200._native as N
+    m = matcher([(0, b"ab")])
+    h = ctypes.c_void_p()
+    err = N.WsErrorInfo()
+    assert N.lib().ws_stream_begin(m._h, ctypes.byref(h), ctypes.byref(err)) == 0
+    out = (N.WsMatch64 * 2)()
+    cnt = ctypes.c_uint64()
+    data = b"ab" * 5
+    st = N.lib().ws_stream_feed(h, data, len(data), out, 2, ctypes.byref(cnt), ctypes.byref(err))
+    assert st == 11 and cnt.value == 2 and err.count == 5
+    got = [(out[k].start, out[k].end) for k in range(cnt.value)]
+    while True:
+        st = N.lib().ws_stream_feed(h, None, 0, out, 2, ctypes.byref(cnt), ctypes.byref(err))
+        got += [(out[k].start, out[k].end) for k in range(cnt.value)]
+        if st == 0:
+            break
+        assert st == 11
+    assert N.lib().ws_stream_end(h, out, 2, ctypes.byref(cnt), ctypes.byref(err)) == 0 and cnt.value == 0
+    N.lib().ws_stream_destroy(h)
+    assert sorted(got) == [(2 * k, 2 * k + 2) for k in range(5)]

@@ -361,6 +361,11 @@ class AutoMatcherConfig:
             self.c.proposer_seed = int(seed)
         return self
 
+    def batch_mib(self, n: int):
+        """Bytes per batch launch sequence, in MiB (0: 1024)."""
+        self.c.batch_mib = int(n)
+        return self
+
     def profile(self, yes: bool = True):
         """Record CUDA events around each kernel phase (GpuMatcher.info())."""
         self.c.flags = (self.c.flags | 1) if yes else (self.c.flags & ~1)
@@ -566,24 +571,134 @@ class AutoMatcher:
 # ----------------------------------------------------------------- batch
 @dataclass
 class ScanItem:
+    """batch::ScanItem (core/src/batch.rs:13-18)."""
     id: int
     data: object
 
 
 @dataclass(frozen=True)
 class TaggedMatch:
+    """batch::TaggedMatch (core/src/batch.rs:22-27): offsets relative to the item."""
     source_id: int
     matched: Match
 
 
 @dataclass
 class BatchConfig:
+    """batch::BatchConfig (core/src/batch.rs:31-48)."""
     max_inputs: int = 4096
     max_bytes: int = 256 * 1024 * 1024
     sort_by_size: bool = True
 
 
-def _batch_raw(matcher: GpuMatcher, items: Sequence[ScanItem]) -> list[TaggedMatch]:
+@dataclass
+class CoalesceMap:
+    """batch::CoalesceMap (core/src/batch.rs:51-57): ``entries`` holds
+    ``(source_id, start_offset_in_buffer, length)``."""
+    entries: list
+    buffer: bytes
+
+
+_U32_MAX = 0xFFFFFFFF
+
+
+def _tagged_key(t: TaggedMatch):
+    return (t.source_id, t.matched.start, t.matched.pattern_id, t.matched.end)
+
+
+def coalesce(items: Sequence[ScanItem]) -> CoalesceMap:
+    """batch::coalesce (core/src/batch.rs:65-98): one contiguous buffer and the
+    item map; InputTooLarge beyond 32-bit offsets."""
+    total = 0
+    for it in items:
+        n = it.data.nbytes if isinstance(it.data, np.ndarray) else len(it.data)
+        if n > _U32_MAX:
+            raise InputTooLarge(n, _U32_MAX)
+        total += n
+    if total > _U32_MAX:
+        raise InputTooLarge(total, _U32_MAX)
+    parts, entries, off = [], [], 0
+    for it in items:
+        b = bytes(memoryview(it.data).cast("B")) if not isinstance(it.data, np.ndarray) else it.data.tobytes()
+        entries.append((int(it.id), off, len(b)))
+        parts.append(b)
+        off += len(b)
+    return CoalesceMap(entries, b"".join(parts))
+
+
+def decoalesce(cmap: CoalesceMap, global_matches: Sequence[Match]) -> list[TaggedMatch]:
+    """batch::decoalesce (core/src/batch.rs:106-167): attribute position-sorted
+    matches of a coalesced buffer to their items, dropping matches that cross
+    an item boundary; sorted by (source_id, start, pattern_id, end)."""
+    tagged, cursor, entries = [], 0, cmap.entries
+    for m in global_matches:
+        while cursor < len(entries) and not m.start < entries[cursor][1] + entries[cursor][2]:
+            cursor += 1
+        if cursor >= len(entries):
+            break
+        sid, off, ln = entries[cursor]
+        if m.start < off or m.end > off + ln:
+            continue
+        tagged.append(TaggedMatch(sid, Match(m.pattern_id, m.start - off, m.end - off)))
+    tagged.sort(key=_tagged_key)
+    return tagged
+
+
+def planned_batches(inputs: Sequence, config: BatchConfig) -> list[list[int]]:
+    """The batch planner of core/src/batch.rs:197-236: largest inputs first
+    (when ``sort_by_size``), closing a batch at ``max_inputs`` items or
+    ``max_bytes`` bytes."""
+    if not inputs:
+        return []
+    max_inputs, max_bytes = max(config.max_inputs, 1), max(config.max_bytes, 1)
+    lens = [len(x) if not isinstance(x, np.ndarray) else x.nbytes for x in inputs]
+    order = list(range(len(inputs)))
+    if config.sort_by_size:
+        order.sort(key=lambda i: -lens[i])  # stable: equal sizes keep input order
+    batches, cur, cur_bytes = [], [], 0
+    for idx in order:
+        ln = lens[idx]
+        if cur and (len(cur) >= max_inputs or cur_bytes + ln > max_bytes):
+            batches.append(cur)
+            cur, cur_bytes = [], 0
+        cur.append(idx)
+        cur_bytes += ln
+        if len(cur) >= max_inputs or cur_bytes >= max_bytes:
+            batches.append(cur)
+            cur, cur_bytes = [], 0
+    if cur:
+        batches.append(cur)
+    return batches
+
+
+def tagged_to_nested(tagged: Iterable[TaggedMatch], input_count: int) -> list[list[Match]]:
+    """core/src/batch.rs:238-250: group tagged matches by input index."""
+    grouped: list[list[Match]] = [[] for _ in range(input_count)]
+    for t in tagged:
+        if 0 <= t.source_id < input_count:
+            grouped[t.source_id].append(t.matched)
+    return grouped
+
+
+def _batch_array(matcher: "GpuMatcher", arr, n: int) -> np.ndarray:
+    """ws_scan_batch over a prepared WsItem array; (k, 4) uint64 rows
+    (source_id, pattern_id, start, end), sorted."""
+    cap = max(int(matcher.config.c.max_matches), 1)
+    out = np.empty(cap, dtype=np.dtype([("sid", "<u8"), ("pid", "<u4"), ("start", "<u4"), ("end", "<u4"),
+                                         ("res", "<u4")]))
+    cnt = ctypes.c_uint64()
+    _call(N.lib().ws_scan_batch, matcher._h, arr, n, out.ctypes.data_as(ctypes.POINTER(N.WsTaggedMatch)), cap,
+          ctypes.byref(cnt))
+    o = out[: cnt.value]
+    res = np.empty((cnt.value, 4), dtype=np.uint64)
+    res[:, 0] = o["sid"]
+    res[:, 1] = o["pid"]
+    res[:, 2] = o["start"]
+    res[:, 3] = o["end"]
+    return res
+
+
+def _batch_raw(matcher: "GpuMatcher", items: Sequence[ScanItem]) -> list[TaggedMatch]:
     n = len(items)
     if n == 0:
         return []
@@ -595,74 +710,126 @@ def _batch_raw(matcher: GpuMatcher, items: Sequence[ScanItem]) -> list[TaggedMat
         arr[i].id = int(it.id)
         arr[i].data = ptr
         arr[i].len = ln
-    cap = max(int(matcher.config.c.max_matches), 1)
-    out = (N.WsTaggedMatch * cap)()
-    cnt = ctypes.c_uint64()
-    _call(N.lib().ws_scan_batch, matcher._h, arr, n, out, cap, ctypes.byref(cnt))
-    res = []
-    for k in range(cnt.value):
-        o = out[k]
-        res.append(TaggedMatch(int(o.source_id), Match(int(o.pattern_id), int(o.start), int(o.end))))
+    rows = _batch_array(matcher, arr, n)
+    del keep
+    return [TaggedMatch(int(a), Match(int(b), int(c), int(d))) for a, b, c, d in rows.tolist()]
+
+
+def scan_batch_packed(matcher: "GpuMatcher | AutoMatcher", arena, lengths, ids=None) -> np.ndarray:
+    """Batch scan of items stored back to back in one host buffer (``arena``;
+    a pinned tensor avoids the staging copy).  ``lengths[i]`` bytes belong to
+    item ``ids[i]`` (default ``i``).  Returns an (n, 4) uint64 array of
+    (source_id, pattern_id, start, end), item-relative offsets, sorted by
+    (source_id, start, pattern_id, end) -- the result of ``scan_batch_gpu``."""
+    m = matcher.matcher() if isinstance(matcher, AutoMatcher) else matcher
+    ptr, total, keep = _buffer(arena)
+    lengths = np.asarray(lengths, dtype=np.uint64)
+    n = int(lengths.size)
+    if int(lengths.sum()) > total:
+        raise ValueError("item lengths exceed the arena")
+    if n == 0:
+        return np.empty((0, 4), dtype=np.uint64)
+    starts = np.zeros(n, dtype=np.uint64)
+    np.cumsum(lengths[:-1], out=starts[1:])
+    rec = np.empty(n, dtype=np.dtype([("id", "<u8"), ("data", "<u8"), ("len", "<u8")]))
+    rec["id"] = np.arange(n, dtype=np.uint64) if ids is None else np.asarray(ids, dtype=np.uint64)
+    rec["data"] = np.uint64(ptr) + starts
+    rec["len"] = lengths
+    arr = ctypes.cast(rec.ctypes.data, ctypes.POINTER(N.WsItem))
+    res = _batch_array(m, arr, n)
+    del keep
     return res
 
 
-def scan_batch(matcher: GpuMatcher, inputs: Sequence, config: BatchConfig | None = None) -> list[list[Match]]:
-    """batch::scan_batch (core/src/batch.rs:296-303): per-input match lists."""
-    items = [ScanItem(i, d) for i, d in enumerate(inputs)]
+def scan_batch(matcher: "GpuMatcher", inputs: Sequence, config: BatchConfig | None = None) -> list[list[Match]]:
+    """batch::scan_batch (core/src/batch.rs:312-319): per-input match lists.
+    Inputs are grouped as the reference's planner groups them; each group is
+    one device launch sequence scanning every item on its own."""
+    config = config or BatchConfig()
     grouped: list[list[Match]] = [[] for _ in inputs]
-    for t in _batch_raw(matcher, items):
-        grouped[t.source_id].append(t.matched)
+    for batch in planned_batches(inputs, config):
+        for t in _batch_raw(matcher, [ScanItem(i, inputs[i]) for i in batch]):
+            grouped[t.source_id].append(t.matched)
     return grouped
 
 
-def scan_batch_auto(matcher: AutoMatcher, inputs: Sequence, config: BatchConfig | None = None) -> list[list[Match]]:
+def scan_batch_auto(matcher: "AutoMatcher", inputs: Sequence, config: BatchConfig | None = None) -> list[list[Match]]:
+    """batch::scan_batch_auto (core/src/batch.rs:321-328), always on the GPU."""
     return scan_batch(matcher.matcher(), inputs, config)
 
 
-def scan_batch_gpu(matcher: AutoMatcher | GpuMatcher, items: Iterable[ScanItem]) -> list[TaggedMatch]:
-    """batch::scan_batch_gpu (core/src/batch.rs:336-363): tagged, sorted by
-    (source_id, start, pattern_id, end)."""
+def scan_batch_gpu(matcher: "AutoMatcher | GpuMatcher", items: Iterable[ScanItem]) -> list[TaggedMatch]:
+    """batch::scan_batch_gpu (core/src/batch.rs:336-363): tagged matches sorted
+    by (source_id, start, pattern_id, end); no match crosses an item.  All
+    items go to the device planner (1 GiB per launch sequence by default)."""
     m = matcher.matcher() if isinstance(matcher, AutoMatcher) else matcher
     return _batch_raw(m, list(items))
 
 
+def _pattern_set_scan_batch(self, items: Iterable[ScanItem], matcher: "GpuMatcher | None" = None):
+    """``patterns.scan_batch(items)`` as README.md shows it: routes to the GPU."""
+    if matcher is None:
+        matcher = self.__dict__.get("_batch_matcher")
+        if matcher is None:
+            matcher = GpuMatcher(self)
+            self.__dict__["_batch_matcher"] = matcher
+    return scan_batch_gpu(matcher, items)
+
+
+PatternSet.scan_batch = _pattern_set_scan_batch
+
+
 # ---------------------------------------------------------------- stream
+_WS_ERR_OVERFLOW = 11
+
+
 class StreamPipeline:
-    """StreamPipeline (core/src/pipeline.rs:15-153) with DFA-state carry.
+    """StreamPipeline (core/src/pipeline.rs:15-153) with exact state carry.
 
-    ``scan(data)`` feeds the data through the device stream API in blocks of
-    the backend's ``max_block_size``; matches equal a whole-input scan."""
+    ``scan(data)`` pushes the data through the device stream API
+    (``ws_stream_*``), which decides every match exactly once; the result
+    equals a whole-input scan, with no overlap heuristic.  ``overlap_window``
+    is accepted for API compatibility and not needed."""
 
-    def __init__(self, backend: GpuMatcher, overlap_window: int = 0):
-        self.backend = backend
+    def __init__(self, backend: "GpuMatcher | AutoMatcher", overlap_window: int = 0):
+        self.backend = backend.matcher() if isinstance(backend, AutoMatcher) else backend
         self.overlap_window = overlap_window
 
-    def scan(self, data) -> list[Match]:
+    @staticmethod
+    def new(backend, overlap_window: int = 0) -> "StreamPipeline":
+        return StreamPipeline(backend, overlap_window)
+
+    def scan_array(self, data, block: int | None = None) -> np.ndarray:
+        """(n, 3) uint64 array of (pattern_id, start, end) sorted by (start, pattern_id, end)."""
         ptr, n, keep = _buffer(data)
-        if n == 0:
-            return []
-        block = max(int(self.backend.max_block_size()), 1)
-        out: list[Match] = []
+        parts = []
         with Stream(self.backend) as s:
-            base = ctypes.c_void_p(ptr).value
-            for off in range(0, n, block):
-                out.extend(s.feed_ptr(base + off, min(block, n - off)))
-            out.extend(s.end())
+            step = n if not block else max(int(block), 1)
+            for off in range(0, n, max(step, 1)):
+                parts.append(s.feed_ptr_array(ptr + off, min(step, n - off)))
+            parts.append(s.end_array())
         del keep
-        out.sort(key=lambda m: (m.start, m.pattern_id, m.end))
-        return out
+        a = np.concatenate(parts) if parts else np.empty((0, 3), dtype=np.uint64)
+        order = np.lexsort((a[:, 2], a[:, 0], a[:, 1])) if len(a) else np.empty(0, dtype=np.int64)
+        return a[order]
+
+    def scan(self, data) -> list[Match]:
+        return [Match(int(p), int(s), int(e)) for p, s, e in self.scan_array(data).tolist()]
 
 
 class Stream:
-    """Incremental scan with 64-bit offsets (ws_stream_*)."""
+    """Incremental scan with 64-bit offsets (ws_stream_*): every match is
+    returned by exactly one ``feed`` or by ``end``."""
 
-    def __init__(self, matcher: GpuMatcher):
+    def __init__(self, matcher: "GpuMatcher | AutoMatcher"):
+        matcher = matcher.matcher() if isinstance(matcher, AutoMatcher) else matcher
         self.m = matcher
         h = ctypes.c_void_p()
         _call(N.lib().ws_stream_begin, matcher._h, ctypes.byref(h))
         self._h = h
         self._cap = max(int(matcher.config.c.max_matches), 1)
-        self._out = (N.WsMatch64 * self._cap)()
+        self._out = np.empty(self._cap, dtype=np.dtype([("pid", "<u4"), ("res", "<u4"), ("start", "<u8"),
+                                                        ("end", "<u8")]))
 
     def __enter__(self):
         return self
@@ -670,13 +837,49 @@ class Stream:
     def __exit__(self, *a):
         self.close()
 
-    def _collect(self, n) -> list[Match]:
-        return [Match(int(self._out[k].pattern_id), int(self._out[k].start), int(self._out[k].end)) for k in range(n)]
+    def _rows(self, n: int) -> np.ndarray:
+        o = self._out[:n]
+        a = np.empty((n, 3), dtype=np.uint64)
+        a[:, 0], a[:, 1], a[:, 2] = o["pid"], o["start"], o["end"]
+        return a
+
+    def _collect(self, call) -> np.ndarray:
+        """Runs ``call(out, cap, n_out, err)``; while it reports overflow with
+        some matches delivered, drains the rest with more calls."""
+        parts = []
+        while True:
+            cnt = ctypes.c_uint64()
+            err = N.WsErrorInfo()
+            st = call(self._out.ctypes.data_as(ctypes.POINTER(N.WsMatch64)), self._cap, ctypes.byref(cnt),
+                      ctypes.byref(err))
+            parts.append(self._rows(cnt.value))
+            if st == _WS_ERR_OVERFLOW and cnt.value > 0:
+                continue
+            if st != 0:
+                _raise(st, err)
+            return np.concatenate(parts)
+
+    def feed_ptr_array(self, ptr: int, n: int) -> np.ndarray:
+        lib, h = N.lib(), self._h
+        first = [True]
+
+        def call(out, cap, cnt, err):
+            if first[0]:
+                first[0] = False
+                return lib.ws_stream_feed(h, ptr, n, out, cap, cnt, err)
+            return lib.ws_stream_feed(h, None, 0, out, cap, cnt, err)
+        return self._collect(call)
+
+    def end_array(self) -> np.ndarray:
+        lib, h = N.lib(), self._h
+        return self._collect(lambda out, cap, cnt, err: lib.ws_stream_end(h, out, cap, cnt, err))
+
+    @staticmethod
+    def _to_matches(a: np.ndarray) -> list[Match]:
+        return [Match(int(p), int(s), int(e)) for p, s, e in a.tolist()]
 
     def feed_ptr(self, ptr: int, n: int) -> list[Match]:
-        cnt = ctypes.c_uint64()
-        _call(N.lib().ws_stream_feed, self._h, ptr, n, self._out, self._cap, ctypes.byref(cnt))
-        return self._collect(cnt.value)
+        return self._to_matches(self.feed_ptr_array(ptr, n))
 
     def feed(self, data) -> list[Match]:
         ptr, n, keep = _buffer(data)
@@ -685,11 +888,15 @@ class Stream:
         return r
 
     def end(self) -> list[Match]:
-        cnt = ctypes.c_uint64()
-        _call(N.lib().ws_stream_end, self._h, self._out, self._cap, ctypes.byref(cnt))
-        return self._collect(cnt.value)
+        return self._to_matches(self.end_array())
 
     def close(self):
         if getattr(self, "_h", None):
             N.lib().ws_stream_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -61,7 +61,7 @@ class WsConfig(ctypes.Structure):
                 ("dfa_max_states", ctypes.c_uint32), ("walk_chunk", ctypes.c_uint32),
                 ("proposer", ctypes.c_uint32), ("proposer_train_bytes", ctypes.c_uint64),
                 ("proposer_seed", ctypes.c_uint64), ("flags", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 7)]
+                ("batch_mib", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
 
 class WsMatcherInfo(ctypes.Structure):

@@ -14,38 +14,12 @@
 #include <chrono>
 #include <cstring>
 
-#include "ws_internal.h"
-#include "ws_dfa.h"
+#include "ws_matcher.h"
 #include "ws_proposer.h"
 
 using namespace ws;
 
-struct ws_ctx {
-  int device = 0;
-  int sm_count = 0;
-};
-
-namespace {
-
-// Per-call scratch: a stream, the device input copy, the output and counters.
-struct Scratch {
-  cudaStream_t stream = nullptr;
-  DeviceBuffer input;        // padded device copy of the input
-  DeviceBuffer out;          // ws_match[capacity]
-  DeviceBuffer counters;     // unsigned long long[8]
-  DeviceBuffer rx;           // regex scratch (ws_dfa.cu manages the layout)
-  DeviceBuffer lit;          // literal survivor list
-  void* pinned = nullptr;    // pinned staging for pageable host input
-  size_t pinned_bytes = 0;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaEvent_t busy = nullptr;  // recorded after the last use
-  ~Scratch() {
-    if (busy) cudaEventDestroy(busy);
-    if (stream) cudaStreamDestroy(stream);
-    if (pinned) cudaFreeHost(pinned);
-    for (auto e : ev) if (e) cudaEventDestroy(e);
-  }
-};
+namespace ws {
 
 void ensure(DeviceBuffer& b, size_t need) {
   if (b.bytes >= need) return;
@@ -62,27 +36,6 @@ void fill_err(ws_error_info* err, const Failure& f) {
   std::snprintf(err->message, sizeof(err->message), "%s", f.message.c_str());
 }
 
-template <class F>
-ws_status guarded(ws_error_info* err, F&& fn) {
-  if (err) std::memset(err, 0, sizeof(*err));
-  try {
-    fn();
-    return WS_OK;
-  } catch (const WsError& e) {
-    fill_err(err, e.f);
-    return e.f.status;
-  } catch (const CompileError& e) {
-    if (err) std::snprintf(err->message, sizeof(err->message), "%s", e.what());
-    return WS_ERR_COMPILE;
-  } catch (const std::bad_alloc&) {
-    if (err) std::snprintf(err->message, sizeof(err->message), "host allocation failed");
-    return WS_ERR_DEVICE;
-  } catch (const std::exception& e) {
-    if (err) std::snprintf(err->message, sizeof(err->message), "%s", e.what());
-    return WS_ERR_DEVICE;
-  }
-}
-
 bool is_pinned(const void* p) {
   cudaPointerAttributes at;
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
@@ -90,121 +43,6 @@ bool is_pinned(const void* p) {
     return false;
   }
   return at.type == cudaMemoryTypeHost;
-}
-
-}  // namespace
-
-struct ws_matcher {
-  ws_ctx* ctx = nullptr;
-  ws_config cfg;
-  LiteralPlan lit;
-  RegexPlan rx;
-  uint32_t n_patterns = 0;
-  std::mutex pool_mu;
-  std::vector<std::unique_ptr<Scratch>> pool;
-  std::mutex info_mu;
-  ws_matcher_info info;
-  bool profile = false;          // record phase events (single caller at a time)
-  cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t rx_events[8] = {};
-  ~ws_matcher() {
-    for (auto e : pev) if (e) cudaEventDestroy(e);
-    for (auto e : rx_events) if (e) cudaEventDestroy(e);
-  }
-
-  std::unique_ptr<Scratch> take() {
-    {
-      std::lock_guard<std::mutex> g(pool_mu);
-      if (!pool.empty()) {
-        auto s = std::move(pool.back());
-        pool.pop_back();
-        return s;
-      }
-    }
-    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
-    auto s = std::make_unique<Scratch>();
-    check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    for (auto& e : s->ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
-    check_cuda(cudaEventCreateWithFlags(&s->busy, cudaEventDisableTiming), "cudaEventCreate");
-    s->counters.alloc(64);
-    return s;
-  }
-  void give(std::unique_ptr<Scratch> s) {
-    std::lock_guard<std::mutex> g(pool_mu);
-    pool.push_back(std::move(s));
-  }
-};
-
-namespace {
-
-// Copies host input into the scratch's device buffer (zero padding after it).
-void stage_input(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len) {
-  ensure(s.input, len + 64);
-  if (len == 0) return;
-  if (is_pinned(data)) {
-    check_cuda(cudaMemcpyAsync(s.input.ptr, data, len, cudaMemcpyHostToDevice, s.stream), "H2D input");
-    return;
-  }
-  // pageable: double-buffered staging through pinned memory
-  const size_t piece = 8u << 20;
-  if (s.pinned_bytes < 2 * piece) {
-    if (s.pinned) cudaFreeHost(s.pinned);
-    s.pinned = nullptr;
-    check_cuda(cudaHostAlloc(&s.pinned, 2 * piece, cudaHostAllocDefault), "cudaHostAlloc");
-    s.pinned_bytes = 2 * piece;
-  }
-  uint8_t* pin = static_cast<uint8_t*>(s.pinned);
-  cudaEvent_t done[2] = {s.ev[2], s.ev[3]};
-  bool used[2] = {false, false};
-  for (uint64_t off = 0, k = 0; off < len; off += piece, ++k) {
-    int slot = (int)(k & 1);
-    if (used[slot]) check_cuda(cudaEventSynchronize(done[slot]), "staging sync");
-    size_t n = (size_t)std::min<uint64_t>(piece, len - off);
-    std::memcpy(pin + slot * piece, data + off, n);
-    check_cuda(cudaMemcpyAsync(static_cast<uint8_t*>(s.input.ptr) + off, pin + slot * piece, n,
-                               cudaMemcpyHostToDevice, s.stream), "H2D input");
-    check_cuda(cudaEventRecord(done[slot], s.stream), "event record");
-    used[slot] = true;
-  }
-  (void)m;
-}
-
-uint64_t device_capacity(const ws_matcher* m) { return std::max<uint64_t>(m->cfg.max_matches, 1); }
-
-// Enqueues the full scan of a device-resident input on `st`; nothing is read
-// back.  With profiling enabled, phase events are recorded on `st` as well.
-void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
-                  ws_match* d_out, uint64_t cap, unsigned long long* d_counter) {
-  const bool prof = m->profile;
-  uint32_t launches = 0;
-  check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
-  if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
-  if (m->lit.n_literals) {
-    uint64_t scap = literal_survivor_cap(len);
-    ensure(s.lit, literal_scratch_bytes(scap));
-    LiteralLaunch ll{d_data, len, d_out, cap, d_counter, s.lit.ptr, scap};
-    launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
-    launches += 2;
-  }
-  if (prof) check_cuda(cudaEventRecord(m->pev[1], st), "event");
-  if (m->rx.n_regex) {
-    RegexLaunch rl{d_data, len, d_out, cap, d_counter, m->cfg.regex_mode};
-    launches += run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
-  }
-  if (prof) check_cuda(cudaEventRecord(m->pev[2], st), "event");
-  check_cuda(cudaEventRecord(s.busy, st), "event");
-  std::lock_guard<std::mutex> g(m->info_mu);
-  m->info.last_launches = launches;
-  m->info.last_chunks = m->rx.last_chunks;
-}
-
-// Raises MatchBufferOverflow when a regex scratch buffer overflowed.
-void check_regex_overflow(ws_matcher* m, Scratch& s) {
-  if (!m->rx.n_regex || !s.rx.ptr) return;
-  unsigned long long flag = 0;
-  check_cuda(cudaMemcpy(&flag, static_cast<uint8_t*>(s.rx.ptr) + kRegexErrorFlagOffset, 8, cudaMemcpyDeviceToHost),
-             "D2H flag");
-  if (flag) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow (raise max_matches)", 0, 0, m->cfg.max_matches);
 }
 
 void sort_matches(ws_match* p, uint64_t n) {
@@ -215,7 +53,125 @@ void sort_matches(ws_match* p, uint64_t n) {
   });
 }
 
-}  // namespace
+uint8_t* staging(Scratch& s, size_t piece) {
+  if (s.pinned_bytes < 2 * piece) {
+    for (int k = 0; k < 2; ++k)
+      if (s.pin_busy[k]) check_cuda(cudaEventSynchronize(s.ev[2 + k]), "staging sync");
+    s.pin_busy[0] = s.pin_busy[1] = false;
+    if (s.pinned) cudaFreeHost(s.pinned);
+    s.pinned = nullptr;
+    s.pinned_bytes = 0;
+    check_cuda(cudaHostAlloc(&s.pinned, 2 * piece, cudaHostAllocDefault), "cudaHostAlloc");
+    s.pinned_bytes = 2 * piece;
+  }
+  return static_cast<uint8_t*>(s.pinned);
+}
+
+uint8_t* staging_slot(Scratch& s, int k, size_t piece) {
+  uint8_t* pin = staging(s, piece);
+  if (s.pin_busy[k]) {
+    check_cuda(cudaEventSynchronize(s.ev[2 + k]), "staging sync");
+    s.pin_busy[k] = false;
+  }
+  return pin + (size_t)k * (s.pinned_bytes / 2);
+}
+
+void staging_issued(Scratch& s, int k) {
+  check_cuda(cudaEventRecord(s.ev[2 + k], s.stream), "event record");
+  s.pin_busy[k] = true;
+}
+
+void stage_copy(Scratch& s, uint8_t* d_dst, const uint8_t* data, uint64_t len) {
+  if (len == 0) return;
+  if (is_pinned(data)) {
+    check_cuda(cudaMemcpyAsync(d_dst, data, len, cudaMemcpyHostToDevice, s.stream), "H2D input");
+    return;
+  }
+  // pageable: double-buffered staging through pinned memory
+  const size_t piece = 8u << 20;
+  for (uint64_t off = 0, k = 0; off < len; off += piece, ++k) {
+    const int slot = (int)(k & 1);
+    uint8_t* pin = staging_slot(s, slot, piece);
+    size_t n = (size_t)std::min<uint64_t>(piece, len - off);
+    std::memcpy(pin, data + off, n);
+    check_cuda(cudaMemcpyAsync(d_dst + off, pin, n, cudaMemcpyHostToDevice, s.stream), "H2D input");
+    staging_issued(s, slot);
+  }
+}
+
+void stage_input(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len) {
+  (void)m;
+  ensure(s.input, len + 64);
+  stage_copy(s, s.input.as<uint8_t>(), data, len);
+}
+
+uint64_t device_capacity(const ws_matcher* m) { return std::max<uint64_t>(m->cfg.max_matches, 1); }
+
+void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
+                  ws_match* d_out, uint64_t cap, unsigned long long* d_counter, const ScanExtras& x) {
+  const bool prof = m->profile;
+  uint32_t launches = 0;
+  check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
+  if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
+  if (m->lit.n_literals && x.literals) {
+    uint64_t scap = literal_survivor_cap(len);
+    ensure(s.lit, literal_scratch_bytes(scap));
+    LiteralLaunch ll{d_data, len, d_out, cap, d_counter, s.lit.ptr, scap};
+    ll.item_end = x.item_end;
+    ll.n_items = x.n_items;
+    ll.min_end = x.lit_min_end;
+    launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
+    launches += 2;
+  }
+  if (prof) check_cuda(cudaEventRecord(m->pev[1], st), "event");
+  if (m->rx.n_regex) {
+    RegexLaunch rl{d_data, len, d_out, cap, d_counter, m->cfg.regex_mode};
+    rl.item_end = x.item_end;
+    rl.n_items = x.n_items;
+    rl.cursor = x.cursor;
+    rl.base = x.base;
+    rl.frontier = x.frontier;
+    launches += run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
+  }
+  if (prof) check_cuda(cudaEventRecord(m->pev[2], st), "event");
+  check_cuda(cudaEventRecord(s.busy, st), "event");
+  std::lock_guard<std::mutex> g(m->info_mu);
+  m->info.last_launches = launches;
+  m->info.last_chunks = m->rx.last_chunks;
+}
+
+void check_regex_overflow(ws_matcher* m, Scratch& s) {
+  if (!m->rx.n_regex || !s.rx.ptr) return;
+  unsigned long long flag = 0;
+  check_cuda(cudaMemcpy(&flag, static_cast<uint8_t*>(s.rx.ptr) + kRegexErrorFlagOffset, 8, cudaMemcpyDeviceToHost),
+             "D2H flag");
+  if (flag) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow (raise max_matches)", 0, 0, m->cfg.max_matches);
+}
+
+}  // namespace ws
+
+std::unique_ptr<Scratch> ws_matcher::take() {
+  {
+    std::lock_guard<std::mutex> g(pool_mu);
+    if (!pool.empty()) {
+      auto s = std::move(pool.back());
+      pool.pop_back();
+      return s;
+    }
+  }
+  check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+  auto s = std::make_unique<Scratch>();
+  check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto& e : s->ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+  check_cuda(cudaEventCreateWithFlags(&s->busy, cudaEventDisableTiming), "cudaEventCreate");
+  s->counters.alloc(64);
+  return s;
+}
+
+void ws_matcher::give(std::unique_ptr<Scratch> s) {
+  std::lock_guard<std::mutex> g(pool_mu);
+  pool.push_back(std::move(s));
+}
 
 extern "C" {
 
@@ -270,6 +226,10 @@ ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_co
     m->ctx = ctx;
     if (cfg) m->cfg = *cfg; else ws_config_default(&m->cfg);
     m->n_patterns = t->n_patterns;
+    m->is_regex.assign(t->n_patterns, 0);
+    for (uint32_t r = 0; r < t->n_regex; ++r)
+      if (t->regex_pattern_ids[r] < t->n_patterns) m->is_regex[t->regex_pattern_ids[r]] = 1;
+    for (uint32_t i = 0; i < t->n_literals; ++i) m->max_literal_len = std::max(m->max_literal_len, t->offsets[2 * i + 1]);
     std::memset(&m->info, 0, sizeof(m->info));
     plan_literals(*t, m->lit);
     plan_regex(*t, m->cfg, ctx->sm_count, m->rx);

@@ -1,0 +1,224 @@
+// Batch scan of many items in one launch sequence.
+//
+// Replaces scan_batch / scan_batch_gpu / scan_batch_auto
+// (core/src/batch.rs:252-363).  The reference coalesces up to 4,096 items or
+// 256 MiB into one buffer (coalesce, batch.rs:65-98), runs a full GpuMatcher
+// round trip per batch, and afterwards drops matches that cross item
+// boundaries (decoalesce, batch.rs:106-167).  Here the items are gathered
+// into one device buffer per launch sequence (1 GiB by default) together with
+// a table of item end offsets, and the kernels are item-aware:
+//   - literal verify rejects an occurrence that runs past its item's end;
+//   - the regex reverse walk stops at the start of the item holding the match
+//     end, the leftmost-first end walk and the plain walk stop at the end of
+//     the item holding the start, so K holds only in-item candidates and each
+//     item gets its own find_iter chain (the chain cursor never crosses an
+//     item because every match ends inside its item);
+// which makes the result the per-item scan of scan_batch_cpu
+// (batch.rs:170-195): L + R inside each item, no cross-item matches.  A tag
+// kernel converts coalesced offsets to (source_id, item-relative offsets);
+// the host sorts by (source_id, start, pattern_id, end) as batch.rs:157-163.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <numeric>
+
+#include "ws_matcher.h"
+
+using namespace ws;
+
+namespace {
+
+// Every match of a coalesced launch, tagged with its item's id and shifted to
+// item-relative offsets.
+__global__ void tag_kernel(const ws_match* in, const unsigned long long* count, uint64_t cap, const uint32_t* ends,
+                           const uint64_t* ids, uint32_t n_items, ws_tagged_match* out) {
+  unsigned long long n = *count;
+  if (n > cap) n = cap;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+    ws_match mm = in[k];
+    uint32_t lo = 0, hi = n_items;  // first item whose end is above the start
+    while (lo < hi) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (ends[mid] > mm.start) hi = mid; else lo = mid + 1;
+    }
+    const uint32_t base = lo ? ends[lo - 1] : 0;
+    ws_tagged_match t;
+    t.source_id = ids[lo];
+    t.pattern_id = mm.pattern_id;
+    t.start = mm.start - base;
+    t.end = mm.end - base;
+    t.reserved = 0;
+    out[k] = t;
+  }
+}
+
+// Gathers host byte runs into one contiguous device range through two pinned
+// staging pieces (the host copy of one piece overlaps the DMA of the other);
+// large pinned runs are copied directly.
+class Gather {
+ public:
+  Gather(Scratch& s, uint8_t* d_dst) : s_(s), d_dst_(d_dst) {}
+
+  void push(const uint8_t* src, uint64_t n) {
+    if (n >= kDirect && is_pinned(src)) {
+      flush();
+      check_cuda(cudaMemcpyAsync(d_dst_ + off_, src, n, cudaMemcpyHostToDevice, s_.stream), "H2D item");
+      off_ += n;
+      return;
+    }
+    while (n) {
+      if (!pin_) {
+        pin_ = staging_slot(s_, slot_, kPiece);
+        piece_off_ = off_;
+      }
+      size_t k = (size_t)std::min<uint64_t>(n, kPiece - fill_);
+      std::memcpy(pin_ + fill_, src, k);
+      fill_ += k;
+      off_ += k;
+      src += k;
+      n -= k;
+      if (fill_ == kPiece) flush();
+    }
+  }
+
+  void flush() {
+    if (!pin_) return;
+    if (fill_) {
+      check_cuda(cudaMemcpyAsync(d_dst_ + piece_off_, pin_, fill_, cudaMemcpyHostToDevice, s_.stream),
+                 "H2D batch piece");
+      staging_issued(s_, slot_);
+      slot_ ^= 1;
+    }
+    fill_ = 0;
+    pin_ = nullptr;
+  }
+
+ private:
+  static constexpr size_t kPiece = 8u << 20;
+  static constexpr uint64_t kDirect = 1u << 20;
+  Scratch& s_;
+  uint8_t* d_dst_;
+  uint8_t* pin_ = nullptr;  // current slot being filled
+  int slot_ = 0;
+  size_t fill_ = 0;
+  uint64_t off_ = 0, piece_off_ = 0;
+};
+
+}  // namespace
+
+extern "C" ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t n_items, ws_tagged_match* out,
+                                   uint64_t cap, uint64_t* n_out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !n_out || (n_items && !items) || (cap && !out)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *n_out = 0;
+    // batch.rs:65-98: every item must be addressable with 32-bit offsets
+    std::vector<uint64_t> order;
+    order.reserve(n_items);
+    for (uint64_t i = 0; i < n_items; ++i) {
+      if (items[i].len > 0xFFFFFFFFull)
+        raise(WS_ERR_INPUT_TOO_LARGE, "batch item is too large for 32-bit match offsets", i, items[i].len,
+              0xFFFFFFFFull);
+      if (items[i].len && !items[i].data) raise(WS_ERR_INVALID_ARGUMENT, "batch item with null data", i);
+      if (items[i].len) order.push_back(i);  // an empty item has no matches
+    }
+    if (order.empty()) return;
+    // items in source-id order (stable), packed greedily into launch sequences
+    std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return items[a].id < items[b].id; });
+    const uint64_t budget = std::min<uint64_t>((uint64_t)(m->cfg.batch_mib ? m->cfg.batch_mib : 1024) << 20,
+                                               0xFFFFFFFFull);
+    std::vector<std::pair<size_t, size_t>> groups;  // [first, last) in order
+    {
+      size_t a = 0;
+      uint64_t bytes = 0;
+      for (size_t k = 0; k < order.size(); ++k) {
+        uint64_t len = items[order[k]].len;
+        if (k > a && bytes + len > budget) {
+          groups.emplace_back(a, k);
+          a = k;
+          bytes = 0;
+        }
+        bytes += len;
+      }
+      groups.emplace_back(a, order.size());
+    }
+
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    ScratchLease s(m);
+    check_cuda(cudaStreamWaitEvent(s->stream, s->busy, 0), "wait");
+    const uint64_t dcap = device_capacity(m);
+    ensure(s->out, dcap * sizeof(ws_match));
+    auto* d_counter = s->counters.as<unsigned long long>();
+    uint64_t total = 0;
+    std::vector<uint32_t> ends;
+    std::vector<uint64_t> ids;
+    for (const auto& gr : groups) {
+      const size_t ni = gr.second - gr.first;
+      ends.resize(ni);
+      ids.resize(ni);
+      uint64_t bytes = 0;
+      for (size_t k = 0; k < ni; ++k) {
+        const ws_item& it = items[order[gr.first + k]];
+        bytes += it.len;
+        ends[k] = (uint32_t)bytes;
+        ids[k] = it.id;
+      }
+      // device layout: [input bytes + pad][item ends u32][item ids u64][tagged matches]
+      ensure(s->input, bytes + 64);
+      const size_t ends_off = 0, ids_off = (ni * 4 + 255) & ~(size_t)255,
+                   tag_off = ids_off + ((ni * 8 + 255) & ~(size_t)255);
+      ensure(s->aux, tag_off + dcap * sizeof(ws_tagged_match));
+      uint8_t* aux = s->aux.as<uint8_t>();
+      {
+        // items adjacent in host memory (slices of one arena) move as one run
+        Gather g(*s, s->input.as<uint8_t>());
+        const uint8_t* run = nullptr;
+        uint64_t run_len = 0;
+        for (size_t k = 0; k < ni; ++k) {
+          const ws_item& it = items[order[gr.first + k]];
+          if (run && it.data == run + run_len) {
+            run_len += it.len;
+            continue;
+          }
+          if (run) g.push(run, run_len);
+          run = it.data;
+          run_len = it.len;
+        }
+        if (run) g.push(run, run_len);
+        g.flush();
+        stage_copy(*s, aux + ends_off, reinterpret_cast<const uint8_t*>(ends.data()), ni * 4);
+        stage_copy(*s, aux + ids_off, reinterpret_cast<const uint8_t*>(ids.data()), ni * 8);
+      }
+      check_cuda(cudaMemsetAsync(s->input.as<uint8_t>() + bytes, 0, 64, s->stream), "memset pad");
+      ScanExtras x;
+      x.item_end = reinterpret_cast<const uint32_t*>(aux + ends_off);
+      x.n_items = (uint32_t)ni;
+      enqueue_scan(m, *s, s->stream, s->input.as<uint8_t>(), bytes, s->out.as<ws_match>(), dcap, d_counter, x);
+      auto* d_tag = reinterpret_cast<ws_tagged_match*>(aux + tag_off);
+      tag_kernel<<<m->ctx->sm_count * 4, 256, 0, s->stream>>>(s->out.as<ws_match>(), d_counter, dcap,
+                                                                reinterpret_cast<const uint32_t*>(aux + ends_off),
+                                                                reinterpret_cast<const uint64_t*>(aux + ids_off),
+                                                                (uint32_t)ni, d_tag);
+      check_cuda(cudaGetLastError(), "tag_kernel");
+      unsigned long long count = 0;
+      check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");
+      check_cuda(cudaStreamSynchronize(s->stream), "batch scan");
+      check_regex_overflow(m, *s);
+      if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one batch launch", 0, count, dcap);
+      if (total + count <= cap && count) {
+        check_cuda(cudaMemcpyAsync(out + total, d_tag, count * sizeof(ws_tagged_match), cudaMemcpyDeviceToHost,
+                                   s->stream), "D2H tagged matches");
+        check_cuda(cudaStreamSynchronize(s->stream), "D2H sync");
+      }
+      total += count;
+      check_cuda(cudaEventRecord(s->busy, s->stream), "event");
+    }
+    *n_out = total;
+    if (total > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, total, cap);
+    std::sort(out, out + total, [](const ws_tagged_match& a, const ws_tagged_match& b) {
+      if (a.source_id != b.source_id) return a.source_id < b.source_id;
+      if (a.start != b.start) return a.start < b.start;
+      if (a.pattern_id != b.pattern_id) return a.pattern_id < b.pattern_id;
+      return a.end < b.end;
+    });
+  });
+}

@@ -107,6 +107,10 @@ struct ScanPtrs {
   ws_match* out;
   uint64_t out_cap;
   unsigned long long* out_counter;
+  const uint32_t* item_end;     // batch item ends (n_items), else null
+  uint32_t n_items;
+  unsigned long long* cursor64;  // stream: per-regex find_iter position, else null
+  uint64_t base, frontier;
 };
 
 ScanPtrs make_ptrs(const RxLayout& L, void* base, const RegexLaunch& l) {
@@ -137,6 +141,11 @@ ScanPtrs make_ptrs(const RxLayout& L, void* base, const RegexLaunch& l) {
   p.out = l.out;
   p.out_cap = l.cap;
   p.out_counter = l.counter;
+  p.item_end = l.item_end;
+  p.n_items = l.n_items;
+  p.cursor64 = l.cursor;
+  p.base = l.base;
+  p.frontier = l.frontier;
   return p;
 }
 
@@ -288,7 +297,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
   for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < p.len; s += stride) {
     uint32_t cold_row = 0;
     uint32_t st = state_of(gd.start_anchored, first, rows, lane4, &cold_row);
-    for (uint64_t e = s; e < p.len; ++e) {
+    const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, (uint32_t)s)) : p.len;
+    for (uint64_t e = s; e < stop; ++e) {
       uint32_t b = __ldg(p.data + e);
       uint32_t w = WS_STEP_FAST(img, st, b);
       if ((int32_t)w >= 0) {
@@ -470,7 +480,8 @@ __global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs 
     const uint32_t* rmp = t.rmptr + gd.rmptr_off;
     const uint32_t C = gd.n_classes;
     uint32_t st = gd.rev_start;
-    for (uint64_t pos = ev.e; pos > 0; --pos) {
+    const uint64_t lo = p.n_items ? item_start_of(p.item_end, p.n_items, ev.e - 1) : 0;
+    for (uint64_t pos = ev.e; pos > lo; --pos) {
       uint32_t w = __ldg(tab + st * C + __ldg(cm + __ldg(p.data + pos - 1)));
       if (w & F_DEAD) break;
       st = w & F_MASK;
@@ -577,7 +588,8 @@ __global__ void k_lf_kernel(DevTables t, ScanPtrs p, uint32_t n_regex) {
     const uint32_t* tab = t.lf + info.x;
     uint32_t st = info.y;
     int64_t last = -1;
-    for (uint64_t pos = s; pos < p.len; ++pos) {
+    const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, s)) : p.len;
+    for (uint64_t pos = s; pos < stop; ++pos) {
       uint32_t w = __ldg(tab + st * info.w + __ldg(cm + __ldg(p.data + pos)));
       if (w & F_DEAD) break;
       st = w & F_MASK;
@@ -594,16 +606,21 @@ __global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
   if (r >= t.n_regex) return;
   const uint32_t a = p.offs[r], b = p.offs[r + 1];
   const uint32_t pid = t.pid[r];
-  uint64_t last_end = 0;
+  // stream scans: resume at the regex's cursor, decide only starts before the
+  // frontier (both in stream offsets; the buffer starts at p.base <= cursor)
+  uint64_t last_end = p.cursor64 ? p.cursor64[r] - p.base : 0;
+  const uint64_t limit = p.cursor64 ? p.frontier - p.base : ~0ull;
   for (uint32_t j = a; j < b; ++j) {
     uint32_t e = p.lfend[j];
     if (e == 0xFFFFFFFFu) continue;
     uint32_t s = p.starts[j];
     if (s < last_end) continue;
+    if (s >= limit) break;
     unsigned long long idx = atomicAdd(p.out_counter, 1ull);
     if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, e};
     last_end = e;
   }
+  if (p.cursor64) p.cursor64[r] = max(p.base + last_end, p.frontier);
 }
 
 // Copies K candidates into a ws_match buffer (diagnostics).

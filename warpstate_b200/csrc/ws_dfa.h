@@ -81,6 +81,17 @@ struct RegexLaunch {
   uint64_t cap;
   unsigned long long* counter;
   uint32_t mode;
+  // Batch scans: ascending exclusive item ends in `data`; every match lies
+  // inside one item and each item has its own find_iter chain.
+  const uint32_t* item_end = nullptr;
+  uint32_t n_items = 0;
+  // Stream scans: `data` holds stream bytes [base, base + len).  cursor[r]
+  // (device, one u64 per regex) is regex r's find_iter position: matches
+  // starting before it were decided by earlier calls.  Only matches starting
+  // before `frontier` are decided now; cursor[r] advances to
+  // max(last match end, frontier).
+  unsigned long long* cursor = nullptr;
+  uint64_t base = 0, frontier = 0;
 };
 
 void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, RegexPlan& plan);

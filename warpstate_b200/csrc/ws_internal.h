@@ -111,7 +111,33 @@ struct LiteralLaunch {
   unsigned long long* counter;  // device; incremented per match (true count)
   void* scratch;                // literal_scratch_bytes(survivor_cap) bytes
   uint64_t survivor_cap;
+  // Batch scans: ascending exclusive end offsets of the items coalesced in
+  // `data` (n_items of them); a match must end inside the item it starts in.
+  const uint32_t* item_end = nullptr;
+  uint32_t n_items = 0;
+  // Stream scans: only matches ending after this offset are new.
+  uint64_t min_end = 0;
 };
+
+// Exclusive end of the item that contains offset `s` (the first end above s).
+__host__ __device__ inline uint32_t item_end_of(const uint32_t* ends, uint32_t n, uint32_t s) {
+  uint32_t lo = 0, hi = n;  // first index with ends[idx] > s
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (ends[mid] > s) hi = mid; else lo = mid + 1;
+  }
+  return lo < n ? ends[lo] : 0xFFFFFFFFu;
+}
+
+// Start of the item that contains offset `s` (the last end at or below s).
+__host__ __device__ inline uint32_t item_start_of(const uint32_t* ends, uint32_t n, uint32_t s) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (ends[mid] > s) hi = mid; else lo = mid + 1;
+  }
+  return lo > 0 ? ends[lo - 1] : 0;
+}
 size_t literal_scratch_bytes(uint64_t survivor_cap);
 inline uint64_t literal_survivor_cap(uint64_t len) { return len / 64 + 4096; }
 void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& a, cudaStream_t st, int sm_count);

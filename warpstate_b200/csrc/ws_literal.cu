@@ -61,6 +61,9 @@ struct LitArgs {
   uint32_t* survivor_hi;     // unused for inputs < 4 GiB
   unsigned long long* survivor_count;
   uint64_t survivor_cap;
+  const uint32_t* item_end;  // batch: ascending item ends (n_items), else null
+  uint32_t n_items;
+  uint64_t min_end;          // stream: matches ending at or before it were reported
 };
 
 __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint32_t bits) {
@@ -102,6 +105,8 @@ __device__ void verify_position(const LitArgs& a, uint64_t s) {
         if (__ldg(lit + k) != __ldg(a.data + s + k)) { eq = false; break; }
       }
       if (!eq) continue;
+      if (s + info.y <= a.min_end) continue;
+      if (a.n_items && s + info.y > item_end_of(a.item_end, a.n_items, (uint32_t)s)) continue;  // crosses items
       unsigned long long idx = atomicAdd(a.counter, 1ull);
       if (idx < a.cap) {
         ws_match mm;
@@ -328,6 +333,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.survivors = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(l.scratch) + 64);
   a.survivor_hi = nullptr;
   a.survivor_cap = l.survivor_cap;
+  a.item_end = l.item_end;
+  a.n_items = l.n_items;
+  a.min_end = l.min_end;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   size_t smem = literal_smem_bytes(plan);
   check_cuda(cudaFuncSetAttribute(literal_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),

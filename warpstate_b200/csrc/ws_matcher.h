@@ -1,0 +1,139 @@
+// Matcher object of the C ABI and the helpers that the single-buffer scan
+// (ws_api.cu), the batch scan (ws_batch.cu) and the stream scan
+// (ws_stream.cu) share: per-call scratch from a pool, input staging, the
+// enqueue of the literal and regex pipelines, error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "ws_internal.h"
+#include "ws_dfa.h"
+
+struct ws_ctx {
+  int device = 0;
+  int sm_count = 0;
+};
+
+namespace ws {
+
+// Per-call scratch: a stream, the device input copy, the output and counters.
+struct Scratch {
+  cudaStream_t stream = nullptr;
+  DeviceBuffer input;        // padded device copy of the input
+  DeviceBuffer out;          // ws_match[capacity]
+  DeviceBuffer counters;     // unsigned long long[8]
+  DeviceBuffer rx;           // regex scratch (ws_dfa.cu manages the layout)
+  DeviceBuffer lit;          // literal survivor list
+  DeviceBuffer aux;          // batch item ends / tagged output
+  void* pinned = nullptr;    // pinned staging for pageable host input
+  size_t pinned_bytes = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // [2], [3]: staging slots drained
+  bool pin_busy[2] = {false, false};                         // a DMA may still read the slot
+  cudaEvent_t busy = nullptr;  // recorded after the last use
+  ~Scratch() {
+    if (busy) cudaEventDestroy(busy);
+    if (stream) cudaStreamDestroy(stream);
+    if (pinned) cudaFreeHost(pinned);
+    for (auto e : ev) if (e) cudaEventDestroy(e);
+  }
+};
+
+// Extra bounds of a scan over coalesced batch items or a stream window.
+struct ScanExtras {
+  const uint32_t* item_end = nullptr;  // batch: ascending item ends (device)
+  uint32_t n_items = 0;
+  bool literals = true;                // run the literal pipeline
+  uint64_t lit_min_end = 0;            // stream: literal matches ending later are new
+  unsigned long long* cursor = nullptr;  // stream: per-regex find_iter positions (device)
+  uint64_t base = 0, frontier = 0;     // stream: window offset and decision frontier
+};
+
+// Pinned staging of `piece` bytes per slot (two slots), allocated on demand.
+uint8_t* staging(Scratch& s, size_t piece);
+// Host pointer of staging slot k, after any DMA still reading it has finished.
+uint8_t* staging_slot(Scratch& s, int k, size_t piece);
+// Marks slot k as read by the DMA just enqueued on the scratch's stream.
+void staging_issued(Scratch& s, int k);
+void ensure(DeviceBuffer& b, size_t need);
+void fill_err(ws_error_info* err, const Failure& f);
+bool is_pinned(const void* p);
+void sort_matches(ws_match* p, uint64_t n);
+
+}  // namespace ws
+
+struct ws_matcher {
+  ws_ctx* ctx = nullptr;
+  ws_config cfg;
+  ws::LiteralPlan lit;
+  ws::RegexPlan rx;
+  uint32_t n_patterns = 0;
+  uint32_t max_literal_len = 0;
+  std::vector<uint8_t> is_regex;  // per pattern id
+  std::mutex pool_mu;
+  std::vector<std::unique_ptr<ws::Scratch>> pool;
+  std::mutex info_mu;
+  ws_matcher_info info;
+  bool profile = false;          // record phase events (single caller at a time)
+  cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t rx_events[8] = {};
+  ~ws_matcher() {
+    for (auto e : pev) if (e) cudaEventDestroy(e);
+    for (auto e : rx_events) if (e) cudaEventDestroy(e);
+  }
+
+  std::unique_ptr<ws::Scratch> take();
+  void give(std::unique_ptr<ws::Scratch> s);
+};
+
+namespace ws {
+
+// Returns a pooled scratch to its matcher when the scope ends.
+struct ScratchLease {
+  ws_matcher* m;
+  std::unique_ptr<Scratch> s;
+  explicit ScratchLease(ws_matcher* mm) : m(mm), s(mm->take()) {}
+  ~ScratchLease() { if (s) m->give(std::move(s)); }
+  Scratch* operator->() { return s.get(); }
+  Scratch& operator*() { return *s; }
+};
+
+template <class F>
+ws_status guarded(ws_error_info* err, F&& fn) {
+  if (err) std::memset(err, 0, sizeof(*err));
+  try {
+    fn();
+    return WS_OK;
+  } catch (const WsError& e) {
+    fill_err(err, e.f);
+    return e.f.status;
+  } catch (const CompileError& e) {
+    if (err) std::snprintf(err->message, sizeof(err->message), "%s", e.what());
+    return WS_ERR_COMPILE;
+  } catch (const std::bad_alloc&) {
+    if (err) std::snprintf(err->message, sizeof(err->message), "host allocation failed");
+    return WS_ERR_DEVICE;
+  } catch (const std::exception& e) {
+    if (err) std::snprintf(err->message, sizeof(err->message), "%s", e.what());
+    return WS_ERR_DEVICE;
+  }
+}
+
+// Host -> device copy on the scratch's stream; pageable sources go through
+// double-buffered pinned staging.
+void stage_copy(Scratch& s, uint8_t* d_dst, const uint8_t* src, uint64_t len);
+// Copies host input into the scratch's device buffer (zero padding after it).
+void stage_input(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len);
+uint64_t device_capacity(const ws_matcher* m);
+// Enqueues the full scan of a device-resident input on `st`; nothing is read
+// back.  With profiling enabled, phase events are recorded on `st` as well.
+void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
+                  ws_match* d_out, uint64_t cap, unsigned long long* d_counter, const ScanExtras& x = ScanExtras());
+// Raises MatchBufferOverflow when a regex scratch buffer overflowed.
+void check_regex_overflow(ws_matcher* m, Scratch& s);
+
+}  // namespace ws

@@ -1,0 +1,215 @@
+// Stream scan: bytes fed in pieces, matches equal to one scan of the whole
+// stream, with 64-bit offsets.
+//
+// Replaces StreamPipeline::scan (core/src/pipeline.rs:87-153), which rescans
+// `overlap_window` bytes around every chunk boundary and then keeps, per
+// (pattern_id, start), the shortest end -- a heuristic that can report a
+// regex match the whole-input find_iter would not.  Here the stream carries
+// exact state between pieces:
+//   - a device window holding the stream bytes that later matches can still
+//     touch: the last max_literal_len - 1 bytes (a literal occurrence that
+//     ends in a later piece starts there) and every byte from the regex
+//     frontier on;
+//   - per regex, the find_iter cursor (u64, device-resident): matches
+//     starting before it are decided.
+// A regex start s is decided once s + max_len <= bytes seen (no match from s
+// can end later), so each piece decides every start below
+// frontier = seen - max_len + 1 and the chain resumes from the cursor next
+// time.  Literal occurrences are complete as soon as their last byte is seen;
+// each piece reports those that end inside it.  Regexes with unbounded
+// matches keep the whole undecided stream in the window (decided at the end).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ws_matcher.h"
+
+using namespace ws;
+
+struct ws_stream {
+  ws_matcher* m = nullptr;
+  std::unique_ptr<Scratch> s;
+  DeviceBuffer win[2];      // ping-pong windows
+  int cur = 0;
+  uint64_t win_base = 0;    // stream offset of the window's first byte
+  uint64_t win_len = 0;
+  uint64_t seen = 0;        // bytes fed so far
+  uint64_t frontier = 0;    // regex starts below it are decided
+  DeviceBuffer cursor;      // per-regex find_iter position (u64)
+  std::vector<ws_match64> pending;  // decided, not yet delivered
+  size_t delivered = 0;
+  std::vector<ws_match> host;       // per-step readback
+  bool failed = false;
+  bool ended = false;
+  ~ws_stream() {
+    if (s && m) m->give(std::move(s));
+  }
+};
+
+namespace {
+
+// New data per step: the window plus the step must stay below 4 GiB (32-bit
+// offsets inside a launch).
+constexpr uint64_t kStep = 1ull << 30;
+
+int64_t regex_max_len(const ws_matcher* m) { return m->rx.n_regex ? m->rx.max_len : 0; }
+
+// Runs one scan of the current window and appends the decided matches.
+void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t frontier) {
+  ws_matcher* m = st->m;
+  Scratch& s = *st->s;
+  const uint64_t dcap = device_capacity(m);
+  ensure(s.out, dcap * sizeof(ws_match));
+  auto* d_counter = s.counters.as<unsigned long long>();
+  ScanExtras x;
+  x.literals = literals;
+  x.lit_min_end = lit_min_end;
+  x.cursor = m->rx.n_regex ? st->cursor.as<unsigned long long>() : nullptr;
+  x.base = st->win_base;
+  x.frontier = frontier;
+  if (!literals && !m->rx.n_regex) return;
+  enqueue_scan(m, s, s.stream, st->win[st->cur].as<uint8_t>(), st->win_len, s.out.as<ws_match>(), dcap, d_counter, x);
+  unsigned long long count = 0;
+  check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
+  check_cuda(cudaStreamSynchronize(s.stream), "stream scan");
+  check_regex_overflow(m, s);
+  if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one stream piece", 0, count, dcap);
+  if (count) {
+    st->host.resize(count);
+    check_cuda(cudaMemcpy(st->host.data(), s.out.ptr, count * sizeof(ws_match), cudaMemcpyDeviceToHost), "D2H");
+    sort_matches(st->host.data(), count);
+    for (const ws_match& mm : st->host) {
+      ws_match64 o;
+      o.pattern_id = mm.pattern_id;
+      o.reserved = 0;
+      o.start = st->win_base + mm.start;
+      o.end = st->win_base + mm.end;
+      st->pending.push_back(o);
+    }
+  }
+}
+
+// Appends `len` bytes (len <= kStep) to the stream and decides what it can.
+void feed_step(ws_stream* st, const uint8_t* data, uint64_t len) {
+  ws_matcher* m = st->m;
+  Scratch& s = *st->s;
+  const uint64_t old_seen = st->seen, seen = old_seen + len;
+  const int64_t mx = regex_max_len(m);
+  // bytes [keep, old_seen) stay in the window
+  uint64_t keep = old_seen;
+  if (m->lit.n_literals && m->max_literal_len > 1) keep = std::min(keep, old_seen - std::min<uint64_t>(old_seen, m->max_literal_len - 1));
+  if (m->rx.n_regex) keep = std::min(keep, st->frontier);
+  keep = std::max(keep, st->win_base);
+  const uint64_t carry = old_seen - keep;
+  if (carry + len > 0xFFFFFFFFull - 64)
+    raise(WS_ERR_INPUT_TOO_LARGE, "stream window exceeds 32-bit offsets (a regex with unbounded matches keeps the "
+          "whole undecided stream)", 0, carry + len, 0xFFFFFFFFull - 64);
+  DeviceBuffer& dst = st->win[st->cur ^ 1];
+  ensure(dst, carry + len + 64);
+  if (carry)
+    check_cuda(cudaMemcpyAsync(dst.ptr, st->win[st->cur].as<uint8_t>() + (keep - st->win_base), carry,
+                               cudaMemcpyDeviceToDevice, s.stream), "D2D carry");
+  stage_copy(s, dst.as<uint8_t>() + carry, data, len);
+  check_cuda(cudaMemsetAsync(dst.as<uint8_t>() + carry + len, 0, 64, s.stream), "memset pad");
+  st->cur ^= 1;
+  st->win_base = keep;
+  st->win_len = carry + len;
+  st->seen = seen;
+  uint64_t frontier = st->frontier;
+  if (mx >= 0 && seen + 1 > (uint64_t)mx) frontier = std::max(frontier, seen + 1 - (uint64_t)mx);
+  frontier = std::min(frontier, seen);
+  scan_window(st, m->lit.n_literals != 0, old_seen - keep, frontier);
+  st->frontier = frontier;
+}
+
+// Copies up to `cap` undelivered matches out; overflow when some remain.
+void deliver(ws_stream* st, ws_match64* out, uint64_t cap, uint64_t* n_out) {
+  const uint64_t avail = st->pending.size() - st->delivered;
+  const uint64_t n = std::min<uint64_t>(avail, cap);
+  if (n) std::memcpy(out, st->pending.data() + st->delivered, n * sizeof(ws_match64));
+  st->delivered += n;
+  *n_out = n;
+  if (st->delivered == st->pending.size()) {
+    st->pending.clear();
+    st->delivered = 0;
+  }
+  if (n < avail)
+    raise(WS_ERR_OVERFLOW, "more stream matches than the output buffer holds; call again with no data to drain", 0,
+          avail, cap);
+}
+
+}  // namespace
+
+extern "C" {
+
+ws_status ws_stream_begin(ws_matcher* m, ws_stream** out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !out) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    auto st = std::make_unique<ws_stream>();
+    st->m = m;
+    st->s = m->take();
+    check_cuda(cudaStreamWaitEvent(st->s->stream, st->s->busy, 0), "wait");
+    if (m->rx.n_regex) {
+      st->cursor.alloc((size_t)m->rx.n_regex * 8);
+      check_cuda(cudaMemsetAsync(st->cursor.ptr, 0, (size_t)m->rx.n_regex * 8, st->s->stream), "memset cursor");
+    }
+    *out = st.release();
+  });
+}
+
+ws_status ws_stream_feed(ws_stream* st, const uint8_t* data, uint64_t len, ws_match64* out, uint64_t cap,
+                         uint64_t* n_out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!st || !n_out || (len && !data) || (cap && !out)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *n_out = 0;
+    if (st->failed) raise(WS_ERR_DEVICE, "stream is unusable after an earlier error");
+    if (st->ended && len) raise(WS_ERR_INVALID_ARGUMENT, "stream already ended");
+    check_cuda(cudaSetDevice(st->m->ctx->device), "cudaSetDevice");
+    try {
+      for (uint64_t off = 0; off < len;) {
+        uint64_t n = std::min<uint64_t>(kStep, len - off);
+        feed_step(st, data + off, n);
+        off += n;
+      }
+    } catch (...) {
+      st->failed = true;
+      throw;
+    }
+    deliver(st, out, cap, n_out);
+  });
+}
+
+ws_status ws_stream_end(ws_stream* st, ws_match64* out, uint64_t cap, uint64_t* n_out, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!st || !n_out || (cap && !out)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    *n_out = 0;
+    if (st->failed) raise(WS_ERR_DEVICE, "stream is unusable after an earlier error");
+    check_cuda(cudaSetDevice(st->m->ctx->device), "cudaSetDevice");
+    if (!st->ended) {
+      st->ended = true;
+      // every remaining regex start is decided now; literals were all reported
+      if (st->m->rx.n_regex && st->win_len && st->frontier < st->seen) {
+        try {
+          scan_window(st, false, 0, st->seen);
+        } catch (...) {
+          st->failed = true;
+          throw;
+        }
+      }
+      st->frontier = st->seen;
+      check_cuda(cudaEventRecord(st->s->busy, st->s->stream), "event");
+    }
+    deliver(st, out, cap, n_out);
+  });
+}
+
+void ws_stream_destroy(ws_stream* st) {
+  if (!st) return;
+  cudaSetDevice(st->m->ctx->device);
+  if (st->s) cudaStreamSynchronize(st->s->stream);
+  delete st;
+}
+
+}  // extern "C"
