@@ -6,9 +6,12 @@ python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--c
 A "step" is one scan of the configuration's whole input (already resident in
 HBM) by the full pattern set.  The default configuration is the 500-regex
 scan over 1 GiB of Markov text (learned-speculative DFA walk, with the plain
-thread-per-start kernel timed beside it).  Under torchrun every rank scans its
-own copy of the workload (weak scaling, no collective on the data path); the
-reported time is the max over ranks.
+thread-per-start kernel timed beside it).  Other configurations:
+literals_large (10,000 literals over 1 GiB), literals_small (100 literals over
+16 MiB), batch (200,000 lognormal items through the device batch scan) and dna
+(4 GiB of ACGT through the 64-bit windowed device scan).  Under torchrun every
+rank scans its own copy of the workload (weak scaling, no collective on the
+data path); the reported time is the max over ranks.
 
 --impl reference times the oracle port of the reference's CPU algorithm for
 the same configuration on the host cores (the reference is a Rust crate with
@@ -23,7 +26,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from pathlib import Path
 
@@ -42,6 +44,7 @@ CONFIGS = {
     "dna": "4 GiB ACGT with 1% N runs, 50,000 k-mers + 200 IUPAC regexes",
 }
 METRIC = "scan GB/s, learned-speculative vs plain DFA kernel, exact match sets, 1 B200"
+CAP = 8 << 20  # device match capacity of the benchmark
 
 
 def make_workload(name: str, size: int | None):
@@ -52,7 +55,7 @@ def make_workload(name: str, size: int | None):
     if name == "literals_small":
         return W.literals_small(size=size or 16 * W.MiB)
     if name == "batch":
-        return W.batch()
+        return W.batch(n_items=size or 200_000)
     if name == "dna":
         return W.dna(size=size or 4 * W.GiB)
     raise SystemExit(f"unknown config {name}")
@@ -67,7 +70,7 @@ def load_peaks():
 
 
 def read_traffic(kernel: str, config: str):
-    """Bytes per launch from the committed ncu summary, if one exists."""
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
     p = ROOT / "profiles" / f"{kernel}_{config}.txt"
     if not p.exists():
         return None
@@ -135,19 +138,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ----------------------------------------------------------- CPU baseline
 def cpu_baseline(wl, seconds: float = 12.0):
-    """Oracle port of the reference's CPU algorithm on a bounded sample."""
+    """Oracle port of the reference's CPU algorithm on a bounded sample of the
+    same workload, all host threads."""
     import oracle
     threads = oracle.hw_threads()
-    pats = wl.patterns
+    if wl.items is not None:
+        items = wl.items
+        probe = 2000
+        t = time.perf_counter()
+        oracle.batch_scan(wl.patterns, wl.data, items[:probe], threads=threads)
+        dt = max(time.perf_counter() - t, 1e-6)
+        k = int(min(len(items), max(probe, probe * seconds / dt)))
+        t = time.perf_counter()
+        oracle.batch_scan(wl.patterns, wl.data, items[:k], threads=threads)
+        dt = time.perf_counter() - t
+        nbytes = sum(ln for _, ln in items[:k])
+        return {"value": round(nbytes / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+                "sample": f"first {k} of {len(items)} items ({nbytes} bytes) scanned per item in {dt:.1f} s"}
     data = wl.data
     probe = min(len(data), 1 << 20)
     t = time.perf_counter()
-    oracle.scan_patterns(pats, data[:probe], threads)
+    oracle.scan_patterns(wl.patterns, data[:probe], threads)
     dt = max(time.perf_counter() - t, 1e-6)
-    n = int(min(len(data), max(probe, probe * seconds / dt)))
+    n = int(min(len(data), max(probe, probe * seconds / dt), 0xFFFFFFFF))
     t = time.perf_counter()
-    oracle.scan_patterns(pats, data[:n], threads)
+    oracle.scan_patterns(wl.patterns, data[:n], threads)
     dt = time.perf_counter() - t
     return {"value": round(n / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"first {n} bytes of the same input ({n / dt / 1e6:.1f} MB/s over {dt:.1f} s)"}
@@ -158,7 +175,6 @@ def run_reference(args, rank):
         return
     wl = make_workload(args.config, args.size)
     base = cpu_baseline(wl, seconds=max(2.0, 60.0 / max(args.steps + args.warmup, 1)))
-    vals = [base["value"]]
     line = {"metric": METRIC, "value": base["value"], "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
@@ -166,8 +182,31 @@ def run_reference(args, rank):
             "impl": "reference", "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "oracle port of the reference CPU algorithm (the Rust crate and its wgpu path cannot run here)"}
-    del vals
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+def build_matchers(ws, wl, config):
+    ps = ws.PatternSet.builder()
+    for kind, p in wl.patterns:
+        ps = ps.literal_bytes(p) if kind == 0 else ps.regex(p.decode())
+    ps = ps.build()
+    cfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_SPECULATIVE)
+    m = ws.GpuMatcher.with_config(ps, cfg)
+    plain = None
+    has_regex = any(k == 1 for k, _ in wl.patterns)
+    if has_regex and config in ("regex", "batch", "dna"):
+        pcfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_PLAIN)
+        plain = ws.GpuMatcher.with_config(ps, pcfg)
+    train_s = None
+    if has_regex:
+        # the proposer learns from a separately seeded 256 MiB corpus of the same distribution
+        t0 = time.perf_counter()
+        corpus = W.dna_training_corpus() if config == "dna" else W.regex_training_corpus()
+        m.train_proposer(corpus)
+        train_s = time.perf_counter() - t0
+        del corpus
+    return m, plain, train_s
 
 
 def main():
@@ -177,9 +216,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="regex", choices=sorted(CONFIGS))
-    ap.add_argument("--size", type=int, default=None)
+    ap.add_argument("--size", type=int, default=None, help="input bytes (items for batch)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -192,6 +232,7 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
     dist = None
     if world > 1:
         import datetime
@@ -201,124 +242,164 @@ def main():
     import warpstate_b200 as ws
 
     wl = make_workload(args.config, args.size)
-    n_bytes = int(wl.data.nbytes)
-    ps = ws.PatternSet.builder()
-    for kind, p in wl.patterns:
-        ps = ps.literal_bytes(p) if kind == 0 else ps.regex(p.decode())
-    ps = ps.build()
-
-    cfg = ws.AutoMatcherConfig().max_matches(8 << 20).profile(True)
-    plain = None
-    if args.config == "regex":
-        cfg.regex_mode(ws.REGEX_SPECULATIVE)
-        pcfg = ws.AutoMatcherConfig().max_matches(8 << 20).profile(True).regex_mode(ws.REGEX_PLAIN)
-        plain = ws.GpuMatcher.with_config(ps, pcfg)
-    m = ws.GpuMatcher.with_config(ps, cfg)
-    train_s = None
-    if args.config == "regex":
-        # the proposer learns from a separately seeded 256 MiB corpus of the same distribution
-        t0 = time.perf_counter()
-        corpus = W.regex_training_corpus(256 * W.MiB)
-        m.train_proposer(corpus)
-        train_s = time.perf_counter() - t0
-        del corpus
-
-    d_in = torch.from_numpy(wl.data).to(f"cuda:{local}")
-    cap = 8 << 20
-    d_out = torch.empty((cap, 3), dtype=torch.int32, device=f"cuda:{local}")
-    d_cnt = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local}")
+    m, plain, train_s = build_matchers(ws, wl, args.config)
+    if args.no_plain:
+        plain = None
     stream = torch.cuda.current_stream()
-    flush = None
-    if n_bytes < (256 << 20):
-        flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    batch = wl.items is not None
+    big = args.config == "dna" or wl.data.nbytes > 0xFFFFFFFF
 
-    def timed_steps(matcher, steps, warmup, sampler=None):
+    # device-resident inputs and outputs
+    if batch:
+        lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+        n_bytes = int(lens.sum())
+        n_items = len(lens)
+        d_in = torch.from_numpy(wl.data[:n_bytes]).to(dev)
+        d_ends = torch.from_numpy(np.cumsum(lens).astype(np.uint32).view(np.int32)).to(dev)
+        d_ids = torch.arange(n_items, dtype=torch.int64, device=dev)
+        d_out = torch.empty(CAP * 3, dtype=torch.int64, device=dev)  # ws_tagged_match = 24 B
+    else:
+        n_bytes = int(wl.data.nbytes)
+        n_items = 1
+        d_in = torch.from_numpy(wl.data).to(dev)
+        d_out = torch.empty(CAP * 3, dtype=torch.int64, device=dev)  # ws_match (12 B) or ws_match64 (24 B)
+    d_cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev) if n_bytes < (256 << 20) else None
+
+    def step(matcher):
+        s = stream.cuda_stream
+        if batch:
+            matcher.scan_batch_device(d_in.data_ptr(), n_bytes, d_ends.data_ptr(), d_ids.data_ptr(), n_items,
+                                      d_out.data_ptr(), CAP, d_cnt.data_ptr(), s)
+        elif big:
+            matcher.scan_device64(d_in.data_ptr(), n_bytes, d_out.data_ptr(), CAP, d_cnt.data_ptr(), s)
+        else:
+            matcher.scan_device(d_in.data_ptr(), n_bytes, d_out.data_ptr(), CAP, d_cnt.data_ptr(), s)
+
+    def timed_steps(matcher, steps, warmup):
         for _ in range(warmup):
-            matcher.scan_device(d_in.data_ptr(), n_bytes, d_out.data_ptr(), cap, d_cnt.data_ptr(), stream.cuda_stream)
+            step(matcher)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        total = 0.0
-        kern = []
-        infos = []
+        total, infos = 0.0, []
         for _ in range(steps):
             if flush is not None:
                 flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            matcher.scan_device(d_in.data_ptr(), n_bytes, d_out.data_ptr(), cap, d_cnt.data_ptr(), stream.cuda_stream)
+            step(matcher)
             e1.record(stream)
             e1.synchronize()
             total += e0.elapsed_time(e1)
-            inf = matcher.info()
-            kern.append(inf["last_kernel_ms"])
-            infos.append(inf)
+            infos.append(matcher.info())
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        return total / steps, kern, infos
+        return total / steps, infos
 
-    # speculative (or the only) path
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # the speculative (or only) path
     with ClockSampler(local) as clk:
-        ms, kern, infos = timed_steps(m, args.steps, args.warmup)
+        ms, infos = timed_steps(m, args.steps, args.warmup)
     clocks = clk.summary()
     count = int(d_cnt.item())
-    if count > cap:
-        raise SystemExit(f"match overflow ({count} > {cap})")
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    if count > CAP:
+        raise SystemExit(f"match overflow ({count} > {CAP})")
+    ms_max = max_over_ranks(ms)
     value = world * n_bytes / (ms_max * 1e-3) / 1e9
 
-    plain_gbs = None
-    plain_ms = None
+    plain_gbs = plain_ms = None
     if plain is not None:
-        pms, _, _ = timed_steps(plain, max(2, args.steps // 2), 1)
-        pt = torch.tensor([pms], dtype=torch.float64, device=f"cuda:{local}")
-        if dist:
-            dist.all_reduce(pt, op=dist.ReduceOp.MAX)
-        plain_ms = float(pt.item())
+        pms, _ = timed_steps(plain, max(1, min(2, args.steps)), 1)
+        plain_ms = max_over_ranks(pms)
         plain_gbs = world * n_bytes / (plain_ms * 1e-3) / 1e9
         plain_count = int(d_cnt.item())
         if plain_count != count:
             raise SystemExit(f"plain/speculative match counts differ: {plain_count} vs {count}")
 
+    # batch: per-item dispatch of the plain kernel from host memory (one scan
+    # call, one H2D copy and one readback per item), the shape of the
+    # reference's per-call GPU round trips, on the first items
+    per_item = None
+    if batch and plain is not None:
+        import ctypes
+        import warpstate_b200._native as N
+        k = min(n_items, 2000)
+        offs = np.concatenate([[0], np.cumsum(lens[:k])]).astype(np.int64)
+        host = np.ascontiguousarray(wl.data[: int(offs[k])])
+        out1 = (N.WsMatch * (1 << 20))()
+        cnt1 = ctypes.c_uint64()
+        err1 = N.WsErrorInfo()
+        lib = N.lib()
+        t0 = time.perf_counter()
+        for i in range(k):
+            st = lib.ws_scan(plain._h, host.ctypes.data + int(offs[i]), int(lens[i]), out1, 1 << 20,
+                             ctypes.byref(cnt1), ctypes.byref(err1))
+            if st != 0:
+                raise SystemExit(f"per-item scan failed with status {st}")
+        dt_items = time.perf_counter() - t0
+        per_item = {"items": k, "bytes": int(offs[k]), "ms": round(dt_items * 1e3, 3),
+                    "gbs": round(int(offs[k]) / dt_items / 1e9, 4),
+                    "api": "GpuMatcher.scan (ws_scan), plain kernel, one call per item from host memory"}
+
     # roofline of the dominant kernel
     peak, peak_kind = load_peaks()
-    if args.config == "regex":
-        kidx, kname = 1, "dfa_walk"
-    else:
-        kidx, kname = 0, "literal_scan"
-    kms = statistics.mean(k[kidx] for k in kern) if kern else None
-    alg_bytes = n_bytes + 12 * count
+    has_regex = any(k == 1 for k, _ in wl.patterns)
+    kidx, kname = (1, "dfa_walk") if has_regex else (0, "literal_scan")
+    kms = statistics.mean(i["last_kernel_ms"][kidx] for i in infos) if infos else None
+    alg_bytes = n_bytes + 12 * count + (16 * n_items if batch else 0)
     achieved = alg_bytes / (kms * 1e-3) / 1e9 if kms else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 2) if achieved else None, "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4) if achieved else None,
                 "traffic": read_traffic(kname, args.config), "kernel": kname,
-                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "kernel_ms": round(kms, 4) if kms else None,
+                "peak_source": (f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                                else "fallback 6.65 TB/s"),
                 "algorithmic_bytes_per_launch": alg_bytes}
 
     # end to end through the public API from pinned host memory
     e2e = None
     if not args.no_e2e:
         pinned = torch.empty(n_bytes, dtype=torch.uint8, pin_memory=True)
-        pinned.numpy()[:] = wl.data
+        pinned.numpy()[:] = wl.data[:n_bytes]
         hv = pinned.numpy()
-        m.scan_array(hv)
+        if batch:
+            def call():
+                return ws.scan_batch_packed(m, pinned, lens)
+            d2h = lambda n: 24 * n + 8  # noqa: E731
+        elif big:
+            sp = ws.StreamPipeline(m)
+
+            def call():
+                return sp.scan_array(pinned)
+            d2h = lambda n: 24 * n + 8  # noqa: E731
+        else:
+            def call():
+                return m.scan_array(hv)
+            d2h = lambda n: 12 * n + 8  # noqa: E731
+        res = call()
         torch.cuda.synchronize()
-        k = max(2, min(args.steps, 5))
+        k = max(2, min(args.steps, 5)) if n_bytes < (2 << 30) else 2
         t0 = time.perf_counter()
         for _ in range(k):
-            res = m.scan_array(hv)
+            res = call()
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / k
         if len(res) != count:
             raise SystemExit(f"e2e count {len(res)} != device count {count}")
         e2e = {"value": round(world * n_bytes / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": n_bytes,
-               "d2h_bytes_per_step": 8 + 12 * count, "ms_per_step": round(dt * 1e3, 3)}
+               "d2h_bytes_per_step": d2h(count), "ms_per_step": round(dt * 1e3, 3),
+               "api": ("scan_batch_packed (ws_scan_batch)" if batch else
+                       "StreamPipeline.scan (ws_stream_*)" if big else "GpuMatcher.scan (ws_scan)")}
+        del pinned, hv
 
     base = None
     if rank == 0 and not args.no_cpu:
@@ -339,7 +420,7 @@ def main():
         "dtype": "u8",
         "data": "synthetic",
         "config": {"workload": args.config, "description": CONFIGS[args.config], "bytes_per_rank": n_bytes,
-                   "patterns": len(wl.patterns), "matches": count,
+                   "items": n_items if batch else None, "patterns": len(wl.patterns), "matches": count,
                    "l2": "input larger than L2" if flush is None else "L2 flushed (512 MiB write) between steps",
                    "parallelism": f"replicas x{world}"},
         "roofline": roofline,
@@ -348,15 +429,20 @@ def main():
         "gpu_launches": int(launches) * args.steps,
         "clocks": clocks,
     }
-    if plain_gbs is not None:
+    if has_regex:
         last = infos[-1]
-        line["regex"] = {"speculative_gbs": round(value, 3), "plain_gbs": round(plain_gbs, 3),
-                         "speedup_vs_plain": round(value / plain_gbs, 3), "plain_ms_per_step": round(plain_ms, 4),
+        line["regex"] = {"speculative_gbs": round(value, 3),
+                         "plain_gbs": round(plain_gbs, 3) if plain_gbs else None,
+                         "speedup_vs_plain": round(value / plain_gbs, 3) if plain_gbs else None,
+                         "plain_ms_per_step": round(plain_ms, 4) if plain_ms else None,
                          "proposer_top1": last["proposer_top1"], "proposer_top4": last["proposer_top4"],
                          "proposer_train_s": round(train_s, 2) if train_s else None,
                          "fixup_chunks": last["last_fixup_chunks"], "chunks": last["last_chunks"],
                          "groups": last["n_groups"], "states": last["total_states"],
                          "phase_ms": [round(x, 4) for x in last["last_kernel_ms"]]}
+    if per_item is not None:
+        line["batch"] = {"per_item_plain_dispatch": per_item,
+                         "batched_gbs": round(value, 3)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

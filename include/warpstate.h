@@ -141,7 +141,8 @@ typedef struct {
   uint64_t proposer_seed;          /* corpus seed for proposer training */
   uint32_t flags;                  /* WS_FLAG_* below */
   uint32_t batch_mib;              /* ws_scan_batch: bytes per launch sequence, MiB (0: 1024) */
-  uint32_t reserved[6];
+  uint32_t window_mib;             /* streams, ws_scan_device64: new bytes per window, MiB (0: 1024) */
+  uint32_t reserved[5];
 } ws_config;
 
 enum { WS_REGEX_SPECULATIVE = 0, WS_REGEX_PLAIN = 1 };
@@ -199,6 +200,28 @@ ws_status ws_scan_literals_noalloc(ws_matcher* m, const uint8_t* d_data, uint64_
 ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t n_items,
                         ws_tagged_match* out, uint64_t cap, uint64_t* n_out,
                         ws_error_info* err);
+
+/* Device-resident form of ws_scan_batch (no reference counterpart: the
+ * reference always coalesces on the host, core/src/batch.rs:65-98).  The items
+ * are already coalesced in device memory: d_data (16-byte aligned, len < 4 GiB)
+ * holds them back to back, d_item_end[i] is the exclusive end of item i
+ * (ascending, the last equal to len) and d_ids[i] its source id.  Tagged
+ * matches (item-relative offsets) go to d_out in no particular order;
+ * *d_count (device) receives the true count.  Asynchronous on `stream`. */
+ws_status ws_scan_batch_device(ws_matcher* m, const uint8_t* d_data, uint64_t len,
+                               const uint32_t* d_item_end, const uint64_t* d_ids, uint64_t n_items,
+                               ws_tagged_match* d_out, uint64_t cap, uint64_t* d_count,
+                               void* stream, ws_error_info* err);
+
+/* Device-resident scan of an input of any size with 64-bit offsets (the
+ * stream machinery over a buffer already in device memory: windows of up to
+ * 1 GiB with exact state carry).  The reference caps scans at u32 offsets
+ * (core/src/gpu/mod.rs:248-262); this has no counterpart there.  Matches go to
+ * d_out in no particular order; *d_count (device) receives the true count.
+ * Asynchronous on `stream`. */
+ws_status ws_scan_device64(ws_matcher* m, const uint8_t* d_data, uint64_t len,
+                           ws_match64* d_out, uint64_t cap, uint64_t* d_count,
+                           void* stream, ws_error_info* err);
 
 /* StreamPipeline (core/src/pipeline.rs:87-153) with state carry: feed bytes in
  * pieces of any size; matches are reported once, with global 64-bit offsets,

@@ -241,3 +241,57 @@ def test_stream_drains_when_the_output_is_small():
     assert N.lib().ws_stream_end(h, out, 2, ctypes.byref(cnt), ctypes.byref(err)) == 0 and cnt.value == 0
     N.lib().ws_stream_destroy(h)
     assert sorted(got) == [(2 * k, 2 * k + 2) for k in range(5)]
+
+
+# ------------------------------------------------------ device-resident
+def _torch():
+    import torch
+    return torch
+
+
+def test_scan_device64_windows_equal_whole_scan():
+    # windows of 1 MiB over a 3 MiB device buffer: the 64-bit device scan
+    # carries state across windows exactly like a stream
+    torch = _torch()
+    wl = w.regex(size=3 << 20, n=80, seed=41)
+    pats = wl.patterns + w.literals_large(size=1 << 10, n=200, seed=42).patterns
+    for mode in (PLAIN, SPEC):
+        m = matcher(pats, mode=mode, window_mib=1)
+        exp = oracle.scan_patterns(pats, wl.data).astype(np.uint64)
+        d_in = torch.from_numpy(wl.data).cuda()
+        cap = 1 << 16
+        d_out = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+        d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        s = torch.cuda.current_stream()
+        m.scan_device64(d_in.data_ptr(), d_in.numel(), d_out.data_ptr(), cap, d_cnt.data_ptr(), s.cuda_stream)
+        torch.cuda.synchronize()
+        n = int(d_cnt.item())
+        a = d_out[: 3 * n].view(n, 3).cpu().numpy()
+        got = np.stack([a[:, 0] & 0xFFFFFFFF, a[:, 1], a[:, 2]], axis=1).astype(np.uint64)
+        got = got[np.lexsort((got[:, 2], got[:, 0], got[:, 1]))]
+        assert len(exp) > 50 and np.array_equal(got, exp), mode
+
+
+def test_scan_batch_device_equals_oracle():
+    torch = _torch()
+    wl = _batch_workload(n_items=1500, seed=43)
+    m = matcher(wl.patterns)
+    lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+    ends = np.cumsum(lens).astype(np.uint32)
+    ids = (np.arange(len(lens), dtype=np.int64) * 3 + 1)
+    d_in = torch.from_numpy(wl.data[: int(lens.sum())]).cuda()
+    d_ends = torch.from_numpy(ends.view(np.int32)).cuda()
+    d_ids = torch.from_numpy(ids).cuda()
+    cap = 1 << 16
+    d_out = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream()
+    m.scan_batch_device(d_in.data_ptr(), d_in.numel(), d_ends.data_ptr(), d_ids.data_ptr(), len(lens),
+                        d_out.data_ptr(), cap, d_cnt.data_ptr(), s.cuda_stream)
+    torch.cuda.synchronize()
+    n = int(d_cnt.item())
+    a = d_out[: 3 * n].view(n, 3).cpu().numpy().view(np.uint64)
+    got = np.stack([a[:, 0], a[:, 1] & 0xFFFFFFFF, a[:, 1] >> 32, a[:, 2] & 0xFFFFFFFF], axis=1)
+    got = got[np.lexsort((got[:, 3], got[:, 1], got[:, 2], got[:, 0]))]
+    exp = oracle.batch_scan(wl.patterns, wl.data, wl.items, ids.astype(np.uint64))
+    assert len(exp) > 100 and np.array_equal(got, exp)

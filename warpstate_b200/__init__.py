@@ -366,6 +366,11 @@ class AutoMatcherConfig:
         self.c.batch_mib = int(n)
         return self
 
+    def window_mib(self, n: int):
+        """New bytes per window of a stream or a 64-bit device scan, in MiB (0: 1024)."""
+        self.c.window_mib = int(n)
+        return self
+
     def profile(self, yes: bool = True):
         """Record CUDA events around each kernel phase (GpuMatcher.info())."""
         self.c.flags = (self.c.flags | 1) if yes else (self.c.flags & ~1)
@@ -462,6 +467,17 @@ class GpuMatcher:
     def scan_device(self, d_data: int, length: int, d_out: int, cap: int, d_count: int, stream: int = 0):
         """Device-resident scan (pointers are CUDA device addresses)."""
         _call(N.lib().ws_scan_device, self._h, d_data, length, d_out, cap, d_count, stream)
+
+    def scan_device64(self, d_data: int, length: int, d_out: int, cap: int, d_count: int, stream: int = 0):
+        """Device-resident scan of any size; ws_match64 output (unsorted)."""
+        _call(N.lib().ws_scan_device64, self._h, d_data, length, d_out, cap, d_count, stream)
+
+    def scan_batch_device(self, d_data: int, length: int, d_item_end: int, d_ids: int, n_items: int, d_out: int,
+                          cap: int, d_count: int, stream: int = 0):
+        """Device-resident batch scan of items coalesced in d_data (u32 item
+        ends, u64 ids); ws_tagged_match output (unsorted)."""
+        _call(N.lib().ws_scan_batch_device, self._h, d_data, length, d_item_end, d_ids, n_items, d_out, cap, d_count,
+              stream)
 
     def train_proposer(self, corpus, seed: int = 0x5EED) -> dict:
         """Trains the learned boundary-state proposer of the speculative regex

@@ -61,7 +61,7 @@ class WsConfig(ctypes.Structure):
                 ("dfa_max_states", ctypes.c_uint32), ("walk_chunk", ctypes.c_uint32),
                 ("proposer", ctypes.c_uint32), ("proposer_train_bytes", ctypes.c_uint64),
                 ("proposer_seed", ctypes.c_uint64), ("flags", ctypes.c_uint32),
-                ("batch_mib", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+                ("batch_mib", ctypes.c_uint32), ("window_mib", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 5)]
 
 
 class WsMatcherInfo(ctypes.Structure):
@@ -96,6 +96,11 @@ SIGNATURES = {
                                                 ctypes.POINTER(WsErrorInfo)]),
     "ws_scan_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsItem), ctypes.c_uint64,
                                      ctypes.POINTER(WsTaggedMatch), ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),
+    "ws_scan_batch_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(WsErrorInfo)]),
+    "ws_scan_device64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                        ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_feed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(WsMatch64),
                                       ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),

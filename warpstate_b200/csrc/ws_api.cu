@@ -107,10 +107,11 @@ void stage_input(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len) {
 
 uint64_t device_capacity(const ws_matcher* m) { return std::max<uint64_t>(m->cfg.max_matches, 1); }
 
-void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
-                  ws_match* d_out, uint64_t cap, unsigned long long* d_counter, const ScanExtras& x) {
+uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
+                      ws_match* d_out, uint64_t cap, unsigned long long* d_counter, const ScanExtras& x) {
   const bool prof = m->profile;
   uint32_t launches = 0;
+  m->use_summed = false;
   check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
   if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
   if (m->lit.n_literals && x.literals) {
@@ -138,6 +139,19 @@ void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_d
   std::lock_guard<std::mutex> g(m->info_mu);
   m->info.last_launches = launches;
   m->info.last_chunks = m->rx.last_chunks;
+  return launches;
+}
+
+void read_phases(ws_matcher* m, double* ms) {
+  check_cuda(cudaEventSynchronize(m->pev[2]), "event sync");
+  ws_matcher_info tmp;
+  std::memset(&tmp, 0, sizeof(tmp));
+  float a = 0, b = 0;
+  if (cudaEventElapsedTime(&a, m->pev[0], m->pev[1]) == cudaSuccess) tmp.last_kernel_ms[0] = a;
+  if (cudaEventElapsedTime(&b, m->pev[0], m->pev[2]) == cudaSuccess) tmp.last_kernel_ms[7] = b;
+  if (m->rx.n_regex) regex_collect_timing(m->rx, m->rx_events, tmp);
+  cudaGetLastError();
+  for (int k = 0; k < 8; ++k) ms[k] = tmp.last_kernel_ms[k];
 }
 
 void check_regex_overflow(ws_matcher* m, Scratch& s) {
@@ -312,7 +326,9 @@ ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out) {
   if (!m || !out) return WS_ERR_INVALID_ARGUMENT;
   auto* mm = const_cast<ws_matcher*>(m);
   std::lock_guard<std::mutex> g(mm->info_mu);
-  if (mm->profile && mm->pev[2] && cudaEventQuery(mm->pev[2]) != cudaErrorNotReady) {
+  if (mm->profile && mm->use_summed) {
+    for (int k = 0; k < 8; ++k) mm->info.last_kernel_ms[k] = mm->summed_ms[k];
+  } else if (mm->profile && mm->pev[2] && cudaEventQuery(mm->pev[2]) != cudaErrorNotReady) {
     cudaEventSynchronize(mm->pev[2]);
     float a = 0, b = 0;
     if (cudaEventElapsedTime(&a, mm->pev[0], mm->pev[1]) == cudaSuccess) mm->info.last_kernel_ms[0] = a;

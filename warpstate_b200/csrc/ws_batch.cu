@@ -106,6 +106,41 @@ class Gather {
 
 }  // namespace
 
+extern "C" ws_status ws_scan_batch_device(ws_matcher* m, const uint8_t* d_data, uint64_t len,
+                                          const uint32_t* d_item_end, const uint64_t* d_ids, uint64_t n_items,
+                                          ws_tagged_match* d_out, uint64_t cap, uint64_t* d_count, void* stream,
+                                          ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !d_count || (len && (!d_data || !d_item_end || !d_ids))) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    if (((uintptr_t)d_data & 15) != 0) raise(WS_ERR_INVALID_ARGUMENT, "device input must be 16-byte aligned");
+    if (len > 0xFFFFFFFFull - 64)
+      raise(WS_ERR_INPUT_TOO_LARGE, "coalesced batch is too large for 32-bit offsets", 0, len, 0xFFFFFFFFull - 64);
+    if (n_items > 0xFFFFFFFFull) raise(WS_ERR_INVALID_ARGUMENT, "too many items");
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    ScratchLease s(m);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    check_cuda(cudaStreamWaitEvent(st, s->busy, 0), "wait");
+    auto* d_counter = reinterpret_cast<unsigned long long*>(d_count);
+    if (len == 0 || n_items == 0) {
+      check_cuda(cudaMemsetAsync(d_counter, 0, 8, st), "memset");
+      check_cuda(cudaEventRecord(s->busy, st), "event");
+      return;
+    }
+    const uint64_t dcap = std::max<uint64_t>(cap, 1);
+    ensure(s->out, dcap * sizeof(ws_match));
+    ScanExtras x;
+    x.item_end = d_item_end;
+    x.n_items = (uint32_t)n_items;
+    const uint32_t launches = enqueue_scan(m, *s, st, d_data, len, s->out.as<ws_match>(), dcap, d_counter, x);
+    tag_kernel<<<m->ctx->sm_count * 4, 256, 0, st>>>(s->out.as<ws_match>(), d_counter, std::min(dcap, cap), d_item_end,
+                                                      d_ids, (uint32_t)n_items, d_out);
+    check_cuda(cudaGetLastError(), "tag_kernel");
+    check_cuda(cudaEventRecord(s->busy, st), "event");
+    std::lock_guard<std::mutex> g(m->info_mu);
+    m->info.last_launches = launches + 1;
+  });
+}
+
 extern "C" ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t n_items, ws_tagged_match* out,
                                    uint64_t cap, uint64_t* n_out, ws_error_info* err) {
   return guarded(err, [&] {

@@ -81,6 +81,9 @@ struct ws_matcher {
   bool profile = false;          // record phase events (single caller at a time)
   cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t rx_events[8] = {};
+  // phase times summed over the windows of the last multi-window scan
+  bool use_summed = false;
+  double summed_ms[8] = {};
   ~ws_matcher() {
     for (auto e : pev) if (e) cudaEventDestroy(e);
     for (auto e : rx_events) if (e) cudaEventDestroy(e);
@@ -131,9 +134,25 @@ void stage_input(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len);
 uint64_t device_capacity(const ws_matcher* m);
 // Enqueues the full scan of a device-resident input on `st`; nothing is read
 // back.  With profiling enabled, phase events are recorded on `st` as well.
-void enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
-                  ws_match* d_out, uint64_t cap, unsigned long long* d_counter, const ScanExtras& x = ScanExtras());
+// Returns the number of kernel launches enqueued.
+uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t* d_data, uint64_t len,
+                      ws_match* d_out, uint64_t cap, unsigned long long* d_counter,
+                      const ScanExtras& x = ScanExtras());
+// Waits for the last profiled scan and reads its phase times (ms[8], the
+// layout of ws_matcher_info.last_kernel_ms).
+void read_phases(ws_matcher* m, double* ms);
 // Raises MatchBufferOverflow when a regex scratch buffer overflowed.
 void check_regex_overflow(ws_matcher* m, Scratch& s);
+
+// One window of a scan in steps (stream feeds, ws_scan_device64): the bytes
+// seen so far are [0, seen), the previous window started at win_base, regex
+// starts below `frontier` are decided.  The new window is [keep, seen); after
+// the step every start below the returned frontier is decided (all of them
+// when `last`).
+struct StepPlan {
+  uint64_t keep, frontier;
+};
+StepPlan plan_step(const ws_matcher* m, uint64_t win_base, uint64_t old_seen, uint64_t seen, uint64_t frontier,
+                   bool last);
 
 }  // namespace ws

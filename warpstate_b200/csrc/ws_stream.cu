@@ -50,7 +50,7 @@ namespace {
 
 // New data per step: the window plus the step must stay below 4 GiB (32-bit
 // offsets inside a launch).
-constexpr uint64_t kStep = 1ull << 30;
+uint64_t step_bytes(const ws_matcher* m) { return (uint64_t)(m->cfg.window_mib ? m->cfg.window_mib : 1024) << 20; }
 
 int64_t regex_max_len(const ws_matcher* m) { return m->rx.n_regex ? m->rx.max_len : 0; }
 
@@ -89,21 +89,45 @@ void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t fr
   }
 }
 
-// Appends `len` bytes (len <= kStep) to the stream and decides what it can.
+}  // namespace
+
+namespace ws {
+
+StepPlan plan_step(const ws_matcher* m, uint64_t win_base, uint64_t old_seen, uint64_t seen, uint64_t frontier,
+                   bool last) {
+  StepPlan p;
+  // bytes [keep, old_seen) stay in the window: the literal tail and every
+  // undecided regex start
+  uint64_t keep = old_seen;
+  if (m->lit.n_literals && m->max_literal_len > 1)
+    keep = std::min(keep, old_seen - std::min<uint64_t>(old_seen, m->max_literal_len - 1));
+  if (m->rx.n_regex) keep = std::min(keep, frontier);
+  p.keep = std::max(keep, win_base);
+  const int64_t mx = regex_max_len(m);
+  if (last) {
+    frontier = seen;
+  } else if (mx >= 0 && seen + 1 > (uint64_t)mx) {
+    frontier = std::max(frontier, seen + 1 - (uint64_t)mx);
+  }
+  p.frontier = std::min(frontier, seen);
+  if (seen - p.keep > 0xFFFFFFFFull - 64)
+    raise(WS_ERR_INPUT_TOO_LARGE, "scan window exceeds 32-bit offsets (a regex with unbounded matches keeps the "
+          "whole undecided input in the window)", 0, seen - p.keep, 0xFFFFFFFFull - 64);
+  return p;
+}
+
+}  // namespace ws
+
+namespace {
+
+// Appends `len` bytes (len <= step_bytes) to the stream and decides what it can.
 void feed_step(ws_stream* st, const uint8_t* data, uint64_t len) {
   ws_matcher* m = st->m;
   Scratch& s = *st->s;
   const uint64_t old_seen = st->seen, seen = old_seen + len;
-  const int64_t mx = regex_max_len(m);
-  // bytes [keep, old_seen) stay in the window
-  uint64_t keep = old_seen;
-  if (m->lit.n_literals && m->max_literal_len > 1) keep = std::min(keep, old_seen - std::min<uint64_t>(old_seen, m->max_literal_len - 1));
-  if (m->rx.n_regex) keep = std::min(keep, st->frontier);
-  keep = std::max(keep, st->win_base);
+  const StepPlan plan = plan_step(m, st->win_base, old_seen, seen, st->frontier, false);
+  const uint64_t keep = plan.keep;
   const uint64_t carry = old_seen - keep;
-  if (carry + len > 0xFFFFFFFFull - 64)
-    raise(WS_ERR_INPUT_TOO_LARGE, "stream window exceeds 32-bit offsets (a regex with unbounded matches keeps the "
-          "whole undecided stream)", 0, carry + len, 0xFFFFFFFFull - 64);
   DeviceBuffer& dst = st->win[st->cur ^ 1];
   ensure(dst, carry + len + 64);
   if (carry)
@@ -115,11 +139,31 @@ void feed_step(ws_stream* st, const uint8_t* data, uint64_t len) {
   st->win_base = keep;
   st->win_len = carry + len;
   st->seen = seen;
-  uint64_t frontier = st->frontier;
-  if (mx >= 0 && seen + 1 > (uint64_t)mx) frontier = std::max(frontier, seen + 1 - (uint64_t)mx);
-  frontier = std::min(frontier, seen);
-  scan_window(st, m->lit.n_literals != 0, old_seen - keep, frontier);
-  st->frontier = frontier;
+  scan_window(st, m->lit.n_literals != 0, old_seen - keep, plan.frontier);
+  st->frontier = plan.frontier;
+}
+
+// Appends one window's matches to a 64-bit output: offsets shifted by the
+// window's stream offset, the step's true count added to the running total
+// (so a total above `cap` reports the overflow with the true count).
+__global__ void __launch_bounds__(1024) widen_kernel(const ws_match* in, const unsigned long long* step_count,
+                                                     uint64_t step_cap, uint64_t base, ws_match64* out, uint64_t cap,
+                                                     unsigned long long* total) {
+  const unsigned long long n = *step_count;
+  const unsigned long long at = *total;
+  const unsigned long long avail = n < step_cap ? n : step_cap;
+  for (unsigned long long k = threadIdx.x; k < avail; k += blockDim.x) {
+    if (at + k >= cap) break;
+    ws_match mm = in[k];
+    ws_match64 o;
+    o.pattern_id = mm.pattern_id;
+    o.reserved = 0;
+    o.start = base + mm.start;
+    o.end = base + mm.end;
+    out[at + k] = o;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *total = at + n;
 }
 
 // Copies up to `cap` undelivered matches out; overflow when some remain.
@@ -169,7 +213,7 @@ ws_status ws_stream_feed(ws_stream* st, const uint8_t* data, uint64_t len, ws_ma
     check_cuda(cudaSetDevice(st->m->ctx->device), "cudaSetDevice");
     try {
       for (uint64_t off = 0; off < len;) {
-        uint64_t n = std::min<uint64_t>(kStep, len - off);
+        uint64_t n = std::min<uint64_t>(step_bytes(st->m), len - off);
         feed_step(st, data + off, n);
         off += n;
       }
@@ -202,6 +246,69 @@ ws_status ws_stream_end(ws_stream* st, ws_match64* out, uint64_t cap, uint64_t* 
       check_cuda(cudaEventRecord(st->s->busy, st->s->stream), "event");
     }
     deliver(st, out, cap, n_out);
+  });
+}
+
+ws_status ws_scan_device64(ws_matcher* m, const uint8_t* d_data, uint64_t len, ws_match64* d_out, uint64_t cap,
+                           uint64_t* d_count, void* stream, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !d_count || (len && !d_data)) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    if (((uintptr_t)d_data & 15) != 0) raise(WS_ERR_INVALID_ARGUMENT, "device input must be 16-byte aligned");
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    ScratchLease s(m);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    check_cuda(cudaStreamWaitEvent(cs, s->busy, 0), "wait");
+    auto* total = reinterpret_cast<unsigned long long*>(d_count);
+    check_cuda(cudaMemsetAsync(total, 0, 8, cs), "memset count");
+    if (len == 0) {
+      check_cuda(cudaEventRecord(s->busy, cs), "event");
+      return;
+    }
+    // the whole schedule is known on the host: windows are slices of d_data
+    const uint64_t scap = std::max<uint64_t>(cap, 1);
+    ensure(s->out, scap * sizeof(ws_match));
+    const size_t cursor_bytes = ((size_t)m->rx.n_regex * 8 + 255) & ~(size_t)255;
+    ensure(s->aux, cursor_bytes + 256);
+    auto* cursor = s->aux.as<unsigned long long>();
+    auto* step_count = reinterpret_cast<unsigned long long*>(s->aux.as<uint8_t>() + cursor_bytes);
+    if (m->rx.n_regex) check_cuda(cudaMemsetAsync(cursor, 0, (size_t)m->rx.n_regex * 8, cs), "memset cursor");
+    uint64_t seen = 0, win_base = 0, frontier = 0;
+    uint32_t launches = 0;
+    double summed[8] = {};
+    while (seen < len) {
+      const uint64_t n = std::min<uint64_t>(step_bytes(m), len - seen);
+      const bool last = seen + n == len;
+      const StepPlan plan = plan_step(m, win_base, seen, seen + n, frontier, last);
+      // windows are slices of d_data: start them on a 16-byte boundary (the
+      // kernels load 16-byte vectors); the extra leading bytes hold only
+      // literal occurrences already reported and regex starts already decided
+      const uint64_t keep = plan.keep & ~15ull;
+      ScanExtras x;
+      x.literals = m->lit.n_literals != 0;
+      x.lit_min_end = seen - keep;
+      x.cursor = m->rx.n_regex ? cursor : nullptr;
+      x.base = keep;
+      x.frontier = plan.frontier;
+      launches += enqueue_scan(m, *s, cs, d_data + keep, seen + n - keep, s->out.as<ws_match>(), scap, step_count, x);
+      widen_kernel<<<1, 1024, 0, cs>>>(s->out.as<ws_match>(), step_count, scap, keep, d_out, cap, total);
+      check_cuda(cudaGetLastError(), "widen_kernel");
+      launches += 1;
+      if (m->profile) {  // profiling: phase times summed over the windows
+        double ms[8];
+        read_phases(m, ms);
+        for (int k = 0; k < 8; ++k) summed[k] += ms[k];
+      }
+      seen += n;
+      win_base = keep;
+      frontier = plan.frontier;
+    }
+    check_cuda(cudaEventRecord(s->busy, cs), "event");
+    std::lock_guard<std::mutex> g(m->info_mu);
+    m->info.last_launches = launches;
+    if (m->profile) {
+      for (int k = 0; k < 8; ++k) m->summed_ms[k] = summed[k];
+      m->use_summed = true;
+    }
   });
 }
 

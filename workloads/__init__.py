@@ -289,6 +289,11 @@ def regex_training_corpus(size: int = 256 * MiB, seed: int = 3) -> np.ndarray:
     return fill_markov(size, PRINTABLE, seed * 1000 + 77, seed * 1000 + 4)
 
 
+def dna_training_corpus(size: int = 256 * MiB, seed: int = 5) -> np.ndarray:
+    """Separately seeded corpus of the nucleotide configuration's distribution."""
+    return fill_acgt(size, seed * 1000 + 77)
+
+
 def batch(n_items: int = 200_000, n_lit: int = 1500, n_rx: int = 500, seed: int = 4,
           median: float = 4096.0, sigma: float = 1.5, lo: int = 64, hi: int = MiB) -> Workload:
     r = Rng(seed * 1000 + 1)
