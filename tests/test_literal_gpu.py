@@ -54,6 +54,32 @@ def test_literals_large_scaled():
     assert len(got) >= 4096
 
 
+def test_nucleotide_kmers_long_grams():
+    # 50,000 k-mers over ACGT saturate 4-byte grams: the plan switches to
+    # 16-byte grams and the L2 prefix Bloom; results stay exact
+    kmers = w.gen_literals(50_000, 20, 32, b"ACGT", [1.0] * 4, 5001)
+    data = w.fill_acgt(8 << 20, 5003)
+    w.plant(data, kmers[:4096], 1024, 5005)
+    pats = [(0, k) for k in kmers]
+    m, _ = gpu_scan(pats, data[:64])
+    assert m.info()["filter_q"] == 16
+    got = check(pats, data)
+    assert len(got) >= 4096
+
+
+def test_nucleotide_mixed_short_and_medium_literals():
+    # short literals ride along in the prefix Bloom; 8-byte grams when the
+    # shortest long literal has 11 bytes
+    kmers = w.gen_literals(20_000, 11, 24, b"ACGT", [1.0] * 4, 5011)
+    data = w.fill_acgt(1 << 20, 5013)
+    w.plant(data, kmers[:512], 1024, 5015)
+    pats = [(0, k) for k in kmers] + [(0, b"ACG"), (0, b"TT"), (0, b"N")]
+    m, _ = gpu_scan(pats, data[:64])
+    assert m.info()["filter_q"] == 8
+    got = check(pats, data)
+    assert len(got) >= 512
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 15, 16, 17, 31, 33, 63, 64, 65, 511, 512, 513, 4097])
 def test_ragged_lengths_and_tail_matches(n):
     rng = np.random.default_rng(n)

@@ -249,7 +249,7 @@ ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_co
     plan_regex(*t, m->cfg, ctx->sm_count, m->rx);
     m->info.n_literals = t->n_literals;
     m->info.n_regex = t->n_regex;
-    m->info.filter_q = 4;
+    m->info.filter_q = m->lit.gram_len;
     m->info.filter_period = m->lit.period;
     m->info.filter_bits = m->lit.table_bits;
     regex_fill_info(m->rx, m->info);

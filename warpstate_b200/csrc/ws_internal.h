@@ -93,12 +93,49 @@ struct LiteralPlan {
   std::vector<uint32_t> short_bits;   // 65536 bits
   std::vector<uint32_t> lit_info;     // 4 per literal: offset (in lit_bytes), len, pattern id, 0
   std::vector<uint8_t> lit_bytes;     // literals, each 4-byte aligned
-  DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries;
+  // Low-entropy pattern sets (e.g. nucleotide k-mers) saturate 4-byte grams:
+  // stage 1 then hashes longer grams (gram_len 8 or 16 bytes) and stage 1.5
+  // adds a second, L2-resident Bloom bitmap of the first min(len, 16) bytes.
+  uint32_t gram_len = 4;
+  uint32_t parts16 = 0;               // bit i: some literal has a key of i+1 bytes (<= 16)
+  std::vector<uint32_t> bloom2;       // 2^kBloom2Bits bits, only when gram_len > 4
+  DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2;
   uint32_t n_buckets = 0;
 };
 
+constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
+
 // Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).
 inline uint32_t gram_hash(uint32_t gram, uint32_t bits) { return (gram * 0x9E3779B1u) >> (32 - bits); }
+
+// Multiply-add hash of 2 or 4 words with a final avalanche (xor-shift,
+// multiply, xor-shift), for long grams and 16-byte prefix keys.
+__host__ __device__ inline uint32_t mix_words(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t salt) {
+  uint32_t h = w0 * 0x9E3779B1u + w1 * 0x85EBCA77u + w2 * 0xC2B2AE3Du + w3 * 0x27D4EB2Fu + salt * 0x165667B1u;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  return h;
+}
+
+// Stage-1 key of a gram of 4, 8 or 16 bytes (g[0..gram_len/4)).
+__host__ __device__ inline uint32_t long_gram_hash(uint32_t g0, uint32_t g1, uint32_t g2, uint32_t g3, uint32_t gram_len,
+                                                   uint32_t bits) {
+  return (gram_len == 8 ? mix_words(g0, g1, 0, 0, 8) : mix_words(g0, g1, g2, g3, 16)) >> (32 - bits);
+}
+
+// Word k of a key keeps only the bytes below pl.
+__host__ __device__ inline uint32_t key_word(uint32_t x, uint32_t k, uint32_t pl) {
+  if (pl >= 4 * k + 4) return x;
+  if (pl <= 4 * k) return 0u;
+  return x & ((1u << (8 * (pl - 4 * k))) - 1u);
+}
+
+// Stage-1.5b key of the first pl (1..16) bytes of the four words x.
+__host__ __device__ inline uint32_t prefix16_key(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3, uint32_t pl) {
+  return mix_words(key_word(x0, 0, pl), key_word(x1, 1, pl), key_word(x2, 2, pl), key_word(x3, 3, pl), pl) >>
+         (32 - kBloom2Bits);
+}
 
 void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan);
 

@@ -126,6 +126,7 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
     plan.lit_info[4 * li + 1] = len;
     plan.lit_info[4 * li + 2] = t.literal_pattern_ids[li];
     plan.lit_bytes.insert(plan.lit_bytes.end(), lit, lit + len);
+    plan.parts16 |= 1u << (std::min<uint32_t>(std::max<uint32_t>(len, 1), 16) - 1);
     {
       // Bloom bitmap of the first min(len, 8) bytes (the kernel's prefix_key)
       uint32_t pl = std::max<uint32_t>(std::min<uint32_t>(len, HASH_WINDOW), 1);
@@ -159,6 +160,52 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
     }
   }
   while (plan.lit_bytes.size() % 16) plan.lit_bytes.push_back(0);
+  // A low-entropy pattern set (a small alphabet whose 4-grams the literals
+  // mostly cover, e.g. nucleotide k-mers) lets most input positions through
+  // 4-byte grams: then switch to the longest gram every long literal holds at
+  // all P phases, and add the 16-byte-prefix Bloom.
+  if (plan.has_long && P == 4) {
+    bool seen_byte[256] = {};
+    std::vector<uint32_t> grams;
+    for (uint32_t li = 0; li < t.n_literals; ++li) {
+      const uint32_t len = t.offsets[2 * li + 1];
+      const uint8_t* lit = t.packed_bytes + t.offsets[2 * li];
+      for (uint32_t k = 0; k < len; ++k) seen_byte[lit[k]] = true;
+      for (uint32_t k = 0; len >= 4 && k < P; ++k) {
+        uint32_t g;
+        std::memcpy(&g, lit + k, 4);
+        grams.push_back(g);
+      }
+    }
+    std::sort(grams.begin(), grams.end());
+    const double distinct = (double)(std::unique(grams.begin(), grams.end()) - grams.begin());
+    double alphabet = 0;
+    for (bool b : seen_byte) alphabet += b ? 1.0 : 0.0;
+    const double coverage = distinct / std::min(alphabet * alphabet * alphabet * alphabet, 4294967296.0);
+    const uint32_t G = min_long >= 19 ? 16 : min_long >= 11 ? 8 : 4;
+    if (coverage > 0.25 && G > 4) {
+      plan.gram_len = G;
+      std::fill(plan.filter.begin(), plan.filter.end(), 0u);
+      plan.bloom2.assign((size_t)1 << (kBloom2Bits - 5), 0u);
+      for (uint32_t li = 0; li < t.n_literals; ++li) {
+        const uint32_t len = t.offsets[2 * li + 1];
+        const uint8_t* lit = t.packed_bytes + t.offsets[2 * li];
+        for (uint32_t k = 0; len >= 4 && k < P; ++k) {
+          uint32_t g[4] = {0, 0, 0, 0};
+          std::memcpy(g, lit + k, G);
+          uint32_t h = long_gram_hash(g[0], g[1], g[2], g[3], G, bits);
+          plan.filter[h >> 3] |= (1u << (P - 1 - k)) << ((h & 7) * 4);
+        }
+        // every literal (short ones too) is in the prefix Bloom
+        uint32_t x[4] = {0, 0, 0, 0};
+        const uint32_t pl = std::min<uint32_t>(len, 16);
+        std::memcpy(x, lit, pl);
+        uint32_t key = prefix16_key(x[0], x[1], x[2], x[3], pl);
+        plan.bloom2[key >> 5] |= 1u << (key & 31);
+      }
+      plan.d_bloom2.upload(plan.bloom2.data(), plan.bloom2.size() * 4);
+    }
+  }
   plan.n_buckets = t.n_buckets;
   plan.d_filter.upload(plan.filter.data(), plan.filter.size() * 4);
   plan.d_bloom.upload(plan.bloom.data(), plan.bloom.size() * 4);

@@ -64,6 +64,9 @@ struct LitArgs {
   const uint32_t* item_end;  // batch: ascending item ends (n_items), else null
   uint32_t n_items;
   uint64_t min_end;          // stream: matches ending at or before it were reported
+  uint32_t gram_len;         // stage-1 gram bytes: 4, 8 or 16 (8 and 16 with P = 4)
+  uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
+  const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
 };
 
 __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint32_t bits) {
@@ -119,14 +122,31 @@ __device__ void verify_position(const LitArgs& a, uint64_t s) {
   }
 }
 
+__device__ __forceinline__ uint32_t nib_long(const uint32_t* tab, uint32_t g0, uint32_t g1, uint32_t g2, uint32_t g3,
+                                             uint32_t gram_len, uint32_t bits) {
+  uint32_t h = long_gram_hash(g0, g1, g2, g3, gram_len, bits);
+  return (tab[h >> 3] >> ((h & 7) << 2)) & 0xFu;
+}
+
 // 16-bit mask of owned positions that may start a literal (stage 1).  w[0..3]
-// are the thread's own words; w4 is the first word of the next thread (needed
-// by the P = 1 and P = 2 layouts and by lane 31).
+// are the thread's own words; w[4..7] are the next thread's words (w[4] is
+// needed by the P = 1 and P = 2 layouts and by lane 31, w[5..7] by grams
+// longer than 4 bytes).
 __device__ __forceinline__ uint32_t stage1(const LitArgs& a, const uint32_t* filt, const uint32_t* shortb,
-                                           const uint32_t (&w)[5], uint32_t lane) {
+                                           const uint32_t (&w)[8], uint32_t lane) {
   uint32_t mask = 0;
   if (a.has_long) {
-    if (a.period == 4) {
+    if (a.gram_len > 4) {
+      // P = 4, grams of 8 or 16 bytes starting at the four aligned words
+      uint32_t n0 = nib_long(filt, w[0], w[1], w[2], w[3], a.gram_len, a.bits);
+      uint32_t n1 = nib_long(filt, w[1], w[2], w[3], w[4], a.gram_len, a.bits);
+      uint32_t n2 = nib_long(filt, w[2], w[3], w[4], w[5], a.gram_len, a.bits);
+      uint32_t n3 = nib_long(filt, w[3], w[4], w[5], w[6], a.gram_len, a.bits);
+      uint32_t n4 = __shfl_down_sync(0xFFFFFFFFu, n0, 1);
+      if (lane == 31) n4 = nib_long(filt, w[4], w[5], w[6], w[7], a.gram_len, a.bits);
+      uint32_t m = n0 | (n1 << 4) | (n2 << 8) | (n3 << 12) | (n4 << 16);
+      mask |= (m >> 3) & 0xFFFFu;
+    } else if (a.period == 4) {
       uint32_t n0 = nib(filt, w[0], a.bits);
       uint32_t n1 = nib(filt, w[1], a.bits);
       uint32_t n2 = nib(filt, w[2], a.bits);
@@ -228,8 +248,18 @@ __global__ void __launch_bounds__(kThreads, 1) literal_filter_kernel(LitArgs a) 
       blk[132] = 0;
       blk[133] = 0;
     }
-    uint32_t w[5] = {cur.x, cur.y, cur.z, cur.w, __shfl_down_sync(0xFFFFFFFFu, cur.x, 1)};
-    if (lane == 31) w[4] = tail.x;
+    uint32_t w[8] = {cur.x, cur.y, cur.z, cur.w, __shfl_down_sync(0xFFFFFFFFu, cur.x, 1), 0, 0, 0};
+    if (a.gram_len > 4) {
+      w[5] = __shfl_down_sync(0xFFFFFFFFu, cur.y, 1);
+      w[6] = __shfl_down_sync(0xFFFFFFFFu, cur.z, 1);
+      w[7] = __shfl_down_sync(0xFFFFFFFFu, cur.w, 1);
+    }
+    if (lane == 31) {
+      w[4] = tail.x;
+      w[5] = tail.y;
+      w[6] = tail.z;
+      w[7] = tail.w;
+    }
     uint32_t mask = stage1(a, filt, shortb, w, lane);
     const uint64_t blk_base = b * 512;
     const uint64_t base = v * 16;
@@ -269,6 +299,19 @@ __global__ void __launch_bounds__(kThreads, 1) literal_filter_kernel(LitArgs a) 
             uint32_t key = prefix_key(lo, hi, pl);
             keep |= (bloom[key >> 5] >> (key & 31)) & 1u;
           }
+        }
+        if (keep && a.bloom2) {
+          // stage 1.5b: the first min(len, 16) bytes against the L2 bitmap
+          uint32_t x3 = blk[wi + 3], x4 = blk[wi + 4];
+          uint32_t y2 = __funnelshift_r(x2, x3, sh), y3 = __funnelshift_r(x3, x4, sh);
+          bool k2 = false;
+          for (uint32_t pl = 1; pl <= 16; ++pl) {
+            if ((a.parts16 >> (pl - 1)) & 1u) {
+              uint32_t key = prefix16_key(lo, hi, y2, y3, pl);
+              k2 |= (__ldg(a.bloom2 + (key >> 5)) >> (key & 31)) & 1u;
+            }
+          }
+          keep = k2;
         }
       }
       uint32_t ball = __ballot_sync(0xFFFFFFFFu, keep);
@@ -336,6 +379,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.item_end = l.item_end;
   a.n_items = l.n_items;
   a.min_end = l.min_end;
+  a.gram_len = plan.gram_len;
+  a.parts16 = plan.parts16;
+  a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   size_t smem = literal_smem_bytes(plan);
   check_cuda(cudaFuncSetAttribute(literal_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
