@@ -223,6 +223,20 @@ ws_status ws_scan_device64(ws_matcher* m, const uint8_t* d_data, uint64_t len,
                            ws_match64* d_out, uint64_t cap, uint64_t* d_count,
                            void* stream, ws_error_info* err);
 
+/* One shard of a scan split across GPUs: the multi-GPU form of
+ * MultiGpuMatcher::scan (core/src/multi_gpu.rs:126-160), exact for regexes.
+ * d_data holds input bytes [base, base + len): the shard's own range
+ * [base, own_end) plus a halo long enough for any match starting before
+ * own_end.  Literal matches starting in the own range are reported; each regex
+ * resumes its find_iter chain at d_cursor[r] (device, one u64 per regex,
+ * stream offsets; pass base when nothing before the shard reaches into it) and
+ * decides every match starting before own_end, after which d_cursor[r] holds
+ * max(end of its last match, own_end): the next shard's incoming cursor.
+ * Offsets in d_out are stream offsets.  Asynchronous on `stream`. */
+ws_status ws_scan_shard(ws_matcher* m, const uint8_t* d_data, uint64_t len, uint64_t base,
+                        uint64_t own_end, uint64_t* d_cursor, ws_match64* d_out, uint64_t cap,
+                        uint64_t* d_count, void* stream, ws_error_info* err);
+
 /* StreamPipeline (core/src/pipeline.rs:87-153) with state carry: feed bytes in
  * pieces of any size; matches are reported once, with global 64-bit offsets,
  * as soon as they are final.  The union over all feeds plus end equals ws_scan
@@ -254,6 +268,8 @@ typedef struct {
   uint64_t last_kcandidates;
   double last_kernel_ms[8];      /* literal, walk, propose, fixup, reverse, resolve, plain, total */
   uint32_t last_launches;
+  uint32_t max_literal_len;      /* longest literal (bytes) */
+  int64_t max_regex_len;         /* longest regex match (bytes), -1 unbounded */
 } ws_matcher_info;
 ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
 

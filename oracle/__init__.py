@@ -40,6 +40,8 @@ def lib():
         L.or_regex_free.argtypes = [ctypes.c_void_p]
         L.or_regex_nullable.restype = ctypes.c_int
         L.or_regex_nullable.argtypes = [ctypes.c_void_p]
+        L.or_regex_maxlen.restype = ctypes.c_longlong
+        L.or_regex_maxlen.argtypes = [ctypes.c_void_p]
         L.or_regex_literal.restype = ctypes.c_int
         L.or_regex_literal.argtypes = [ctypes.c_char_p, u8p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.or_regex_pathological.restype = ctypes.c_int
@@ -133,6 +135,11 @@ class Regex:
     @property
     def nullable(self) -> bool:
         return bool(lib().or_regex_nullable(self.h))
+
+    @property
+    def maxlen(self) -> int:
+        """Longest match in bytes, -1 when unbounded."""
+        return int(lib().or_regex_maxlen(self.h))
 
     def find_iter(self, data) -> list[tuple[int, int]]:
         d, pd = _u8(data)

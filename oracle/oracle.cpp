@@ -790,6 +790,7 @@ or_regex* or_regex_new(const char* pattern, char* err, size_t err_cap) {
 
 void or_regex_free(or_regex* r) { delete r; }
 int or_regex_nullable(const or_regex* r) { return r->prog.nullable ? 1 : 0; }
+long long or_regex_maxlen(const or_regex* r) { return r->prog.maxlen; }
 
 int or_regex_literal(const char* pattern, uint8_t* out, size_t cap, size_t* out_len) {
   try {

@@ -62,6 +62,8 @@ typedef struct or_regex or_regex;
 or_regex* or_regex_new(const char* pattern, char* err, size_t err_cap);
 void or_regex_free(or_regex* r);
 int or_regex_nullable(const or_regex* r);
+/* Longest match in bytes, -1 when unbounded. */
+long long or_regex_maxlen(const or_regex* r);
 /* 1 if the regex would be demoted to a literal; the bytes go to out (cap). */
 int or_regex_literal(const char* pattern, uint8_t* out, size_t cap, size_t* out_len);
 /* 1 if pathological (nested repetition under an outer repetition with max>1). */

@@ -71,7 +71,8 @@ class WsMatcherInfo(ctypes.Structure):
                 ("filter_bits", ctypes.c_uint32), ("proposer_top1", ctypes.c_double),
                 ("proposer_top4", ctypes.c_double), ("last_fixup_chunks", ctypes.c_uint64),
                 ("last_chunks", ctypes.c_uint64), ("last_kcandidates", ctypes.c_uint64),
-                ("last_kernel_ms", ctypes.c_double * 8), ("last_launches", ctypes.c_uint32)]
+                ("last_kernel_ms", ctypes.c_double * 8), ("last_launches", ctypes.c_uint32),
+                ("max_literal_len", ctypes.c_uint32), ("max_regex_len", ctypes.c_int64)]
 
 
 # Every symbol of include/warpstate.h, with its ctypes signature.
@@ -101,6 +102,9 @@ SIGNATURES = {
                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(WsErrorInfo)]),
     "ws_scan_device64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                         ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(WsErrorInfo)]),
+    "ws_scan_shard": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                     ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_feed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(WsMatch64),
                                       ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),

@@ -121,6 +121,7 @@ uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t*
     ll.item_end = x.item_end;
     ll.n_items = x.n_items;
     ll.min_end = x.lit_min_end;
+    ll.max_start = x.lit_max_start;
     launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
     launches += 2;
   }
@@ -250,6 +251,7 @@ ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_co
     m->info.n_literals = t->n_literals;
     m->info.n_regex = t->n_regex;
     m->info.filter_q = m->lit.gram_len;
+    m->info.max_literal_len = m->max_literal_len;
     m->info.filter_period = m->lit.period;
     m->info.filter_bits = m->lit.table_bits;
     regex_fill_info(m->rx, m->info);

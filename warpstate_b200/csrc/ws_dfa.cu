@@ -608,7 +608,7 @@ __global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
   const uint32_t pid = t.pid[r];
   // stream scans: resume at the regex's cursor, decide only starts before the
   // frontier (both in stream offsets; the buffer starts at p.base <= cursor)
-  uint64_t last_end = p.cursor64 ? p.cursor64[r] - p.base : 0;
+  uint64_t last_end = (p.cursor64 && p.cursor64[r] > p.base) ? p.cursor64[r] - p.base : 0;
   const uint64_t limit = p.cursor64 ? p.frontier - p.base : ~0ull;
   for (uint32_t j = a; j < b; ++j) {
     uint32_t e = p.lfend[j];
@@ -1115,6 +1115,7 @@ void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
   info.max_classes = P.max_classes;
   info.proposer_top1 = P.top1;
   info.proposer_top4 = P.top4;
+  info.max_regex_len = P.n_regex ? P.max_len : 0;
 }
 
 namespace {

@@ -154,6 +154,8 @@ struct LiteralLaunch {
   uint32_t n_items = 0;
   // Stream scans: only matches ending after this offset are new.
   uint64_t min_end = 0;
+  // Shard scans: only matches starting before this offset are this shard's.
+  uint64_t max_start = ~0ull;
 };
 
 // Exclusive end of the item that contains offset `s` (the first end above s).

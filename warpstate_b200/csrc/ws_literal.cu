@@ -64,7 +64,8 @@ struct LitArgs {
   const uint32_t* item_end;  // batch: ascending item ends (n_items), else null
   uint32_t n_items;
   uint64_t min_end;          // stream: matches ending at or before it were reported
-  uint32_t gram_len;         // stage-1 gram bytes: 4, 8 or 16 (8 and 16 with P = 4)
+  uint64_t max_start;        // shard: matches starting at or after it belong to the next shard
+  uint32_t gram_len;        // stage-1 gram bytes: 4, 8 or 16 (8 and 16 with P = 4)
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
 };
@@ -89,6 +90,7 @@ __device__ __forceinline__ uint4 load_vec(const uint8_t* data, uint64_t len, uin
 
 // The reference's per-position probe and exact verify (stage 2).
 __device__ void verify_position(const LitArgs& a, uint64_t s) {
+  if (s >= a.max_start) return;
   uint32_t h = 2166136261u;
   uint64_t rem = a.len - s;
   uint32_t maxp = (uint32_t)(rem < a.window ? rem : a.window);
@@ -379,6 +381,7 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.item_end = l.item_end;
   a.n_items = l.n_items;
   a.min_end = l.min_end;
+  a.max_start = l.max_start;
   a.gram_len = plan.gram_len;
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;

@@ -49,6 +49,7 @@ struct ScanExtras {
   uint32_t n_items = 0;
   bool literals = true;                // run the literal pipeline
   uint64_t lit_min_end = 0;            // stream: literal matches ending later are new
+  uint64_t lit_max_start = ~0ull;      // shard: literal matches starting earlier are this shard's
   unsigned long long* cursor = nullptr;  // stream: per-regex find_iter positions (device)
   uint64_t base = 0, frontier = 0;     // stream: window offset and decision frontier
 };

@@ -312,6 +312,45 @@ ws_status ws_scan_device64(ws_matcher* m, const uint8_t* d_data, uint64_t len, w
   });
 }
 
+ws_status ws_scan_shard(ws_matcher* m, const uint8_t* d_data, uint64_t len, uint64_t base, uint64_t own_end,
+                        uint64_t* d_cursor, ws_match64* d_out, uint64_t cap, uint64_t* d_count, void* stream,
+                        ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m || !d_count || (len && !d_data) || (m->rx.n_regex && !d_cursor))
+      raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    if (((uintptr_t)d_data & 15) != 0) raise(WS_ERR_INVALID_ARGUMENT, "device input must be 16-byte aligned");
+    if (own_end < base || own_end > base + len) raise(WS_ERR_INVALID_ARGUMENT, "own range outside the shard buffer");
+    if (len > 0xFFFFFFFFull - 64)
+      raise(WS_ERR_INPUT_TOO_LARGE, "shard buffer is too large for 32-bit offsets", 0, len, 0xFFFFFFFFull - 64);
+    check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+    ScratchLease s(m);
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    check_cuda(cudaStreamWaitEvent(cs, s->busy, 0), "wait");
+    auto* total = reinterpret_cast<unsigned long long*>(d_count);
+    check_cuda(cudaMemsetAsync(total, 0, 8, cs), "memset count");
+    if (len == 0 || own_end == base) {
+      check_cuda(cudaEventRecord(s->busy, cs), "event");
+      return;
+    }
+    const uint64_t scap = std::max<uint64_t>(cap, 1);
+    ensure(s->out, scap * sizeof(ws_match));
+    ensure(s->aux, 256);
+    auto* step_count = s->aux.as<unsigned long long>();
+    ScanExtras x;
+    x.literals = m->lit.n_literals != 0;
+    x.lit_max_start = own_end - base;
+    x.cursor = m->rx.n_regex ? reinterpret_cast<unsigned long long*>(d_cursor) : nullptr;
+    x.base = base;
+    x.frontier = own_end;
+    uint32_t launches = enqueue_scan(m, *s, cs, d_data, len, s->out.as<ws_match>(), scap, step_count, x);
+    widen_kernel<<<1, 1024, 0, cs>>>(s->out.as<ws_match>(), step_count, scap, base, d_out, cap, total);
+    check_cuda(cudaGetLastError(), "widen_kernel");
+    check_cuda(cudaEventRecord(s->busy, cs), "event");
+    std::lock_guard<std::mutex> g(m->info_mu);
+    m->info.last_launches = launches + 1;
+  });
+}
+
 void ws_stream_destroy(ws_stream* st) {
   if (!st) return;
   cudaSetDevice(st->m->ctx->device);
