@@ -355,7 +355,7 @@ def main():
     # roofline of the dominant kernel
     peak, peak_kind = load_peaks()
     has_regex = any(k == 1 for k, _ in wl.patterns)
-    kidx, kname = (1, "dfa_walk") if has_regex else (0, "literal_scan")
+    kidx, kname = (1, "dfa_walk_kernel") if has_regex else (0, "literal_filter_kernel")
     kms = statistics.mean(i["last_kernel_ms"][kidx] for i in infos) if infos else None
     alg_bytes = n_bytes + 12 * count + (16 * n_items if batch else 0)
     achieved = alg_bytes / (kms * 1e-3) / 1e9 if kms else None
