@@ -186,12 +186,18 @@ def run_reference(args, rank):
 
 
 # ------------------------------------------------------------------ ours
-def build_matchers(ws, wl, config):
+def build_matchers(ws, wl, config, walk_chunk=None, proposer=True, dfa_max_states=None):
     ps = ws.PatternSet.builder()
     for kind, p in wl.patterns:
         ps = ps.literal_bytes(p) if kind == 0 else ps.regex(p.decode())
     ps = ps.build()
     cfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_SPECULATIVE)
+    if walk_chunk:
+        cfg.walk_chunk(walk_chunk)
+    if dfa_max_states:
+        cfg.dfa_max_states(dfa_max_states)
+    if not proposer:
+        cfg.proposer(ws.PROPOSER_NONE)
     m = ws.GpuMatcher.with_config(ps, cfg)
     plain = None
     has_regex = any(k == 1 for k, _ in wl.patterns)
@@ -199,7 +205,7 @@ def build_matchers(ws, wl, config):
         pcfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_PLAIN)
         plain = ws.GpuMatcher.with_config(ps, pcfg)
     train_s = None
-    if has_regex:
+    if has_regex and proposer:
         # the proposer learns from a separately seeded 256 MiB corpus of the same distribution
         t0 = time.perf_counter()
         corpus = W.dna_training_corpus() if config == "dna" else W.regex_training_corpus()
@@ -220,6 +226,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--walk-chunk", type=int, default=None, help="speculative walk chunk bytes")
+    ap.add_argument("--no-proposer", action="store_true", help="guess the unanchored start at every boundary")
+    ap.add_argument("--dfa-max-states", type=int, default=None, help="states per merged group DFA")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -242,7 +251,8 @@ def main():
     import warpstate_b200 as ws
 
     wl = make_workload(args.config, args.size)
-    m, plain, train_s = build_matchers(ws, wl, args.config)
+    m, plain, train_s = build_matchers(ws, wl, args.config, args.walk_chunk, not args.no_proposer,
+                                       args.dfa_max_states)
     if args.no_plain:
         plain = None
     stream = torch.cuda.current_stream()
