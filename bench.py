@@ -204,15 +204,16 @@ def build_matchers(ws, wl, config, walk_chunk=None, proposer=True, dfa_max_state
     if has_regex and config in ("regex", "batch", "dna"):
         pcfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_PLAIN)
         plain = ws.GpuMatcher.with_config(ps, pcfg)
-    train_s = None
-    if has_regex and proposer:
-        # the proposer learns from a separately seeded 256 MiB corpus of the same distribution
-        t0 = time.perf_counter()
+    tune = None
+    if has_regex:
+        # a separately seeded 256 MiB corpus of the same distribution: the
+        # autotuner picks group size, hot rows, proposer and chunk on it (knobs
+        # given on the command line stay fixed)
         corpus = W.dna_training_corpus() if config == "dna" else W.regex_training_corpus()
-        m.train_proposer(corpus)
-        train_s = time.perf_counter() - t0
+        flags = (0 if dfa_max_states else ws.GpuMatcher.TUNE_GROUPS) | (0 if walk_chunk else ws.GpuMatcher.TUNE_CHUNK)
+        tune = m.tune(corpus, flags=flags)
         del corpus
-    return m, plain, train_s
+    return m, plain, tune
 
 
 def main():
@@ -251,7 +252,7 @@ def main():
     import warpstate_b200 as ws
 
     wl = make_workload(args.config, args.size)
-    m, plain, train_s = build_matchers(ws, wl, args.config, args.walk_chunk, not args.no_proposer,
+    m, plain, tune = build_matchers(ws, wl, args.config, args.walk_chunk, not args.no_proposer,
                                        args.dfa_max_states)
     if args.no_plain:
         plain = None
@@ -448,7 +449,7 @@ def main():
                          "speedup_vs_plain": round(value / plain_gbs, 3) if plain_gbs else None,
                          "plain_ms_per_step": round(plain_ms, 4) if plain_ms else None,
                          "proposer_top1": last["proposer_top1"], "proposer_top4": last["proposer_top4"],
-                         "proposer_train_s": round(train_s, 2) if train_s else None,
+                         "tune": tune,
                          "fixup_chunks": last["last_fixup_chunks"], "chunks": last["last_chunks"],
                          "groups": last["n_groups"], "states": last["total_states"],
                          "phase_ms": [round(x, 4) for x in last["last_kernel_ms"]]}

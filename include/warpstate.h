@@ -257,6 +257,28 @@ void ws_stream_destroy(ws_stream* s);
 ws_status ws_matcher_train_proposer(ws_matcher* m, const uint8_t* corpus, uint64_t len, uint64_t seed,
                                     ws_error_info* err);
 
+/* Autotuner of the regex walk on a sample corpus (no counterpart in the
+ * reference).  With WS_TUNE_GROUPS it rebuilds the merged group DFAs at
+ * several size limits and keeps the plan whose scan of the corpus is fastest;
+ * it then learns the hot-row placement from the corpus, trains the proposer
+ * (when the config enables it) and, with WS_TUNE_CHUNK, times the speculative
+ * walk at several chunk sizes with and without the proposer and keeps the
+ * fastest.  Every choice gives the same matches; only speed differs.  The
+ * corpus is host memory of at least 64 KiB; the timings scan it tiled to 1 GiB.
+ * Call it before scanning, not while scans run. */
+enum { WS_TUNE_GROUPS = 1, WS_TUNE_CHUNK = 2 };
+typedef struct {
+  uint32_t dfa_max_states, n_groups, walk_chunk, proposer_used;
+  uint32_t group_candidates[4];      /* size limits tried (0: unused slot) */
+  double group_ms[4];                /* corpus scan time per candidate, ms */
+  uint32_t chunk_candidates[4];      /* walk chunks tried (0: unused slot) */
+  double chunk_ms[4][2];             /* [chunk][0: no proposer, 1: proposer], ms */
+  double proposer_top1, proposer_top4;
+  double tune_seconds;
+} ws_tune_report;
+ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint64_t len, uint64_t seed,
+                          uint32_t flags, ws_tune_report* report, ws_error_info* err);
+
 /* Introspection for tests and the benchmark. */
 typedef struct {
   uint32_t n_literals, n_regex, n_groups;

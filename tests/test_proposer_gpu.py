@@ -49,3 +49,28 @@ def test_proposer_training_and_exact_scan():
     # the plain kernel agrees as well
     pm = ws.GpuMatcher.with_config(ps, ws.AutoMatcherConfig().regex_mode(ws.REGEX_PLAIN))
     assert np.array_equal(pm.scan_array(wl.data), exp)
+
+
+def test_autotuner_keeps_matches_exact():
+    # the tuner re-plans the group DFAs, re-ranks hot rows, trains the
+    # proposer and picks a walk chunk; whatever it picks, matches are exact
+    import warpstate_b200 as ws
+    wl = w.regex(size=8 << 20, n=150, seed=17)
+    corpus = w.fill_markov(16 << 20, w.PRINTABLE, 17 * 1000 + 77, 17 * 1000 + 4)
+    b = ws.PatternSet.builder()
+    for _, p in wl.patterns:
+        b = b.regex(p.decode())
+    m = ws.GpuMatcher.with_config(b.build(), ws.AutoMatcherConfig().regex_mode(ws.REGEX_SPECULATIVE))
+    rep = m.tune(corpus)
+    assert rep["dfa_max_states"] in rep["groups_tried"]
+    assert rep["walk_chunk"] in rep["chunks_tried"]
+    assert rep["n_groups"] == m.info()["n_groups"] >= 1
+    exp = oracle.scan_patterns(wl.patterns, wl.data)
+    assert len(exp) > 100
+    assert np.array_equal(m.scan_array(wl.data), exp)
+    # every candidate plan scans exactly too: pin each group size and chunk
+    for states in rep["groups_tried"]:
+        c = ws.AutoMatcherConfig().regex_mode(ws.REGEX_SPECULATIVE).dfa_max_states(states).walk_chunk(16384)
+        mm = ws.GpuMatcher.with_config(b.build(), c)
+        mm.tune(corpus, flags=0)
+        assert np.array_equal(mm.scan_array(wl.data), exp), states

@@ -488,6 +488,25 @@ class GpuMatcher:
         i = self.info()
         return {"top1": i["proposer_top1"], "top4": i["proposer_top4"]}
 
+    TUNE_GROUPS = 1
+    TUNE_CHUNK = 2
+
+    def tune(self, corpus, seed: int = 0x5EED, flags: int = 3) -> dict:
+        """Autotunes the regex walk on `corpus` (same distribution as the
+        inputs): group DFA size, hot-row placement, proposer and walk chunk,
+        each chosen by timing scans on the device.  Matches never change."""
+        ptr, n, keep = _buffer(corpus)
+        rep = N.WsTuneReport()
+        _call(N.lib().ws_matcher_tune, self._h, ptr, n, seed, flags, ctypes.byref(rep))
+        del keep
+        return {"dfa_max_states": rep.dfa_max_states, "n_groups": rep.n_groups, "walk_chunk": rep.walk_chunk,
+                "proposer_used": bool(rep.proposer_used),
+                "groups_tried": {int(c): round(m, 4) for c, m in zip(rep.group_candidates, rep.group_ms) if c},
+                "chunks_tried": {int(c): [round(x, 4) for x in rep.chunk_ms[k]]
+                                 for k, c in enumerate(rep.chunk_candidates) if c},
+                "proposer_top1": rep.proposer_top1, "proposer_top4": rep.proposer_top4,
+                "tune_seconds": round(rep.tune_seconds, 2)}
+
     def regex_candidates(self, data, mode: int) -> np.ndarray:
         ptr, n, keep = _buffer(data)
         cap = max(int(self.config.c.max_matches), 1) * 4

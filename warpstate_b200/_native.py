@@ -75,6 +75,14 @@ class WsMatcherInfo(ctypes.Structure):
                 ("max_literal_len", ctypes.c_uint32), ("max_regex_len", ctypes.c_int64)]
 
 
+class WsTuneReport(ctypes.Structure):
+    _fields_ = [("dfa_max_states", ctypes.c_uint32), ("n_groups", ctypes.c_uint32), ("walk_chunk", ctypes.c_uint32),
+                ("proposer_used", ctypes.c_uint32), ("group_candidates", ctypes.c_uint32 * 4),
+                ("group_ms", ctypes.c_double * 4), ("chunk_candidates", ctypes.c_uint32 * 4),
+                ("chunk_ms", (ctypes.c_double * 2) * 4), ("proposer_top1", ctypes.c_double),
+                ("proposer_top4", ctypes.c_double), ("tune_seconds", ctypes.c_double)]
+
+
 # Every symbol of include/warpstate.h, with its ctypes signature.
 SIGNATURES = {
     "ws_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),
@@ -113,7 +121,9 @@ SIGNATURES = {
     "ws_stream_destroy": (None, [ctypes.c_void_p]),
     "ws_matcher_train_proposer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                                  ctypes.POINTER(WsErrorInfo)]),
-    "ws_matcher_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatcherInfo)]),
+    "ws_matcher_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                       ctypes.c_uint32, ctypes.POINTER(WsTuneReport), ctypes.POINTER(WsErrorInfo)]),
+    "ws_matcher_get_info":(ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatcherInfo)]),
     "ws_regex_candidates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
                                            ctypes.POINTER(WsMatch), ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),
     "ws_status_name": (ctypes.c_char_p, [ctypes.c_int]),

@@ -242,8 +242,11 @@ ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_co
     if (cfg) m->cfg = *cfg; else ws_config_default(&m->cfg);
     m->n_patterns = t->n_patterns;
     m->is_regex.assign(t->n_patterns, 0);
-    for (uint32_t r = 0; r < t->n_regex; ++r)
+    for (uint32_t r = 0; r < t->n_regex; ++r) {
       if (t->regex_pattern_ids[r] < t->n_patterns) m->is_regex[t->regex_pattern_ids[r]] = 1;
+      m->rx_src.emplace_back(t->regex_sources[r]);
+      m->rx_ids.push_back(t->regex_pattern_ids[r]);
+    }
     for (uint32_t i = 0; i < t->n_literals; ++i) m->max_literal_len = std::max(m->max_literal_len, t->offsets[2 * i + 1]);
     std::memset(&m->info, 0, sizeof(m->info));
     plan_literals(*t, m->lit);

@@ -601,26 +601,40 @@ __global__ void k_lf_kernel(DevTables t, ScanPtrs p, uint32_t n_regex) {
 
 // find_iter chain per regex: leftmost candidate start with its leftmost-first
 // end, then the next candidate at or after that end.
+// One warp per regex: the warp loads 32 sorted candidates at a time and picks
+// the chain's next match among them with a ballot (the first candidate whose
+// start is at or after the current end), so the serial part is one ballot per
+// reported match.
 __global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= t.n_regex) return;
+  const uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (r >= t.n_regex) return;  // whole warps exit together
   const uint32_t a = p.offs[r], b = p.offs[r + 1];
   const uint32_t pid = t.pid[r];
   // stream scans: resume at the regex's cursor, decide only starts before the
   // frontier (both in stream offsets; the buffer starts at p.base <= cursor)
   uint64_t last_end = (p.cursor64 && p.cursor64[r] > p.base) ? p.cursor64[r] - p.base : 0;
   const uint64_t limit = p.cursor64 ? p.frontier - p.base : ~0ull;
-  for (uint32_t j = a; j < b; ++j) {
-    uint32_t e = p.lfend[j];
-    if (e == 0xFFFFFFFFu) continue;
-    uint32_t s = p.starts[j];
-    if (s < last_end) continue;
-    if (s >= limit) break;
-    unsigned long long idx = atomicAdd(p.out_counter, 1ull);
-    if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, e};
-    last_end = e;
+  for (uint32_t j0 = a; j0 < b; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const bool in = j < b;
+    const uint32_t e = in ? p.lfend[j] : 0xFFFFFFFFu;
+    const uint32_t s = in ? p.starts[j] : 0xFFFFFFFFu;
+    const bool past = in && (uint64_t)s >= limit;
+    while (true) {
+      const bool ok = in && e != 0xFFFFFFFFu && (uint64_t)s >= last_end && !past;
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
+      if (!m) break;
+      const int k = __ffs(m) - 1;
+      if ((int)lane == k) {
+        unsigned long long idx = atomicAdd(p.out_counter, 1ull);
+        if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, e};
+      }
+      last_end = __shfl_sync(0xFFFFFFFFu, e, k);
+    }
+    if (__any_sync(0xFFFFFFFFu, past)) break;  // sorted: every later start is past too
   }
-  if (p.cursor64) p.cursor64[r] = max(p.base + last_end, p.frontier);
+  if (p.cursor64 && lane == 0) p.cursor64[r] = max(p.base + last_end, p.frontier);
 }
 
 // Copies K candidates into a ws_match buffer (diagnostics).
@@ -735,7 +749,7 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
 }  // namespace
 
 // ------------------------------------------------------------------- host plan
-RegexPlan::~RegexPlan() { proposer_destroy(proposer); }
+void ProposerDeleter::operator()(Proposer* p) const { proposer_destroy(p); }
 
 namespace {
 
@@ -1147,7 +1161,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   k_scatter_kernel<<<hg, 256, 0, st>>>(p);
   k_sort_kernel<<<(unsigned)std::min<uint32_t>(P.n_regex, 4096), 512, 0, st>>>(p, P.n_regex);
   k_lf_kernel<<<sm_count * 8, 128, 0, st>>>(t, p, P.n_regex);
-  k_chain_kernel<<<(P.n_regex + 127) / 128, 128, 0, st>>>(t, p);
+  k_chain_kernel<<<(P.n_regex + 3) / 4, 128, 0, st>>>(t, p);  // a warp per regex
   check_cuda(cudaGetLastError(), "resolution kernels");
   launches += 6;
   finalize_kernel<<<1, 1, 0, st>>>(p);

@@ -44,6 +44,12 @@ struct GroupDev {
   uint32_t pad;
 };
 
+struct Proposer;
+// Frees a trained proposer (ws_proposer.cu).
+struct ProposerDeleter {
+  void operator()(Proposer* p) const;
+};
+
 struct RegexPlan {
   uint32_t n_regex = 0;
   uint32_t n_groups = 0;
@@ -64,14 +70,13 @@ struct RegexPlan {
   std::vector<std::vector<uint32_t>> gregex;
   std::vector<uint32_t> nhot_u, nhot_a;
   // proposer
-  struct Proposer* proposer = nullptr;   // trained by ws_matcher_train_proposer
+  std::unique_ptr<Proposer, ProposerDeleter> proposer;  // trained by ws_matcher_train_proposer
   bool use_proposer = true;               // config: MLP guesses (else the unanchored start)
   double top1 = 0, top4 = 0, start_rate = 0;
   uint32_t walk_chunk = 4096;            // speculative chunk bytes (multiple of 256)
   // last scan
   uint64_t last_chunks = 0, last_fixup = 0, last_k = 0;
   uint32_t last_launches = 0;
-  ~RegexPlan();
 };
 
 struct RegexLaunch {

@@ -7,6 +7,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/warpstate.h"
@@ -66,6 +67,12 @@ struct DeviceBuffer {
   DeviceBuffer() = default;
   DeviceBuffer(const DeviceBuffer&) = delete;
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    std::swap(ptr, o.ptr);
+    std::swap(bytes, o.bytes);
+    return *this;
+  }
   ~DeviceBuffer();
   void alloc(size_t n);
   void upload(const void* src, size_t n);

@@ -75,6 +75,9 @@ struct ws_matcher {
   uint32_t n_patterns = 0;
   uint32_t max_literal_len = 0;
   std::vector<uint8_t> is_regex;  // per pattern id
+  // regex sources and ids, kept so that the autotuner can re-plan the groups
+  std::vector<std::string> rx_src;
+  std::vector<uint32_t> rx_ids;
   std::mutex pool_mu;
   std::vector<std::unique_ptr<ws::Scratch>> pool;
   std::mutex info_mu;

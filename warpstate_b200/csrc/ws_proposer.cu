@@ -674,8 +674,7 @@ void proposer_train(RegexPlan& P, const uint8_t* d_corpus, uint64_t len, uint64_
     stats->steps = steps;
     stats->final_loss = last_loss;
   }
-  proposer_destroy(P.proposer);
-  P.proposer = guard.release();
+  P.proposer.reset(guard.release());
 }
 
 uint32_t proposer_predict(Proposer& p, const uint8_t* data, uint64_t len, uint64_t chunk, uint64_t n_chunks,
