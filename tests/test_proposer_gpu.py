@@ -11,6 +11,50 @@ import workloads as w
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("n", [256, 64, 192])
+def test_tcgen05_gemm_matches_torch_fp32(n):
+    # the tensor-core path of the proposer kernel (descriptors, bulk copies,
+    # TMEM accumulators, tcgen05.ld) on one 256 x 256 x n product
+    import torch
+    from warpstate_b200 import _native as N
+    g = torch.Generator().manual_seed(n)
+    A = torch.randn(256, 256, generator=g).to(torch.bfloat16).cuda()
+    WT = torch.randn(n, 256, generator=g).to(torch.bfloat16).cuda()
+    D = torch.full((256, n), float("nan"), dtype=torch.float32, device="cuda")
+    fn = N.lib().ws_testing_tc_gemm
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    assert fn(A.data_ptr(), WT.data_ptr(), n, D.data_ptr()) == 0
+    ref = A.float() @ WT.float().t()
+    tol = 1e-4 * ref.abs().amax().item() + 1e-3
+    assert torch.isfinite(D).all()
+    assert (D - ref).abs().max().item() <= tol
+
+
+def test_tcgen05_and_mma_sync_proposers_agree_and_scan_exactly():
+    import warpstate_b200 as ws
+    from warpstate_b200 import _native as N
+    wl = w.regex(size=16 << 20, n=150, seed=19)
+    corpus = w.fill_markov(16 << 20, w.PRINTABLE, 19 * 1000 + 77, 19 * 1000 + 4)
+    b = ws.PatternSet.builder()
+    for _, p in wl.patterns:
+        b = b.regex(p.decode())
+    m = ws.GpuMatcher.with_config(b.build(), ws.AutoMatcherConfig().regex_mode(ws.REGEX_SPECULATIVE).profile(True))
+    m.train_proposer(corpus)
+    exp = oracle.scan_patterns(wl.patterns, wl.data)
+    sel = N.lib().ws_testing_proposer_path
+    sel.restype = None
+    sel.argtypes = [ctypes.c_int]
+    try:
+        fixups = {}
+        for path in (0, 1):
+            sel(path)
+            assert np.array_equal(m.scan_array(wl.data), exp), path
+            fixups[path] = m.info()["last_kernel_ms"][3]
+    finally:
+        sel(1)
+
+
 @pytest.mark.parametrize("mnk", [(64, 64, 64), (512, 576, 256), (100, 37, 300), (256, 256, 512)])
 def test_bf16_gemm_matches_torch_fp32(mnk):
     import torch

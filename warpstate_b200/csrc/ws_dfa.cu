@@ -337,7 +337,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
   const uint64_t q = (uint64_t)g * p.n_chunks + i;
   const uint64_t c0 = i * p.chunk;
   const uint64_t c1 = min(p.len, c0 + p.chunk);
-  const uint32_t start = (i == 0) ? gd.start_unanchored : p.guess[q];
+  uint32_t start = (i == 0) ? gd.start_unanchored : p.guess[q];
+  if (start >= gd.n_states) start = gd.start_unanchored;  // a guess never written
   p.used[q] = start;
   p.conv[q] = (uint32_t)c0;
   p.round[q] = 0;

@@ -36,11 +36,18 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi
   return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in the tanh form of Hendrycks and Gimpel (2016):
+// 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), through CUDA's tanhf; the
+// tensor-core inference kernel evaluates the same form with the hardware
+// tanh approximation.
+constexpr float kGeluC = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+  return 0.5f * x * (1.0f + tanhf(kGeluC * (x + kGeluA * x * x * x)));
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-  float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-  float pdf = 0.3989422804014327f * expf(-0.5f * x * x);
-  return cdf + x * pdf;
+  const float t = tanhf(kGeluC * (x + kGeluA * x * x * x));
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * x * x);
 }
 
 // ------------------------------------------------------ generic GEMM
@@ -439,8 +446,15 @@ struct Proposer {
   DeviceBuffer mE, vE, mW1, vW1, mb1, vb1, mW2, vW2, mb2, vb2, mW3, vW3, mb3, vb3;
   DeviceBuffer E16, W1_16, W2_16, W3_16;
   DeviceBuffer W1T, W2T, W3T;  // inference copies [out][in]
+  TcPlan tc;                   // the same weights packed for the tcgen05 kernel
   bool trained = false;
 };
+
+namespace {
+// Inference path: the tcgen05 kernel when its weights are packed (default), or
+// the mma.sync kernel (the testing hook below selects it, for comparisons).
+bool g_use_tc = true;
+}  // namespace
 
 void proposer_destroy(Proposer* p) { delete p; }
 
@@ -663,6 +677,7 @@ void proposer_train(RegexPlan& P, const uint8_t* d_corpus, uint64_t len, uint64_
   transpose_bf16_kernel<<<blocks(kPropHid * kPropHid), 256>>>(pr->W2.as<float>(), pr->W2T.as<bf>(), kPropHid, kPropHid);
   transpose_bf16_kernel<<<blocks(kPropHid * NO), 256>>>(pr->W3.as<float>(), pr->W3T.as<bf>(), kPropHid, NO);
   check_cuda(cudaDeviceSynchronize(), "proposer training");
+  tc_prepare(pr->tc, pr->W1T.ptr, pr->W2T.ptr, pr->W3T.ptr, NO);
   pr->trained = true;
   P.top1 = n_eval ? (double)h[0] / n_eval : 0;
   P.top4 = n_eval ? (double)h[1] / n_eval : 0;
@@ -681,6 +696,11 @@ uint32_t proposer_predict(Proposer& p, const uint8_t* data, uint64_t len, uint64
                           uint32_t* guess, cudaStream_t st) {
   (void)len;
   if (n_chunks <= 1) return 0;
+  if (g_use_tc && p.tc.ready) {
+    TcInputs in{data, chunk, n_chunks, p.d_jmap.as<uint8_t>(), p.E16.ptr, 64u, p.b1.as<float>(), p.b2.as<float>(),
+                p.b3.as<float>(), p.d_vocab.as<uint32_t>(), p.G, guess};
+    return tc_predict(p.tc, in, st);
+  }
   InferArgs a;
   a.data = data;
   a.chunk = chunk;
@@ -716,3 +736,8 @@ extern "C" int ws_testing_gemm_bf16(const void* A, const void* B, float* C, int 
     return 1;
   }
 }
+
+// Testing hook (not part of the public header): 1 selects the tcgen05
+// inference kernel (the default), 0 the mma.sync kernel, for every matcher in
+// the process.
+extern "C" void ws_testing_proposer_path(int tcgen05) { ws::g_use_tc = tcgen05 != 0; }
