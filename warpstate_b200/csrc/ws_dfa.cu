@@ -8,6 +8,7 @@
 #include <numeric>
 
 #include "ws_dfa.h"
+#include "ws_async.h"
 #include "ws_proposer.h"
 
 namespace cg = cooperative_groups;
@@ -189,9 +190,11 @@ constexpr uint32_t kTrapByte = kImgBlock * 4;
 constexpr uint32_t S_SLOW = 0x80000000u, S_MATCH = 0x40000000u, S_COLD = 0x20000000u, S_TRAP = 0x10000000u,
                    S_DEAD = 0x08000000u, S_ROW = 0x07FFFFFFu;
 
+// Shared memory of a walk block: [hot image][byte classes, 256 B][mbarrier, 16 B].
 __host__ __device__ constexpr size_t hot_smem_bytes(uint32_t rows) {
-  return rows ? (size_t)kImgWords * 4 + 256 : 256;
+  return (rows ? (size_t)kImgWords * 4 : 0) + 256 + 16;
 }
+__host__ __device__ constexpr size_t cls_offset(uint32_t rows) { return rows ? (size_t)kImgWords * 4 : 0; }
 
 __host__ __device__ __forceinline__ uint32_t slot_word(uint32_t r) { return (1 + (r >> 5)) * kImgBlock + (r & 31); }
 
@@ -215,15 +218,33 @@ __device__ __forceinline__ uint32_t state_of(uint32_t row, uint32_t first, uint3
 }
 
 // Stages the image (when the group has one) and the class map.
+// Stages a group's hot-row image (224 KiB) and byte-class map into shared
+// memory with two bulk (TMA) copies completing on one mbarrier; a wait that
+// runs out (it should not) falls back to copying with the threads.
 __device__ __forceinline__ void stage_hot(const DevTables& t, uint32_t g, uint32_t off, uint32_t rows,
                                           uint32_t* img, uint8_t* cls_s) {
-  if (rows) {
-    const uint4* src = reinterpret_cast<const uint4*>(t.hot + off);
-    uint4* dst = reinterpret_cast<uint4*>(img);
-    for (uint32_t k = threadIdx.x; k < kImgWords / 4; k += blockDim.x) dst[k] = __ldg(src + k);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(cls_s + 256);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
   }
-  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cls_s[k] = t.cls[g * 256 + k];
   __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar, (rows ? kImgWords * 4 : 0) + 256);
+    if (rows) bulk_copy_g2s(img, t.hot + off, kImgWords * 4, bar);
+    bulk_copy_g2s(cls_s, t.cls + g * 256, 256, bar);
+  }
+  bool ok = false;
+  for (uint32_t it = 0; it < (1u << 22) && !ok; ++it) ok = mbar_try(bar, 0);
+  if (!__syncthreads_and(ok)) {
+    if (rows) {
+      const uint4* src = reinterpret_cast<const uint4*>(t.hot + off);
+      uint4* dst = reinterpret_cast<uint4*>(img);
+      for (uint32_t k = threadIdx.x; k < kImgWords / 4; k += blockDim.x) dst[k] = __ldg(src + k);
+    }
+    for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cls_s[k] = t.cls[g * 256 + k];
+    __syncthreads();
+  }
 }
 
 // Slow path of one transition: handles match / cold / dead and returns false
@@ -253,21 +274,6 @@ __device__ __forceinline__ bool slow_step(uint32_t w, uint32_t b, uint32_t& st, 
   return true;
 }
 
-// Out-of-line slow path of the unanchored walk (keeps the unrolled fast loop
-// small); returns the row of a match state entered, or 0xFFFFFFFF.
-struct SlowOut {
-  uint32_t st, cold_row, m_row;
-};
-
-__device__ __noinline__ SlowOut walk_slow(uint32_t w, uint32_t b, uint32_t st, uint32_t cold_row, uint32_t rows,
-                                          uint32_t lane4, const uint8_t* cls_s, const uint32_t* tab, uint32_t C) {
-  SlowOut o;
-  slow_step(w, b, st, cold_row, 0, rows, lane4, cls_s, tab, C, o.m_row);
-  o.st = st;
-  o.cold_row = cold_row;
-  return o;
-}
-
 #define WS_STEP_FAST(img, st, b) (*reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(img) + (st) + ((b) << 7)))
 
 // One transition through L2 only (fix-up walks, which are short and rare).
@@ -287,7 +293,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
   const uint32_t g = blockIdx.y;
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
-  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + hot_smem_bytes(gd.ahot_rows) - 256;
+  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.ahot_rows);
   stage_hot(t, g, gd.ahot_off, gd.ahot_rows, img, cls_s);
   const uint32_t* tab = t.fwd + gd.fwd_off;
   const uint32_t* mp = t.mptr + gd.mptr_off;
@@ -327,7 +333,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
   const uint32_t g = blockIdx.x;
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
-  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + hot_smem_bytes(gd.hot_rows) - 256;
+  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.hot_rows);
   stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s);
   const uint64_t i = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
   if (i >= p.n_chunks) return;

@@ -15,7 +15,7 @@
 //      them to the slot's mbarrier, which frees the slot for the next copy;
 //   3. after a GEMM's last commit, all 16 warps read the accumulators back
 //      with tcgen05.ld (warp w reads TMEM lanes 32*(w%4).., one row per
-//      thread, 128 columns per warp group) and apply bias + GELU (CUDA's erff)
+//      thread, 128 columns per warp group) and apply bias + GELU (tanh form)
 //      into the next A operand, or, for the heads, take each group's arg-max
 //      and write the guessed state.
 // Every mbarrier wait is bounded; on a time-out the CTA records an error,
@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "ws_async.h"
 #include "ws_proposer.h"
 
 namespace ws {
@@ -47,8 +48,6 @@ constexpr uint32_t kConstBytes = 2 * 256 * 4 + 256 + 64 * kPropEmb * 2;
 constexpr uint32_t kTcSmem = kABytes + kSlots * kSlotBytes + kBarBytes + kConstBytes;
 constexpr uint32_t kWaitSpins = 1u << 24;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 // Shared-memory matrix descriptor, K-major, no swizzle (layout type 0),
 // descriptor version 1 (sm_100): start >> 4 in bits 0-13, leading byte offset
 // (between the two 8-element K halves of an instruction) >> 4 in 16-29,
@@ -64,22 +63,6 @@ __device__ __forceinline__ uint32_t idesc_bf16(uint32_t n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
 // Bounded wait; false (and the abort flag set) after kWaitSpins polls, or
 // when another thread has aborted.
 __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
@@ -92,12 +75,8 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
 }
 
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
+  mbar_expect_tx(bar, bytes);
+  bulk_copy_g2s(dst, src, bytes, bar);
 }
 
 __device__ __forceinline__ void mma_bf16_ss(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -226,7 +205,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) proposer_tc_kernel(TcArgs a) {
   if (tid == 0) {
     for (uint32_t k = 0; k < 2 * kSlots + 1; ++k) mbar_init(&bars[k], 1);
     *abort = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_init_fence();
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
