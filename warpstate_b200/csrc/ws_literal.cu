@@ -68,11 +68,21 @@ struct LitArgs {
   uint32_t gram_len;        // stage-1 gram bytes: 4, 8 or 16 (8 and 16 with P = 4)
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
+  const uint32_t* big;       // stage-1b gram table (2^kBigBits nibbles, L2), or null
 };
 
 __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint32_t bits) {
   uint32_t h = (gram * 0x9E3779B1u) >> (32 - bits);
   return (tab[h >> 3] >> ((h & 7) << 2)) & 0xFu;
+}
+
+// Stage 1b: a nibble that passed the shared-memory table is checked again in
+// the larger table in L2 (same gram hash, more bits), only where it is
+// non-zero: one predicated load per passing gram.
+__device__ __forceinline__ uint32_t nib_big(const uint32_t* big, uint32_t h_full, uint32_t n) {
+  if (!n) return 0;
+  const uint32_t h = h_full >> (32 - kBigBits);
+  return n & ((__ldg(big + (h >> 3)) >> ((h & 7) << 2)) & 0xFu);
 }
 
 // Loads the 16 bytes of vector v, zero-filling past the end of the input.
@@ -124,56 +134,60 @@ __device__ void verify_position(const LitArgs& a, uint64_t s) {
   }
 }
 
-__device__ __forceinline__ uint32_t nib_long(const uint32_t* tab, uint32_t g0, uint32_t g1, uint32_t g2, uint32_t g3,
-                                             uint32_t gram_len, uint32_t bits) {
-  uint32_t h = long_gram_hash(g0, g1, g2, g3, gram_len, bits);
-  return (tab[h >> 3] >> ((h & 7) << 2)) & 0xFu;
-}
-
 // 16-bit mask of owned positions that may start a literal (stage 1).  w[0..3]
 // are the thread's own words; w[4..7] are the next thread's words (w[4] is
 // needed by the P = 1 and P = 2 layouts and by lane 31, w[5..7] by grams
-// longer than 4 bytes).
-__device__ __forceinline__ uint32_t stage1(const LitArgs& a, const uint32_t* filt, const uint32_t* shortb,
-                                           const uint32_t (&w)[8], uint32_t lane) {
+// longer than 4 bytes).  The layout is a compile-time choice (P = period,
+// G = gram bytes, LONG / SHORT = literals of >= 4 / < 4 bytes present).
+template <int P, int G, bool LONG, bool SHORT>
+__device__ __forceinline__ uint32_t stage1(const uint32_t* filt, const uint32_t* shortb, const uint32_t (&w)[8],
+                                           uint32_t lane, uint32_t bits, const uint32_t* big) {
   uint32_t mask = 0;
-  if (a.has_long) {
-    if (a.gram_len > 4) {
-      // P = 4, grams of 8 or 16 bytes starting at the four aligned words
-      uint32_t n0 = nib_long(filt, w[0], w[1], w[2], w[3], a.gram_len, a.bits);
-      uint32_t n1 = nib_long(filt, w[1], w[2], w[3], w[4], a.gram_len, a.bits);
-      uint32_t n2 = nib_long(filt, w[2], w[3], w[4], w[5], a.gram_len, a.bits);
-      uint32_t n3 = nib_long(filt, w[3], w[4], w[5], w[6], a.gram_len, a.bits);
-      uint32_t n4 = __shfl_down_sync(0xFFFFFFFFu, n0, 1);
-      if (lane == 31) n4 = nib_long(filt, w[4], w[5], w[6], w[7], a.gram_len, a.bits);
-      uint32_t m = n0 | (n1 << 4) | (n2 << 8) | (n3 << 12) | (n4 << 16);
+  if (LONG) {
+    if (G > 4 || P == 4) {
+      // P = 4: grams of G bytes starting at the four aligned words; full
+      // 32-bit hashes, the shared-memory table indexed by their top `bits`
+      // bits, the L2 table (when present) by their top kBigBits bits
+      uint32_t h[5];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        if (j == 4 && lane != 31) { h[4] = 0; break; }
+        if (G == 4) h[j] = w[j] * 0x9E3779B1u;
+        else if (G == 8) h[j] = mix_words(w[j], w[j + 1], 0, 0, 8);
+        else h[j] = mix_words(w[j], w[j + 1], w[j + 2], w[j + 3], 16);
+      }
+      uint32_t n[5];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t hs = h[j] >> (32 - bits);
+        n[j] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
+        if (big) n[j] = nib_big(big, h[j], n[j]);
+      }
+      n[4] = __shfl_down_sync(0xFFFFFFFFu, n[0], 1);
+      if (lane == 31) {
+        const uint32_t hs = h[4] >> (32 - bits);
+        n[4] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
+        if (big) n[4] = nib_big(big, h[4], n[4]);
+      }
+      const uint32_t m = n[0] | (n[1] << 4) | (n[2] << 8) | (n[3] << 12) | (n[4] << 16);
       mask |= (m >> 3) & 0xFFFFu;
-    } else if (a.period == 4) {
-      uint32_t n0 = nib(filt, w[0], a.bits);
-      uint32_t n1 = nib(filt, w[1], a.bits);
-      uint32_t n2 = nib(filt, w[2], a.bits);
-      uint32_t n3 = nib(filt, w[3], a.bits);
-      uint32_t n4 = __shfl_down_sync(0xFFFFFFFFu, n0, 1);
-      if (lane == 31) n4 = nib(filt, w[4], a.bits);
-      uint32_t m = n0 | (n1 << 4) | (n2 << 8) | (n3 << 12) | (n4 << 16);
-      mask |= (m >> 3) & 0xFFFFu;
-    } else if (a.period == 2) {
+    } else if (P == 2) {
       uint32_t m = 0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
         uint32_t g = (j & 1) ? __funnelshift_r(w[j >> 1], w[(j >> 1) + 1], 16) : w[j >> 1];
-        m |= nib(filt, g, a.bits) << (2 * j);
+        m |= nib(filt, g, bits) << (2 * j);
       }
       mask |= (m >> 1) & 0xFFFFu;
     } else {
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         uint32_t g = __funnelshift_r(w[j >> 2], w[(j >> 2) + 1], 8 * (j & 3));
-        mask |= (nib(filt, g, a.bits) & 1u) << j;
+        mask |= (nib(filt, g, bits) & 1u) << j;
       }
     }
   }
-  if (a.has_short) {
+  if (SHORT) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       uint32_t g = __funnelshift_r(w[j >> 2], w[(j >> 2) + 1], 8 * (j & 3)) & 0xFFFFu;
@@ -195,22 +209,98 @@ __device__ __forceinline__ uint32_t prefix_key(uint32_t lo, uint32_t hi, uint32_
 constexpr int kBlockWords = 136;  // 512 B warp block + 16 B of the next block + slack
 constexpr int kQueue = 512;       // u16 offsets: at most 16 per lane
 
+// A warp block with at least one stage-1 candidate: the block is copied to
+// shared memory, the candidates are compacted into the queue (popc prefix
+// sums), stage 1.5 runs with all lanes busy, survivors are appended with one
+// atomic per warp.
+template <int G>
+__device__ __forceinline__ void process_block(const LitArgs& a, uint32_t* blk, uint16_t* queue, const uint32_t* bloom,
+                                              uint32_t lane, const uint4& cur, const uint4& tail, uint32_t mask,
+                                              uint32_t blk_base) {
+  reinterpret_cast<uint4*>(blk)[lane] = cur;
+  if (lane == 31) {
+    reinterpret_cast<uint4*>(blk)[32] = tail;
+    blk[132] = 0;
+    blk[133] = 0;
+  }
+  __syncwarp();
+  // compact the candidates of the warp into the queue
+  const uint32_t cnt = __popc(mask);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  uint32_t pos = incl - cnt;
+  while (mask) {
+    uint32_t i = __ffs(mask) - 1;
+    mask &= mask - 1;
+    queue[pos++] = (uint16_t)(lane * 16 + i);
+  }
+  __syncwarp();
+  // stage 1.5 with all lanes busy, then a warp-aggregated append of survivors
+  for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    bool keep = false;
+    uint32_t off = 0;
+    if (k < total) {
+      off = queue[k];
+      const uint32_t wi = off >> 2, sh = (off & 3) * 8;
+      const uint32_t x0 = blk[wi], x1 = blk[wi + 1], x2 = blk[wi + 2];
+      const uint32_t lo = __funnelshift_r(x0, x1, sh), hi = __funnelshift_r(x1, x2, sh);
+      for (uint32_t m = a.parts; m; m &= m - 1) {  // prefix lengths that have literals
+        const uint32_t key = prefix_key(lo, hi, __ffs(m));
+        keep |= (bloom[key >> 5] >> (key & 31)) & 1u;
+      }
+      if (G > 4 && keep) {
+        // stage 1.5b: the first min(len, 16) bytes against the L2 bitmap
+        const uint32_t x3 = blk[wi + 3], x4 = blk[wi + 4];
+        const uint32_t y2 = __funnelshift_r(x2, x3, sh), y3 = __funnelshift_r(x3, x4, sh);
+        bool k2 = false;
+        for (uint32_t m = a.parts16; m; m &= m - 1) {
+          const uint32_t key = prefix16_key(lo, hi, y2, y3, __ffs(m));
+          k2 |= (__ldg(a.bloom2 + (key >> 5)) >> (key & 31)) & 1u;
+        }
+        keep = k2;
+      }
+    }
+    const uint32_t ball = __ballot_sync(0xFFFFFFFFu, keep);
+    if (ball) {
+      unsigned long long wbase = 0;
+      if (lane == 0) wbase = atomicAdd(a.survivor_count, (unsigned long long)__popc(ball));
+      wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
+      if (keep) {
+        const unsigned long long slot = wbase + __popc(ball & ((1u << lane) - 1u));
+        const uint32_t s = blk_base + off;
+        if (slot < a.survivor_cap) a.survivors[slot] = s;
+        else verify_position(a, s);  // list full: verify in place
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Inputs of one launch are below 4 GiB, so block, vector and byte indices are
+// 32-bit.
+template <int P, int G, bool LONG, bool SHORT>
 __global__ void __launch_bounds__(kThreads, 1) literal_filter_kernel(LitArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* filt = smem;                                 // filter_words
   uint32_t* bloom = filt + a.filter_words;               // 2^kBloomBits / 32 words
-  uint32_t* shortb = bloom + (1u << (kBloomBits - 5));   // 2048 words when has_short
-  uint32_t* warpmem = shortb + (a.has_short ? 2048 : 0);
+  uint32_t* shortb = bloom + (1u << (kBloomBits - 5));   // 2048 words when SHORT
+  uint32_t* warpmem = shortb + (SHORT ? 2048 : 0);
 
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.filter);
     uint4* dst = reinterpret_cast<uint4*>(filt);
-    uint32_t n4 = a.has_long ? a.filter_words / 4 : 0;
+    const uint32_t n4 = LONG ? a.filter_words / 4 : 0;
     for (uint32_t k = threadIdx.x; k < n4; k += kThreads) dst[k] = __ldg(src + k);
     const uint4* bs = reinterpret_cast<const uint4*>(a.bloom);
     uint4* bd = reinterpret_cast<uint4*>(bloom);
     for (uint32_t k = threadIdx.x; k < (1u << (kBloomBits - 7)); k += kThreads) bd[k] = __ldg(bs + k);
-    if (a.has_short) {
+    if (SHORT) {
       const uint4* s2 = reinterpret_cast<const uint4*>(a.short_bits);
       uint4* d2 = reinterpret_cast<uint4*>(shortb);
       for (uint32_t k = threadIdx.x; k < 512; k += kThreads) d2[k] = __ldg(s2 + k);
@@ -222,36 +312,28 @@ __global__ void __launch_bounds__(kThreads, 1) literal_filter_kernel(LitArgs a) 
   const uint32_t warp = threadIdx.x >> 5;
   uint32_t* blk = warpmem + warp * (kBlockWords + kQueue / 2);
   uint16_t* queue = reinterpret_cast<uint16_t*>(blk + kBlockWords);
-  const uint64_t nvec = (a.len + 15) / 16;
-  const uint64_t nblk = (nvec + 31) / 32;  // 512-byte warp blocks
-  const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + warp;
-  const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
+  const uint32_t len = (uint32_t)a.len;
+  const uint32_t nvec = (uint32_t)((a.len + 15) >> 4);
+  const uint32_t full_vecs = len >> 4;                 // vectors entirely inside the input
+  const uint32_t nblk = (nvec + 31) >> 5;              // 512-byte warp blocks
+  const uint32_t nwarps = gridDim.x * kWarps;
+  const uint32_t bits = a.bits;
+  auto load = [&](uint32_t v) -> uint4 {
+    if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
+    return v < nvec ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
+  };
 
-  uint64_t b = gwarp;
+  uint32_t b = blockIdx.x * kWarps + warp;
   uint4 cur = make_uint4(0, 0, 0, 0);
-  if (b < nblk) {
-    uint64_t v = b * 32 + lane;
-    cur = (v < nvec) ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
-  }
+  if (b < nblk) cur = load(b * 32 + lane);
   for (; b < nblk; b += nwarps) {
     // software pipeline: the next block's load is in flight during this one
-    uint64_t bn = b + nwarps;
-    uint4 nxt = make_uint4(0, 0, 0, 0);
-    if (bn < nblk) {
-      uint64_t vn = bn * 32 + lane;
-      nxt = (vn < nvec) ? load_vec(a.data, a.len, vn) : make_uint4(0, 0, 0, 0);
-    }
-    const uint64_t v = b * 32 + lane;
-    uint4 tail = make_uint4(0, 0, 0, 0);
-    if (lane == 31 && v + 1 < nvec) tail = load_vec(a.data, a.len, v + 1);
-    reinterpret_cast<uint4*>(blk)[lane] = cur;
-    if (lane == 31) {
-      reinterpret_cast<uint4*>(blk)[32] = tail;
-      blk[132] = 0;
-      blk[133] = 0;
-    }
+    const uint32_t bn = b + nwarps;
+    const uint4 nxt = bn < nblk ? load(bn * 32 + lane) : make_uint4(0, 0, 0, 0);
+    const uint32_t v = b * 32 + lane;
+    const uint4 tail = lane == 31 ? load(v + 1) : make_uint4(0, 0, 0, 0);
     uint32_t w[8] = {cur.x, cur.y, cur.z, cur.w, __shfl_down_sync(0xFFFFFFFFu, cur.x, 1), 0, 0, 0};
-    if (a.gram_len > 4) {
+    if (G > 4) {
       w[5] = __shfl_down_sync(0xFFFFFFFFu, cur.y, 1);
       w[6] = __shfl_down_sync(0xFFFFFFFFu, cur.z, 1);
       w[7] = __shfl_down_sync(0xFFFFFFFFu, cur.w, 1);
@@ -262,75 +344,187 @@ __global__ void __launch_bounds__(kThreads, 1) literal_filter_kernel(LitArgs a) 
       w[6] = tail.z;
       w[7] = tail.w;
     }
-    uint32_t mask = stage1(a, filt, shortb, w, lane);
-    const uint64_t blk_base = b * 512;
-    const uint64_t base = v * 16;
-    if (base + 16 > a.len) {
-      uint64_t valid = a.len > base ? a.len - base : 0;
+    uint32_t mask = stage1<P, G, LONG, SHORT>(filt, shortb, w, lane, bits, a.big);
+    const uint32_t blk_base = b * 512;
+    if (v >= full_vecs) {  // the input's last, partial vector (or past the end)
+      const uint32_t base = v * 16;
+      const uint32_t valid = len > base ? len - base : 0;
       mask &= (valid >= 16) ? 0xFFFFu : ((1u << valid) - 1u);
     }
-    // compact the candidates of the warp into the queue
-    uint32_t cnt = __popc(mask);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-      if (lane >= (uint32_t)d) incl += y;
+    // most warp blocks have no candidate at all once stage 1b is in place
+    if (__ballot_sync(0xFFFFFFFFu, mask != 0) == 0) {
+      cur = nxt;
+      continue;
     }
-    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    uint32_t pos = incl - cnt;
-    while (mask) {
-      uint32_t i = __ffs(mask) - 1;
-      mask &= mask - 1;
-      queue[pos++] = (uint16_t)(lane * 16 + i);
-    }
-    __syncwarp();
-    // stage 1.5 with all lanes busy, then a warp-aggregated append of survivors
-    for (uint32_t k0 = 0; k0 < total; k0 += 32) {
-      uint32_t k = k0 + lane;
-      bool keep = false;
-      uint32_t off = 0;
-      if (k < total) {
-        off = queue[k];
-        uint32_t wi = off >> 2, sh = (off & 3) * 8;
-        uint32_t x0 = blk[wi], x1 = blk[wi + 1], x2 = blk[wi + 2];
-        uint32_t lo = __funnelshift_r(x0, x1, sh), hi = __funnelshift_r(x1, x2, sh);
-#pragma unroll
-        for (uint32_t pl = 1; pl <= 8; ++pl) {
-          if ((a.parts >> (pl - 1)) & 1u) {
-            uint32_t key = prefix_key(lo, hi, pl);
-            keep |= (bloom[key >> 5] >> (key & 31)) & 1u;
-          }
-        }
-        if (keep && a.bloom2) {
-          // stage 1.5b: the first min(len, 16) bytes against the L2 bitmap
-          uint32_t x3 = blk[wi + 3], x4 = blk[wi + 4];
-          uint32_t y2 = __funnelshift_r(x2, x3, sh), y3 = __funnelshift_r(x3, x4, sh);
-          bool k2 = false;
-          for (uint32_t pl = 1; pl <= 16; ++pl) {
-            if ((a.parts16 >> (pl - 1)) & 1u) {
-              uint32_t key = prefix16_key(lo, hi, y2, y3, pl);
-              k2 |= (__ldg(a.bloom2 + (key >> 5)) >> (key & 31)) & 1u;
-            }
-          }
-          keep = k2;
-        }
-      }
-      uint32_t ball = __ballot_sync(0xFFFFFFFFu, keep);
-      if (ball) {
-        unsigned long long wbase = 0;
-        if (lane == 0) wbase = atomicAdd(a.survivor_count, (unsigned long long)__popc(ball));
-        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
-        if (keep) {
-          unsigned long long slot = wbase + __popc(ball & ((1u << lane) - 1u));
-          uint64_t s = blk_base + off;
-          if (slot < a.survivor_cap) a.survivors[slot] = (uint32_t)s;
-          else verify_position(a, s);  // list full: verify in place
-        }
-      }
-    }
+    process_block<G>(a, blk, queue, bloom, lane, cur, tail, mask, blk_base);
     __syncwarp();
     cur = nxt;
+  }
+}
+
+// Stage 1 of the P = 4 layouts with the stage-1b table, split in two so that
+// the L2 loads of a block are in flight while the previous block finishes:
+// grams_issue hashes the five aligned grams of a lane (the fifth only on lane
+// 31), looks them up in shared memory and starts the L2 loads of the passing
+// ones; grams_finish combines them into the 16-bit candidate mask.
+struct Grams {
+  uint32_t h[5], n[5], bw[5];
+};
+
+template <int G>
+__device__ __forceinline__ void grams_issue(const uint32_t* filt, const uint32_t* big, const uint32_t (&w)[8],
+                                            uint32_t lane, uint32_t bits, Grams& s) {
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    if (j == 4 && lane != 31) {
+      s.h[4] = 0;
+      s.n[4] = 0;
+      s.bw[4] = 0;
+      break;
+    }
+    uint32_t hf;
+    if (G == 4) hf = w[j] * 0x9E3779B1u;
+    else if (G == 8) hf = mix_words(w[j], w[j + 1], 0, 0, 8);
+    else hf = mix_words(w[j], w[j + 1], w[j + 2], w[j + 3], 16);
+    const uint32_t hs = hf >> (32 - bits);
+    s.h[j] = hf;
+    s.n[j] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
+    s.bw[j] = s.n[j] ? __ldg(big + ((hf >> (32 - kBigBits)) >> 3)) : 0u;
+  }
+}
+
+__device__ __forceinline__ uint32_t grams_finish(const Grams& s, uint32_t lane) {
+  uint32_t n[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) n[j] = s.n[j] & (s.bw[j] >> (((s.h[j] >> (32 - kBigBits)) & 7) << 2));
+  const uint32_t n4 = __shfl_down_sync(0xFFFFFFFFu, n[0], 1);
+  const uint32_t m = n[0] | (n[1] << 4) | (n[2] << 8) | (n[3] << 12) | ((lane == 31 ? n[4] : n4) << 16);
+  return (m >> 3) & 0xFFFFu;
+}
+
+// The words a lane needs: its own four and the next lane's four (the tail
+// vector on lane 31).
+template <int G>
+__device__ __forceinline__ void lane_words(const uint4& cur, const uint4& tail, uint32_t lane, uint32_t (&w)[8]) {
+  w[0] = cur.x;
+  w[1] = cur.y;
+  w[2] = cur.z;
+  w[3] = cur.w;
+  w[4] = __shfl_down_sync(0xFFFFFFFFu, cur.x, 1);
+  w[5] = w[6] = w[7] = 0;
+  if (G > 4) {
+    w[5] = __shfl_down_sync(0xFFFFFFFFu, cur.y, 1);
+    w[6] = __shfl_down_sync(0xFFFFFFFFu, cur.z, 1);
+    w[7] = __shfl_down_sync(0xFFFFFFFFu, cur.w, 1);
+  }
+  if (lane == 31) {
+    w[4] = tail.x;
+    w[5] = tail.y;
+    w[6] = tail.z;
+    w[7] = tail.w;
+  }
+}
+
+constexpr int kBigThreads = 512;
+constexpr int kBigWarps = kBigThreads / 32;
+
+// P = 4 with the stage-1b table in L2: the same work as literal_filter_kernel
+// in a three-block software pipeline per warp -- the input of block i+2 is
+// loaded, the grams of block i+1 are hashed and their L2 checks issued, then
+// block i is finished -- so that the L2 latency overlaps useful work.
+// 16 warps per CTA leave room for the pipeline's registers.
+template <int G, bool SHORT>
+__global__ void __launch_bounds__(kBigThreads, 1) literal_filter_big_kernel(LitArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* filt = smem;
+  uint32_t* bloom = filt + a.filter_words;
+  uint32_t* shortb = bloom + (1u << (kBloomBits - 5));
+  uint32_t* warpmem = shortb + (SHORT ? 2048 : 0);
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.filter);
+    uint4* dst = reinterpret_cast<uint4*>(filt);
+    for (uint32_t k = threadIdx.x; k < a.filter_words / 4; k += kBigThreads) dst[k] = __ldg(src + k);
+    const uint4* bs = reinterpret_cast<const uint4*>(a.bloom);
+    uint4* bd = reinterpret_cast<uint4*>(bloom);
+    for (uint32_t k = threadIdx.x; k < (1u << (kBloomBits - 7)); k += kBigThreads) bd[k] = __ldg(bs + k);
+    if (SHORT) {
+      const uint4* s2 = reinterpret_cast<const uint4*>(a.short_bits);
+      uint4* d2 = reinterpret_cast<uint4*>(shortb);
+      for (uint32_t k = threadIdx.x; k < 512; k += kBigThreads) d2[k] = __ldg(s2 + k);
+    }
+  }
+  __syncthreads();
+
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = threadIdx.x >> 5;
+  uint32_t* blk = warpmem + warp * (kBlockWords + kQueue / 2);
+  uint16_t* queue = reinterpret_cast<uint16_t*>(blk + kBlockWords);
+  const uint32_t len = (uint32_t)a.len;
+  const uint32_t nvec = (uint32_t)((a.len + 15) >> 4);
+  const uint32_t full_vecs = len >> 4;
+  const uint32_t nblk = (nvec + 31) >> 5;
+  const uint32_t nwarps = gridDim.x * kBigWarps;
+  const uint32_t bits = a.bits;
+  auto load = [&](uint32_t v) -> uint4 {
+    if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
+    return v < nvec ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
+  };
+  const uint4 zero = make_uint4(0, 0, 0, 0);
+
+  uint32_t b = blockIdx.x * kBigWarps + warp;
+  // pipeline registers: block b (cur, grams in flight), block b + nwarps (nxt)
+  uint4 cur = zero, tail_c = zero, nxt = zero, tail_n = zero;
+  Grams gc;
+  if (b < nblk) {
+    cur = load(b * 32 + lane);
+    tail_c = lane == 31 ? load(b * 32 + 32) : zero;
+    uint32_t w[8];
+    lane_words<G>(cur, tail_c, lane, w);
+    grams_issue<G>(filt, a.big, w, lane, bits, gc);
+  }
+  if (b + nwarps < nblk) {
+    nxt = load((b + nwarps) * 32 + lane);
+    tail_n = lane == 31 ? load((b + nwarps) * 32 + 32) : zero;
+  }
+  for (; b < nblk; b += nwarps) {
+    const uint32_t bn = b + nwarps, bn2 = bn + nwarps;
+    // input of block b + 2 nwarps
+    uint4 nxt2 = zero, tail2 = zero;
+    if (bn2 < nblk) {
+      nxt2 = load(bn2 * 32 + lane);
+      tail2 = lane == 31 ? load(bn2 * 32 + 32) : zero;
+    }
+    // grams of block b + nwarps, L2 checks issued
+    Grams gn;
+    if (bn < nblk) {
+      uint32_t w[8];
+      lane_words<G>(nxt, tail_n, lane, w);
+      grams_issue<G>(filt, a.big, w, lane, bits, gn);
+    }
+    // finish block b
+    uint32_t mask = grams_finish(gc, lane);
+    if (SHORT) {
+      uint32_t w[8];
+      lane_words<G>(cur, tail_c, lane, w);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const uint32_t g = __funnelshift_r(w[j >> 2], w[(j >> 2) + 1], 8 * (j & 3)) & 0xFFFFu;
+        mask |= ((shortb[g >> 5] >> (g & 31)) & 1u) << j;
+      }
+    }
+    const uint32_t v = b * 32 + lane;
+    if (v >= full_vecs) {
+      const uint32_t base = v * 16;
+      const uint32_t valid = len > base ? len - base : 0;
+      mask &= (valid >= 16) ? 0xFFFFu : ((1u << valid) - 1u);
+    }
+    if (__ballot_sync(0xFFFFFFFFu, mask != 0) != 0)
+      process_block<G>(a, blk, queue, bloom, lane, cur, tail_c, mask, b * 512);
+    cur = nxt;
+    tail_c = tail_n;
+    gc = gn;
+    nxt = nxt2;
+    tail_n = tail2;
   }
 }
 
@@ -385,15 +579,45 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.gram_len = plan.gram_len;
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
+  a.big = plan.big.empty() ? nullptr : plan.d_big.as<uint32_t>();
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
-  size_t smem = literal_smem_bytes(plan);
-  check_cuda(cudaFuncSetAttribute(literal_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "cudaFuncSetAttribute(literal)");
+  if (l.len > 0xFFFFFFFFull) raise(WS_ERR_INPUT_TOO_LARGE, "literal scan launch beyond 32-bit offsets", 0, l.len,
+                                   0xFFFFFFFFull);
+  const size_t smem = literal_smem_bytes(plan);
   uint64_t nblk = ((l.len + 15) / 16 + 31) / 32;
   uint64_t want = (nblk + kWarps - 1) / kWarps;
   int grid = (int)std::min<uint64_t>((uint64_t)sm_count, std::max<uint64_t>(want, 1));
-  literal_filter_kernel<<<grid, kThreads, smem, st>>>(a);
-  check_cuda(cudaGetLastError(), "literal_filter_kernel launch");
+  // the filter layout is a compile-time choice of the kernel
+  auto run = [&](auto kernel) {
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "cudaFuncSetAttribute(literal)");
+    kernel<<<grid, kThreads, smem, st>>>(a);
+    check_cuda(cudaGetLastError(), "literal_filter_kernel launch");
+  };
+  const bool lg = plan.has_long != 0, sh = plan.has_short != 0;
+  auto run_big = [&](auto kernel) {
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "cudaFuncSetAttribute(literal)");
+    kernel<<<grid, kBigThreads, smem, st>>>(a);
+    check_cuda(cudaGetLastError(), "literal_filter_big_kernel launch");
+  };
+  // the pipelined kernel pays off for 4-byte grams (measured); long grams,
+  // whose hashing dominates, keep 32 warps per SM
+  if (lg && a.big && plan.period == 4 && plan.gram_len == 4) {
+    sh ? run_big(literal_filter_big_kernel<4, true>) : run_big(literal_filter_big_kernel<4, false>);
+  } else if (!lg) {
+    run(literal_filter_kernel<4, 4, false, true>);
+  } else if (plan.gram_len == 16) {
+    sh ? run(literal_filter_kernel<4, 16, true, true>) : run(literal_filter_kernel<4, 16, true, false>);
+  } else if (plan.gram_len == 8) {
+    sh ? run(literal_filter_kernel<4, 8, true, true>) : run(literal_filter_kernel<4, 8, true, false>);
+  } else if (plan.period == 4) {
+    sh ? run(literal_filter_kernel<4, 4, true, true>) : run(literal_filter_kernel<4, 4, true, false>);
+  } else if (plan.period == 2) {
+    sh ? run(literal_filter_kernel<2, 4, true, true>) : run(literal_filter_kernel<2, 4, true, false>);
+  } else {
+    sh ? run(literal_filter_kernel<1, 4, true, true>) : run(literal_filter_kernel<1, 4, true, false>);
+  }
   literal_verify_kernel<<<sm_count * 4, 256, 0, st>>>(a);
   check_cuda(cudaGetLastError(), "literal_verify_kernel launch");
 }
