@@ -628,16 +628,25 @@ __global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
     const uint32_t e = in ? p.lfend[j] : 0xFFFFFFFFu;
     const uint32_t s = in ? p.starts[j] : 0xFFFFFFFFu;
     const bool past = in && (uint64_t)s >= limit;
+    bool picked = false;
     while (true) {
       const bool ok = in && e != 0xFFFFFFFFu && (uint64_t)s >= last_end && !past;
       const unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
       if (!m) break;
       const int k = __ffs(m) - 1;
-      if ((int)lane == k) {
-        unsigned long long idx = atomicAdd(p.out_counter, 1ull);
+      picked |= (int)lane == k;
+      last_end = __shfl_sync(0xFFFFFFFFu, e, k);
+    }
+    // one output reservation per window of 32 candidates
+    const unsigned pm = __ballot_sync(0xFFFFFFFFu, picked);
+    if (pm) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(p.out_counter, (unsigned long long)__popc(pm));
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (picked) {
+        const unsigned long long idx = base + __popc(pm & ((1u << lane) - 1u));
         if (idx < p.out_cap) p.out[idx] = ws_match{pid, s, e};
       }
-      last_end = __shfl_sync(0xFFFFFFFFu, e, k);
     }
     if (__any_sync(0xFFFFFFFFu, past)) break;  // sorted: every later start is past too
   }
