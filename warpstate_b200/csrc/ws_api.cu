@@ -163,6 +163,49 @@ void check_regex_overflow(ws_matcher* m, Scratch& s) {
   if (flag) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow (raise max_matches)", 0, 0, m->cfg.max_matches);
 }
 
+// The windowed form of ws_scan for a large pinned host input (see ws_scan).
+void scan_overlapped(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len, ws_match* out, uint64_t cap,
+                     uint64_t* n_out) {
+  const uint64_t W = kOverlapWindow;
+  const uint64_t nwin = (len + W - 1) / W;
+  ensure(s.input, len + 64);
+  if (!s.copy) check_cuda(cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking), "cudaStreamCreate");
+  check_cuda(cudaStreamWaitEvent(s.copy, s.busy, 0), "wait");
+  std::vector<cudaEvent_t> arrived(nwin, nullptr);
+  struct Events {
+    std::vector<cudaEvent_t>& e;
+    ~Events() { for (auto x : e) if (x) cudaEventDestroy(x); }
+  } cleanup{arrived};
+  uint8_t* d = s.input.as<uint8_t>();
+  for (uint64_t k = 0; k < nwin; ++k) {
+    const uint64_t off = k * W, n = std::min(W, len - off);
+    check_cuda(cudaEventCreateWithFlags(&arrived[k], cudaEventDisableTiming), "cudaEventCreate");
+    check_cuda(cudaMemcpyAsync(d + off, data + off, n, cudaMemcpyHostToDevice, s.copy), "H2D window");
+    check_cuda(cudaEventRecord(arrived[k], s.copy), "event");
+  }
+  check_cuda(cudaMemsetAsync(d + len, 0, 64, s.stream), "memset pad");
+  const uint64_t dcap = device_capacity(m);
+  ensure(s.out64, dcap * sizeof(ws_match64));
+  auto* d_counter = s.counters.as<unsigned long long>();
+  enqueue_windows(m, s, s.stream, d, len, W, s.out64.as<ws_match64>(), dcap, d_counter, [&](uint64_t end) {
+    check_cuda(cudaStreamWaitEvent(s.stream, arrived[(end - 1) / W], 0), "wait window");
+  });
+  unsigned long long count = 0;
+  check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
+  check_cuda(cudaStreamSynchronize(s.stream), "scan");
+  *n_out = count;
+  if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
+  if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);
+  if (count) {
+    std::vector<ws_match64> wide(count);
+    check_cuda(cudaMemcpy(wide.data(), s.out64.ptr, count * sizeof(ws_match64), cudaMemcpyDeviceToHost),
+               "D2H matches");
+    for (uint64_t k = 0; k < count; ++k)
+      out[k] = ws_match{wide[k].pattern_id, (uint32_t)wide[k].start, (uint32_t)wide[k].end};
+    sort_matches(out, count);
+  }
+}
+
 }  // namespace ws
 
 std::unique_ptr<Scratch> ws_matcher::take() {
@@ -285,10 +328,17 @@ ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len, ws_match* ou
     auto s = m->take();
     struct Return { ws_matcher* m; std::unique_ptr<Scratch>& s; ~Return() { if (s) m->give(std::move(s)); } } ret{m, s};
     check_cuda(cudaStreamWaitEvent(s->stream, s->busy, 0), "wait");
-    stage_input(m, *s, data, len);
     uint64_t dcap = device_capacity(m);
-    ensure(s->out, dcap * sizeof(ws_match));
     auto* d_counter = s->counters.as<unsigned long long>();
+    if (len >= 2 * kOverlapWindow && is_pinned(data)) {
+      // large pinned input: copy it in windows on a second stream and scan
+      // each window as soon as it has arrived, so that the host-to-device
+      // copy of window k+1 runs under the scan of window k
+      scan_overlapped(m, *s, data, len, out, cap, n_out);
+      return;
+    }
+    stage_input(m, *s, data, len);
+    ensure(s->out, dcap * sizeof(ws_match));
     enqueue_scan(m, *s, s->stream, s->input.as<uint8_t>(), len, s->out.as<ws_match>(), dcap, d_counter);
     unsigned long long count = 0;
     check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");

@@ -7,6 +7,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -30,13 +31,16 @@ struct Scratch {
   DeviceBuffer rx;           // regex scratch (ws_dfa.cu manages the layout)
   DeviceBuffer lit;          // literal survivor list
   DeviceBuffer aux;          // batch item ends / tagged output
+  DeviceBuffer out64;        // ws_match64 output of windowed scans
   void* pinned = nullptr;    // pinned staging for pageable host input
   size_t pinned_bytes = 0;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // [2], [3]: staging slots drained
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // [0], [1]: window copies; [2], [3]: staging slots drained
   bool pin_busy[2] = {false, false};                         // a DMA may still read the slot
   cudaEvent_t busy = nullptr;  // recorded after the last use
+  cudaStream_t copy = nullptr;  // host-to-device copies overlapped with scans (created on first use)
   ~Scratch() {
     if (busy) cudaEventDestroy(busy);
+    if (copy) cudaStreamDestroy(copy);
     if (stream) cudaStreamDestroy(stream);
     if (pinned) cudaFreeHost(pinned);
     for (auto e : ev) if (e) cudaEventDestroy(e);
@@ -158,5 +162,21 @@ struct StepPlan {
 };
 StepPlan plan_step(const ws_matcher* m, uint64_t win_base, uint64_t old_seen, uint64_t seen, uint64_t frontier,
                    bool last);
+
+// Enqueues the scan of d_data[0, len) on `cs` as windows of `window` new
+// bytes (slices of d_data with exact carry), appending ws_match64 results to
+// d_out (capacity cap) and the true count to *total (zeroed here).
+// `before_window(end)` runs on the host before each window is enqueued, with
+// the end offset of the bytes it reads (a caller copying the input in pieces
+// makes `cs` wait for them there).  Returns the number of kernel launches.
+uint32_t enqueue_windows(ws_matcher* m, Scratch& s, cudaStream_t cs, const uint8_t* d_data, uint64_t len,
+                         uint64_t window, ws_match64* d_out, uint64_t cap, unsigned long long* total,
+                         const std::function<void(uint64_t)>& before_window);
+
+// ws_scan of a large pinned host input copies it in windows of this size on a
+// second stream, each window scanned as soon as it has arrived.
+constexpr uint64_t kOverlapWindow = 128ull << 20;
+void scan_overlapped(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t len, ws_match* out, uint64_t cap,
+                     uint64_t* n_out);
 
 }  // namespace ws

@@ -184,6 +184,63 @@ void deliver(ws_stream* st, ws_match64* out, uint64_t cap, uint64_t* n_out) {
 
 }  // namespace
 
+namespace ws {
+
+uint32_t enqueue_windows(ws_matcher* m, Scratch& s, cudaStream_t cs, const uint8_t* d_data, uint64_t len,
+                         uint64_t window, ws_match64* d_out, uint64_t cap, unsigned long long* total,
+                         const std::function<void(uint64_t)>& before_window) {
+  // the whole schedule is known on the host: windows are slices of d_data
+  check_cuda(cudaMemsetAsync(total, 0, 8, cs), "memset count");
+  const uint64_t scap = std::max<uint64_t>(cap, 1);
+  ensure(s.out, scap * sizeof(ws_match));
+  const size_t cursor_bytes = ((size_t)m->rx.n_regex * 8 + 255) & ~(size_t)255;
+  ensure(s.aux, cursor_bytes + 256);
+  auto* cursor = s.aux.as<unsigned long long>();
+  auto* step_count = reinterpret_cast<unsigned long long*>(s.aux.as<uint8_t>() + cursor_bytes);
+  if (m->rx.n_regex) check_cuda(cudaMemsetAsync(cursor, 0, (size_t)m->rx.n_regex * 8, cs), "memset cursor");
+  uint64_t seen = 0, win_base = 0, frontier = 0;
+  uint32_t launches = 0;
+  double summed[8] = {};
+  while (seen < len) {
+    const uint64_t n = std::min<uint64_t>(window, len - seen);
+    const bool last = seen + n == len;
+    const StepPlan plan = plan_step(m, win_base, seen, seen + n, frontier, last);
+    // windows are slices of d_data: start them on a 16-byte boundary (the
+    // kernels load 16-byte vectors); the extra leading bytes hold only
+    // literal occurrences already reported and regex starts already decided
+    const uint64_t keep = plan.keep & ~15ull;
+    ScanExtras x;
+    x.literals = m->lit.n_literals != 0;
+    x.lit_min_end = seen - keep;
+    x.cursor = m->rx.n_regex ? cursor : nullptr;
+    x.base = keep;
+    x.frontier = plan.frontier;
+    before_window(seen + n);
+    launches += enqueue_scan(m, s, cs, d_data + keep, seen + n - keep, s.out.as<ws_match>(), scap, step_count, x);
+    widen_kernel<<<1, 1024, 0, cs>>>(s.out.as<ws_match>(), step_count, scap, keep, d_out, cap, total);
+    check_cuda(cudaGetLastError(), "widen_kernel");
+    launches += 1;
+    if (m->profile) {  // profiling: phase times summed over the windows
+      double ms[8];
+      read_phases(m, ms);
+      for (int k = 0; k < 8; ++k) summed[k] += ms[k];
+    }
+    seen += n;
+    win_base = keep;
+    frontier = plan.frontier;
+  }
+  check_cuda(cudaEventRecord(s.busy, cs), "event");
+  std::lock_guard<std::mutex> g(m->info_mu);
+  m->info.last_launches = launches;
+  if (m->profile) {
+    for (int k = 0; k < 8; ++k) m->summed_ms[k] = summed[k];
+    m->use_summed = true;
+  }
+  return launches;
+}
+
+}  // namespace ws
+
 extern "C" {
 
 ws_status ws_stream_begin(ws_matcher* m, ws_stream** out, ws_error_info* err) {
@@ -264,51 +321,7 @@ ws_status ws_scan_device64(ws_matcher* m, const uint8_t* d_data, uint64_t len, w
       check_cuda(cudaEventRecord(s->busy, cs), "event");
       return;
     }
-    // the whole schedule is known on the host: windows are slices of d_data
-    const uint64_t scap = std::max<uint64_t>(cap, 1);
-    ensure(s->out, scap * sizeof(ws_match));
-    const size_t cursor_bytes = ((size_t)m->rx.n_regex * 8 + 255) & ~(size_t)255;
-    ensure(s->aux, cursor_bytes + 256);
-    auto* cursor = s->aux.as<unsigned long long>();
-    auto* step_count = reinterpret_cast<unsigned long long*>(s->aux.as<uint8_t>() + cursor_bytes);
-    if (m->rx.n_regex) check_cuda(cudaMemsetAsync(cursor, 0, (size_t)m->rx.n_regex * 8, cs), "memset cursor");
-    uint64_t seen = 0, win_base = 0, frontier = 0;
-    uint32_t launches = 0;
-    double summed[8] = {};
-    while (seen < len) {
-      const uint64_t n = std::min<uint64_t>(step_bytes(m), len - seen);
-      const bool last = seen + n == len;
-      const StepPlan plan = plan_step(m, win_base, seen, seen + n, frontier, last);
-      // windows are slices of d_data: start them on a 16-byte boundary (the
-      // kernels load 16-byte vectors); the extra leading bytes hold only
-      // literal occurrences already reported and regex starts already decided
-      const uint64_t keep = plan.keep & ~15ull;
-      ScanExtras x;
-      x.literals = m->lit.n_literals != 0;
-      x.lit_min_end = seen - keep;
-      x.cursor = m->rx.n_regex ? cursor : nullptr;
-      x.base = keep;
-      x.frontier = plan.frontier;
-      launches += enqueue_scan(m, *s, cs, d_data + keep, seen + n - keep, s->out.as<ws_match>(), scap, step_count, x);
-      widen_kernel<<<1, 1024, 0, cs>>>(s->out.as<ws_match>(), step_count, scap, keep, d_out, cap, total);
-      check_cuda(cudaGetLastError(), "widen_kernel");
-      launches += 1;
-      if (m->profile) {  // profiling: phase times summed over the windows
-        double ms[8];
-        read_phases(m, ms);
-        for (int k = 0; k < 8; ++k) summed[k] += ms[k];
-      }
-      seen += n;
-      win_base = keep;
-      frontier = plan.frontier;
-    }
-    check_cuda(cudaEventRecord(s->busy, cs), "event");
-    std::lock_guard<std::mutex> g(m->info_mu);
-    m->info.last_launches = launches;
-    if (m->profile) {
-      for (int k = 0; k < 8; ++k) m->summed_ms[k] = summed[k];
-      m->use_summed = true;
-    }
+    enqueue_windows(m, *s, cs, d_data, len, step_bytes(m), d_out, cap, total, [](uint64_t) {});
   });
 }
 
