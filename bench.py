@@ -408,8 +408,20 @@ def main():
         dt = (time.perf_counter() - t0) / k
         if len(res) != count:
             raise SystemExit(f"e2e count {len(res)} != device count {count}")
+        # the link ceiling: a plain pinned host-to-device copy of the same bytes
+        dev = torch.empty(n_bytes, dtype=torch.uint8, device="cuda")
+        dev.copy_(pinned, non_blocking=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            dev.copy_(pinned, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        h2d_gbs = n_bytes * k / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        del dev
         e2e = {"value": round(world * n_bytes / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": n_bytes,
                "d2h_bytes_per_step": d2h(count), "ms_per_step": round(dt * 1e3, 3),
+               "h2d_copy_gbs": round(h2d_gbs, 2),
                "api": ("scan_batch_packed (ws_scan_batch)" if batch else
                        "StreamPipeline.scan (ws_stream_*)" if big else "GpuMatcher.scan (ws_scan)")}
         del pinned, hv

@@ -325,3 +325,46 @@ def test_large_pinned_scan_overlaps_copy_and_stays_exact():
             g = g[(g[:, 1] >= lo) & (g[:, 2] <= hi) & lit[g[:, 0]]]
             g[:, 1:] -= lo
             assert np.array_equal(g, exp), (mode, k)
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_pinned_stream_feeds_pipeline_copies_and_stay_exact(mode):
+    # a pinned feed longer than one step copies step k+1 while step k is
+    # scanned; feeds of several steps, of less than one step, and of a
+    # ragged size in between give exactly the whole-input scan
+    torch = _torch()
+    ws = _ws()
+    wl = w.regex(size=(6 << 20) + 777, n=80, seed=63)
+    pats = wl.patterns + w.literals_large(size=1 << 10, n=200, seed=64).patterns
+    exp = oracle.scan_patterns(pats, wl.data).astype(np.uint64)
+    pinned = torch.empty(wl.data.nbytes, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = wl.data
+    m = matcher(pats, mode=mode, window_mib=1)
+    got = ws.StreamPipeline(m).scan_array(pinned)
+    assert len(exp) > 100 and np.array_equal(got, exp)
+    cuts = [0, (2 << 20) + 5, (2 << 20) + 9000, (5 << 20) + 3, wl.data.nbytes]
+    parts = []
+    with ws.Stream(m) as s:
+        for a, b in zip(cuts, cuts[1:]):
+            parts.append(s.feed_ptr_array(pinned.data_ptr() + a, b - a))
+        parts.append(s.end_array())
+    a = np.concatenate(parts)
+    a = a[np.lexsort((a[:, 2], a[:, 0], a[:, 1]))]
+    assert np.array_equal(a, exp)
+
+
+def test_pinned_batch_groups_pipeline_copies_and_stay_exact():
+    # a pinned arena split into 1 MiB launch groups: group k+1 is copied while
+    # group k is scanned, from alternating device buffers
+    torch = _torch()
+    ws = _ws()
+    wl = _batch_workload(n_items=1200, seed=23)
+    lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+    n = int(lens.sum())
+    pinned = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = wl.data[:n]
+    exp = oracle.batch_scan(wl.patterns, wl.data, wl.items)
+    for mib in (1, 1024):
+        m = matcher(wl.patterns, batch_mib=mib)
+        got = ws.scan_batch_packed(m, pinned, lens)
+        assert len(exp) > 100 and np.array_equal(got, exp), mib

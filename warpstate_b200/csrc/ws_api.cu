@@ -76,8 +76,8 @@ uint8_t* staging_slot(Scratch& s, int k, size_t piece) {
   return pin + (size_t)k * (s.pinned_bytes / 2);
 }
 
-void staging_issued(Scratch& s, int k) {
-  check_cuda(cudaEventRecord(s.ev[2 + k], s.stream), "event record");
+void staging_issued(Scratch& s, int k, cudaStream_t st) {
+  check_cuda(cudaEventRecord(s.ev[2 + k], st ? st : s.stream), "event record");
   s.pin_busy[k] = true;
 }
 
@@ -183,16 +183,21 @@ void scan_overlapped(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t le
     check_cuda(cudaMemcpyAsync(d + off, data + off, n, cudaMemcpyHostToDevice, s.copy), "H2D window");
     check_cuda(cudaEventRecord(arrived[k], s.copy), "event");
   }
-  check_cuda(cudaMemsetAsync(d + len, 0, 64, s.stream), "memset pad");
   const uint64_t dcap = device_capacity(m);
-  ensure(s.out64, dcap * sizeof(ws_match64));
   auto* d_counter = s.counters.as<unsigned long long>();
-  enqueue_windows(m, s, s.stream, d, len, W, s.out64.as<ws_match64>(), dcap, d_counter, [&](uint64_t end) {
-    check_cuda(cudaStreamWaitEvent(s.stream, arrived[(end - 1) / W], 0), "wait window");
-  });
   unsigned long long count = 0;
-  check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
-  check_cuda(cudaStreamSynchronize(s.stream), "scan");
+  try {
+    check_cuda(cudaMemsetAsync(d + len, 0, 64, s.stream), "memset pad");
+    ensure(s.out64, dcap * sizeof(ws_match64));
+    enqueue_windows(m, s, s.stream, d, len, W, s.out64.as<ws_match64>(), dcap, d_counter, [&](uint64_t end) {
+      check_cuda(cudaStreamWaitEvent(s.stream, arrived[(end - 1) / W], 0), "wait window");
+    });
+    check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
+    check_cuda(cudaStreamSynchronize(s.stream), "scan");
+  } catch (...) {
+    cudaStreamSynchronize(s.copy);  // no copy may still read the caller's input
+    throw;
+  }
   *n_out = count;
   if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
   if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);

@@ -57,12 +57,12 @@ __global__ void tag_kernel(const ws_match* in, const unsigned long long* count, 
 // large pinned runs are copied directly.
 class Gather {
  public:
-  Gather(Scratch& s, uint8_t* d_dst) : s_(s), d_dst_(d_dst) {}
+  Gather(Scratch& s, uint8_t* d_dst, cudaStream_t st) : s_(s), d_dst_(d_dst), st_(st) {}
 
   void push(const uint8_t* src, uint64_t n) {
     if (n >= kDirect && is_pinned(src)) {
       flush();
-      check_cuda(cudaMemcpyAsync(d_dst_ + off_, src, n, cudaMemcpyHostToDevice, s_.stream), "H2D item");
+      check_cuda(cudaMemcpyAsync(d_dst_ + off_, src, n, cudaMemcpyHostToDevice, st_), "H2D item");
       off_ += n;
       return;
     }
@@ -84,9 +84,9 @@ class Gather {
   void flush() {
     if (!pin_) return;
     if (fill_) {
-      check_cuda(cudaMemcpyAsync(d_dst_ + piece_off_, pin_, fill_, cudaMemcpyHostToDevice, s_.stream),
+      check_cuda(cudaMemcpyAsync(d_dst_ + piece_off_, pin_, fill_, cudaMemcpyHostToDevice, st_),
                  "H2D batch piece");
-      staging_issued(s_, slot_);
+      staging_issued(s_, slot_, st_);
       slot_ ^= 1;
     }
     fill_ = 0;
@@ -98,6 +98,7 @@ class Gather {
   static constexpr uint64_t kDirect = 1u << 20;
   Scratch& s_;
   uint8_t* d_dst_;
+  cudaStream_t st_;
   uint8_t* pin_ = nullptr;  // current slot being filled
   int slot_ = 0;
   size_t fill_ = 0;
@@ -184,69 +185,93 @@ extern "C" ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t
     ensure(s->out, dcap * sizeof(ws_match));
     auto* d_counter = s->counters.as<unsigned long long>();
     uint64_t total = 0;
-    std::vector<uint32_t> ends;
-    std::vector<uint64_t> ids;
-    for (const auto& gr : groups) {
-      const size_t ni = gr.second - gr.first;
-      ends.resize(ni);
-      ids.resize(ni);
+    if (!s->copy) check_cuda(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaStreamWaitEvent(s->copy, s->busy, 0), "wait");
+    // launch group k is gathered into input buffer k & 1 on the copy stream,
+    // group k + 1 while group k is scanned
+    struct Group {
+      std::vector<uint32_t> ends;
+      std::vector<uint64_t> ids;
       uint64_t bytes = 0;
+    } grp[2];
+    DeviceBuffer* inbuf[2] = {&s->input, &s->input_alt};
+    auto gather = [&](size_t gi) {
+      const auto& gr = groups[gi];
+      Group& G = grp[gi & 1];
+      const size_t ni = gr.second - gr.first;
+      G.ends.resize(ni);
+      G.ids.resize(ni);
+      G.bytes = 0;
       for (size_t k = 0; k < ni; ++k) {
         const ws_item& it = items[order[gr.first + k]];
-        bytes += it.len;
-        ends[k] = (uint32_t)bytes;
-        ids[k] = it.id;
+        G.bytes += it.len;
+        G.ends[k] = (uint32_t)G.bytes;
+        G.ids[k] = it.id;
       }
-      // device layout: [input bytes + pad][item ends u32][item ids u64][tagged matches]
-      ensure(s->input, bytes + 64);
-      const size_t ends_off = 0, ids_off = (ni * 4 + 255) & ~(size_t)255,
-                   tag_off = ids_off + ((ni * 8 + 255) & ~(size_t)255);
-      ensure(s->aux, tag_off + dcap * sizeof(ws_tagged_match));
-      uint8_t* aux = s->aux.as<uint8_t>();
-      {
-        // items adjacent in host memory (slices of one arena) move as one run
-        Gather g(*s, s->input.as<uint8_t>());
-        const uint8_t* run = nullptr;
-        uint64_t run_len = 0;
-        for (size_t k = 0; k < ni; ++k) {
-          const ws_item& it = items[order[gr.first + k]];
-          if (run && it.data == run + run_len) {
-            run_len += it.len;
-            continue;
-          }
-          if (run) g.push(run, run_len);
-          run = it.data;
-          run_len = it.len;
+      DeviceBuffer& in = *inbuf[gi & 1];  // its last scan (group gi - 2) has finished
+      ensure(in, G.bytes + 64);
+      // items adjacent in host memory (slices of one arena) move as one run
+      Gather g(*s, in.as<uint8_t>(), s->copy);
+      const uint8_t* run = nullptr;
+      uint64_t run_len = 0;
+      for (size_t k = 0; k < ni; ++k) {
+        const ws_item& it = items[order[gr.first + k]];
+        if (run && it.data == run + run_len) {
+          run_len += it.len;
+          continue;
         }
         if (run) g.push(run, run_len);
-        g.flush();
-        stage_copy(*s, aux + ends_off, reinterpret_cast<const uint8_t*>(ends.data()), ni * 4);
-        stage_copy(*s, aux + ids_off, reinterpret_cast<const uint8_t*>(ids.data()), ni * 8);
+        run = it.data;
+        run_len = it.len;
       }
-      check_cuda(cudaMemsetAsync(s->input.as<uint8_t>() + bytes, 0, 64, s->stream), "memset pad");
-      ScanExtras x;
-      x.item_end = reinterpret_cast<const uint32_t*>(aux + ends_off);
-      x.n_items = (uint32_t)ni;
-      enqueue_scan(m, *s, s->stream, s->input.as<uint8_t>(), bytes, s->out.as<ws_match>(), dcap, d_counter, x);
-      auto* d_tag = reinterpret_cast<ws_tagged_match*>(aux + tag_off);
-      tag_kernel<<<m->ctx->sm_count * 4, 256, 0, s->stream>>>(s->out.as<ws_match>(), d_counter, dcap,
-                                                                reinterpret_cast<const uint32_t*>(aux + ends_off),
-                                                                reinterpret_cast<const uint64_t*>(aux + ids_off),
-                                                                (uint32_t)ni, d_tag);
-      check_cuda(cudaGetLastError(), "tag_kernel");
-      unsigned long long count = 0;
-      check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");
-      check_cuda(cudaStreamSynchronize(s->stream), "batch scan");
-      check_regex_overflow(m, *s);
-      if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one batch launch", 0, count, dcap);
-      if (total + count <= cap && count) {
-        check_cuda(cudaMemcpyAsync(out + total, d_tag, count * sizeof(ws_tagged_match), cudaMemcpyDeviceToHost,
-                                   s->stream), "D2H tagged matches");
-        check_cuda(cudaStreamSynchronize(s->stream), "D2H sync");
+      if (run) g.push(run, run_len);
+      g.flush();
+      check_cuda(cudaMemsetAsync(in.as<uint8_t>() + G.bytes, 0, 64, s->copy), "memset pad");
+      check_cuda(cudaEventRecord(s->ev[gi & 1], s->copy), "event");
+    };
+    try {
+      gather(0);
+      for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& G = grp[gi & 1];
+        const size_t ni = G.ends.size();
+        // device layout of aux: [item ends u32][item ids u64][tagged matches]
+        const size_t ends_off = 0, ids_off = (ni * 4 + 255) & ~(size_t)255,
+                     tag_off = ids_off + ((ni * 8 + 255) & ~(size_t)255);
+        ensure(s->aux, tag_off + dcap * sizeof(ws_tagged_match));
+        uint8_t* aux = s->aux.as<uint8_t>();
+        stage_copy(*s, aux + ends_off, reinterpret_cast<const uint8_t*>(G.ends.data()), ni * 4);
+        stage_copy(*s, aux + ids_off, reinterpret_cast<const uint8_t*>(G.ids.data()), ni * 8);
+        check_cuda(cudaStreamWaitEvent(s->stream, s->ev[gi & 1], 0), "wait group");
+        ScanExtras x;
+        x.item_end = reinterpret_cast<const uint32_t*>(aux + ends_off);
+        x.n_items = (uint32_t)ni;
+        enqueue_scan(m, *s, s->stream, inbuf[gi & 1]->as<uint8_t>(), G.bytes, s->out.as<ws_match>(), dcap,
+                     d_counter, x);
+        auto* d_tag = reinterpret_cast<ws_tagged_match*>(aux + tag_off);
+        tag_kernel<<<m->ctx->sm_count * 4, 256, 0, s->stream>>>(s->out.as<ws_match>(), d_counter, dcap,
+                                                                  reinterpret_cast<const uint32_t*>(aux + ends_off),
+                                                                  reinterpret_cast<const uint64_t*>(aux + ids_off),
+                                                                  (uint32_t)ni, d_tag);
+        check_cuda(cudaGetLastError(), "tag_kernel");
+        if (gi + 1 < groups.size()) gather(gi + 1);
+        unsigned long long count = 0;
+        check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream),
+                   "D2H count");
+        check_cuda(cudaStreamSynchronize(s->stream), "batch scan");
+        check_regex_overflow(m, *s);
+        if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one batch launch", 0, count, dcap);
+        if (total + count <= cap && count) {
+          check_cuda(cudaMemcpyAsync(out + total, d_tag, count * sizeof(ws_tagged_match), cudaMemcpyDeviceToHost,
+                                     s->stream), "D2H tagged matches");
+          check_cuda(cudaStreamSynchronize(s->stream), "D2H sync");
+        }
+        total += count;
       }
-      total += count;
-      check_cuda(cudaEventRecord(s->busy, s->stream), "event");
+    } catch (...) {
+      cudaStreamSynchronize(s->copy);  // no copy may still read the caller's items
+      throw;
     }
+    check_cuda(cudaEventRecord(s->busy, s->stream), "event");
     *n_out = total;
     if (total > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, total, cap);
     std::sort(out, out + total, [](const ws_tagged_match& a, const ws_tagged_match& b) {

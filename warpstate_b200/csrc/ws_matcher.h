@@ -26,6 +26,7 @@ namespace ws {
 struct Scratch {
   cudaStream_t stream = nullptr;
   DeviceBuffer input;        // padded device copy of the input
+  DeviceBuffer input_alt;    // second input buffer: the next batch launch group is copied while one scans
   DeviceBuffer out;          // ws_match[capacity]
   DeviceBuffer counters;     // unsigned long long[8]
   DeviceBuffer rx;           // regex scratch (ws_dfa.cu manages the layout)
@@ -62,8 +63,9 @@ struct ScanExtras {
 uint8_t* staging(Scratch& s, size_t piece);
 // Host pointer of staging slot k, after any DMA still reading it has finished.
 uint8_t* staging_slot(Scratch& s, int k, size_t piece);
-// Marks slot k as read by the DMA just enqueued on the scratch's stream.
-void staging_issued(Scratch& s, int k);
+// Marks slot k as read by the DMA just enqueued on `st` (default: the
+// scratch's stream).
+void staging_issued(Scratch& s, int k, cudaStream_t st = nullptr);
 void ensure(DeviceBuffer& b, size_t need);
 void fill_err(ws_error_info* err, const Failure& f);
 bool is_pinned(const void* p);

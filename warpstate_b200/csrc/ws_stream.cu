@@ -39,6 +39,7 @@ struct ws_stream {
   std::vector<ws_match64> pending;  // decided, not yet delivered
   size_t delivered = 0;
   std::vector<ws_match> host;       // per-step readback
+  unsigned long long count = 0;     // the step's match count, read back
   bool failed = false;
   bool ended = false;
   ~ws_stream() {
@@ -54,8 +55,8 @@ uint64_t step_bytes(const ws_matcher* m) { return (uint64_t)(m->cfg.window_mib ?
 
 int64_t regex_max_len(const ws_matcher* m) { return m->rx.n_regex ? m->rx.max_len : 0; }
 
-// Runs one scan of the current window and appends the decided matches.
-void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t frontier) {
+// Enqueues one scan of the current window; false when there is nothing to scan.
+bool enqueue_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t frontier) {
   ws_matcher* m = st->m;
   Scratch& s = *st->s;
   const uint64_t dcap = device_capacity(m);
@@ -67,12 +68,21 @@ void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t fr
   x.cursor = m->rx.n_regex ? st->cursor.as<unsigned long long>() : nullptr;
   x.base = st->win_base;
   x.frontier = frontier;
-  if (!literals && !m->rx.n_regex) return;
+  if (!literals && !m->rx.n_regex) return false;
   enqueue_scan(m, s, s.stream, st->win[st->cur].as<uint8_t>(), st->win_len, s.out.as<ws_match>(), dcap, d_counter, x);
-  unsigned long long count = 0;
-  check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
+  check_cuda(cudaMemcpyAsync(&st->count, d_counter, sizeof(st->count), cudaMemcpyDeviceToHost, s.stream),
+             "D2H count");
+  return true;
+}
+
+// Waits for the window scan just enqueued and appends the decided matches.
+void finish_window(ws_stream* st) {
+  ws_matcher* m = st->m;
+  Scratch& s = *st->s;
+  const uint64_t dcap = device_capacity(m);
   check_cuda(cudaStreamSynchronize(s.stream), "stream scan");
   check_regex_overflow(m, s);
+  const unsigned long long count = st->count;
   if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one stream piece", 0, count, dcap);
   if (count) {
     st->host.resize(count);
@@ -87,6 +97,11 @@ void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t fr
       st->pending.push_back(o);
     }
   }
+}
+
+// Runs one scan of the current window and appends the decided matches.
+void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t frontier) {
+  if (enqueue_window(st, literals, lit_min_end, frontier)) finish_window(st);
 }
 
 }  // namespace
@@ -120,27 +135,78 @@ StepPlan plan_step(const ws_matcher* m, uint64_t win_base, uint64_t old_seen, ui
 
 namespace {
 
-// Appends `len` bytes (len <= step_bytes) to the stream and decides what it can.
-void feed_step(ws_stream* st, const uint8_t* data, uint64_t len) {
+// Plans the step that appends `len` bytes (len <= step_bytes) and enqueues its
+// window on `cs`: the carried tail of the current window, then the new bytes
+// (a stream other than the scratch's own takes pinned input only).
+StepPlan copy_step(ws_stream* st, const uint8_t* data, uint64_t len, cudaStream_t cs) {
   ws_matcher* m = st->m;
   Scratch& s = *st->s;
-  const uint64_t old_seen = st->seen, seen = old_seen + len;
-  const StepPlan plan = plan_step(m, st->win_base, old_seen, seen, st->frontier, false);
-  const uint64_t keep = plan.keep;
-  const uint64_t carry = old_seen - keep;
+  const uint64_t old_seen = st->seen;
+  const StepPlan plan = plan_step(m, st->win_base, old_seen, old_seen + len, st->frontier, false);
+  const uint64_t carry = old_seen - plan.keep;
   DeviceBuffer& dst = st->win[st->cur ^ 1];
   ensure(dst, carry + len + 64);
   if (carry)
-    check_cuda(cudaMemcpyAsync(dst.ptr, st->win[st->cur].as<uint8_t>() + (keep - st->win_base), carry,
-                               cudaMemcpyDeviceToDevice, s.stream), "D2D carry");
-  stage_copy(s, dst.as<uint8_t>() + carry, data, len);
-  check_cuda(cudaMemsetAsync(dst.as<uint8_t>() + carry + len, 0, 64, s.stream), "memset pad");
+    check_cuda(cudaMemcpyAsync(dst.ptr, st->win[st->cur].as<uint8_t>() + (plan.keep - st->win_base), carry,
+                               cudaMemcpyDeviceToDevice, cs), "D2D carry");
+  if (cs == s.stream)
+    stage_copy(s, dst.as<uint8_t>() + carry, data, len);
+  else
+    check_cuda(cudaMemcpyAsync(dst.as<uint8_t>() + carry, data, len, cudaMemcpyHostToDevice, cs), "H2D step");
+  check_cuda(cudaMemsetAsync(dst.as<uint8_t>() + carry + len, 0, 64, cs), "memset pad");
+  return plan;
+}
+
+// Makes the window that copy_step filled current; returns the literal
+// min-end of its scan (occurrences ending before it were reported).
+uint64_t advance_step(ws_stream* st, uint64_t len, const StepPlan& plan) {
+  const uint64_t old_seen = st->seen;
   st->cur ^= 1;
-  st->win_base = keep;
-  st->win_len = carry + len;
-  st->seen = seen;
-  scan_window(st, m->lit.n_literals != 0, old_seen - keep, plan.frontier);
+  st->win_base = plan.keep;
+  st->win_len = old_seen - plan.keep + len;
+  st->seen = old_seen + len;
   st->frontier = plan.frontier;
+  return old_seen - plan.keep;
+}
+
+// Appends `len` bytes (len <= step_bytes) to the stream and decides what it can.
+void feed_step(ws_stream* st, const uint8_t* data, uint64_t len) {
+  const StepPlan plan = copy_step(st, data, len, st->s->stream);
+  const uint64_t lit_min_end = advance_step(st, len, plan);
+  scan_window(st, st->m->lit.n_literals != 0, lit_min_end, plan.frontier);
+}
+
+// Feeds a pinned input of several steps with the copy of step k+1 (on the
+// scratch's copy stream) running while step k is scanned.  The schedule is
+// the one feed_step follows, so the windows and results are the same.
+void feed_pipelined(ws_stream* st, const uint8_t* data, uint64_t len) {
+  Scratch& s = *st->s;
+  const uint64_t step = step_bytes(st->m);
+  if (!s.copy) check_cuda(cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking), "cudaStreamCreate");
+  // the copy stream follows everything enqueued on the scratch's stream
+  check_cuda(cudaEventRecord(s.busy, s.stream), "event");
+  check_cuda(cudaStreamWaitEvent(s.copy, s.busy, 0), "wait");
+  try {
+    uint64_t n = std::min(step, len);
+    StepPlan plan = copy_step(st, data, n, s.copy);
+    check_cuda(cudaEventRecord(s.ev[0], s.copy), "event");
+    for (uint64_t off = 0, k = 0; off < len; ++k) {
+      check_cuda(cudaStreamWaitEvent(s.stream, s.ev[k & 1], 0), "wait step");
+      const uint64_t lit_min_end = advance_step(st, n, plan);
+      const uint64_t next = off + n, n_next = std::min(step, len - next);
+      // the next window is the other buffer, whose last scan has finished
+      if (n_next) {
+        plan = copy_step(st, data + next, n_next, s.copy);
+        check_cuda(cudaEventRecord(s.ev[(k + 1) & 1], s.copy), "event");
+      }
+      scan_window(st, st->m->lit.n_literals != 0, lit_min_end, st->frontier);
+      off = next;
+      n = n_next;
+    }
+  } catch (...) {
+    cudaStreamSynchronize(s.copy);  // no copy may still read the caller's input
+    throw;
+  }
 }
 
 // Appends one window's matches to a 64-bit output: offsets shifted by the
@@ -269,10 +335,14 @@ ws_status ws_stream_feed(ws_stream* st, const uint8_t* data, uint64_t len, ws_ma
     if (st->ended && len) raise(WS_ERR_INVALID_ARGUMENT, "stream already ended");
     check_cuda(cudaSetDevice(st->m->ctx->device), "cudaSetDevice");
     try {
-      for (uint64_t off = 0; off < len;) {
-        uint64_t n = std::min<uint64_t>(step_bytes(st->m), len - off);
-        feed_step(st, data + off, n);
-        off += n;
+      if (len > step_bytes(st->m) && is_pinned(data)) {
+        feed_pipelined(st, data, len);
+      } else {
+        for (uint64_t off = 0; off < len;) {
+          uint64_t n = std::min<uint64_t>(step_bytes(st->m), len - off);
+          feed_step(st, data + off, n);
+          off += n;
+        }
       }
     } catch (...) {
       st->failed = true;
