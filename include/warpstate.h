@@ -298,7 +298,11 @@ ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
 /* Diagnostic entry points used by the parity tests: the K-candidate set
  * (pattern_id, start, end) of every anchored regex match, computed by the plain
  * thread-per-start kernel (mode WS_REGEX_PLAIN) or by the speculative walk plus
- * reverse walk (WS_REGEX_SPECULATIVE).  Host buffers, unsorted. */
+ * reverse walk (WS_REGEX_SPECULATIVE).  Host buffers, unsorted.
+ * With WS_CAND_DISTINCT or-ed into the mode: the candidates a scan works from,
+ * which hold the same distinct (pattern_id, start) pairs, without the repeats
+ * that a long run of match ends (a+ over a run of a's) makes quadratic. */
+enum { WS_CAND_DISTINCT = 0x100 };
 ws_status ws_regex_candidates(ws_matcher* m, const uint8_t* data, uint64_t len, uint32_t mode,
                               ws_match* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
 

@@ -368,3 +368,24 @@ def test_pinned_batch_groups_pipeline_copies_and_stay_exact():
         m = matcher(wl.patterns, batch_mib=mib)
         got = ws.scan_batch_packed(m, pinned, lens)
         assert len(exp) > 100 and np.array_equal(got, exp), mib
+
+
+def test_batch_order_ties_on_end_and_ids_spanning_groups():
+    # items sharing a source id give matches equal in (source_id, start,
+    # pattern_id) that differ in end: the device ordering breaks the tie by
+    # end, and an id whose items fall in two launch groups is merged in order
+    ws = _ws()
+    pats = [(1, b"a+"), (0, b"aa"), (1, b"b[ab]*")]
+    datas = [b"aaa", b"a", b"aa", b"baab", b"ba", b"aaaa"] * 40
+    ids = [7, 7, 7, 3, 3, 7] * 40
+    exp = oracle.batch_scan(pats, b"".join(datas), _offsets(datas), ids).tolist()
+    for kw in ({}, {"batch_mib": 1}):
+        m = matcher(pats, **kw)
+        got = tagged_rows(ws.scan_batch_gpu(m, [ws.ScanItem(i, d) for i, d in zip(ids, datas)]))
+        assert got == exp, kw
+    # ~1.1 MB: the last item of id 5 falls in a second 1 MiB launch group
+    big = [b"aaa" * 50_000, b"xyz" * 250_000, b"a" * 80_000, b"aa" * 60_000]
+    exp = oracle.batch_scan(pats, b"".join(big), _offsets(big), [5] * 4).tolist()
+    m = matcher(pats, batch_mib=1, max_matches=1 << 21)
+    got = tagged_rows(ws.scan_batch_gpu(m, [ws.ScanItem(5, d) for d in big]))
+    assert got == exp

@@ -145,3 +145,35 @@ def test_unsupported_regexes_fail_loudly():
     for pat in ["^abc", "abc$", "\\bword", "a*", "a|"]:
         with pytest.raises(ws.PatternCompilationFailed):
             matcher([(1, pat.encode())])
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_long_runs_of_match_ends_are_exact(mode):
+    # a+ over long runs of a's: every position ends one match and starts
+    # another.  The speculative path shares reverse-walk marks, cuts the
+    # parallel leftmost-first walks at 1 KiB (the chain finishes the ones it
+    # picks: x[a-z]*y spans 5 KB here) and merge-sorts per-regex start lists
+    # of more than 4096 entries
+    pats = [(1, b"a+"), (1, b"(ab)+c?"), (1, b"x[a-z]*y"), (0, b"aa"), (1, b"a{3}")]
+    n = 150_000 if mode == SPEC else 30_000
+    data = (b"a" * n + b"\n" + b"ab" * (n // 2) + b"c" + b"x" + b"q" * 5000 + b"y" + b"zz"
+            + b"a" * (n // 3))
+    m = matcher(pats, mode=mode, max_matches=1 << 21)
+    got = m.scan_array(data)
+    exp = oracle.scan_patterns(pats, data)
+    assert len(exp) > n and np.array_equal(got, exp)
+
+
+def test_distinct_candidates_hold_the_starts_of_full_k():
+    # the candidates a scan works from hold exactly the distinct
+    # (pattern_id, start) pairs of K, in both modes, with far fewer entries
+    pats = [(1, b"a+"), (1, b"(ab)+"), (1, b"b[ab]*")]
+    data = (b"a" * 1500 + b"b" + b"ab" * 700 + b"\n") * 2
+    m = matcher(pats, max_matches=1 << 21)
+    full = {md: m.regex_candidates(data, md) for md in (PLAIN, SPEC)}
+    assert np.array_equal(oracle.sort_matches(full[PLAIN]), oracle.sort_matches(full[SPEC]))
+    starts = set(map(tuple, full[PLAIN][:, :2].tolist()))
+    for md in (PLAIN, SPEC):
+        d = m.regex_candidates(data, md, distinct=True)
+        assert set(map(tuple, d[:, :2].tolist())) == starts, md
+        assert len(d) * 20 < len(full[md]), (md, len(d), len(full[md]))

@@ -42,6 +42,7 @@ REGEX_SPECULATIVE = 0
 REGEX_PLAIN = 1
 PROPOSER_MLP = 0
 PROPOSER_NONE = 1
+CAND_DISTINCT = 0x100  # ws_regex_candidates: the candidates a scan works from
 
 
 class Match(NamedTuple):
@@ -507,8 +508,12 @@ class GpuMatcher:
                 "proposer_top1": rep.proposer_top1, "proposer_top4": rep.proposer_top4,
                 "tune_seconds": round(rep.tune_seconds, 2)}
 
-    def regex_candidates(self, data, mode: int) -> np.ndarray:
+    def regex_candidates(self, data, mode: int, distinct: bool = False) -> np.ndarray:
+        """K candidates (pattern_id, start, end), unsorted: every anchored match
+        end, or with ``distinct`` the candidates a scan works from (the same
+        distinct (pattern_id, start) pairs, repeats pruned)."""
         ptr, n, keep = _buffer(data)
+        mode = int(mode) | (CAND_DISTINCT if distinct else 0)
         cap = max(int(self.config.c.max_matches), 1) * 4
         out = np.empty((cap, 3), dtype=np.uint32)
         cnt = ctypes.c_uint64()

@@ -201,14 +201,31 @@ void scan_overlapped(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t le
   *n_out = count;
   if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
   if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);
-  if (count) {
+  if (count > kMaxDeviceSorted) {
     std::vector<ws_match64> wide(count);
     check_cuda(cudaMemcpy(wide.data(), s.out64.ptr, count * sizeof(ws_match64), cudaMemcpyDeviceToHost),
                "D2H matches");
     for (uint64_t k = 0; k < count; ++k)
       out[k] = ws_match{wide[k].pattern_id, (uint32_t)wide[k].start, (uint32_t)wide[k].end};
     sort_matches(out, count);
+    return;
   }
+  // the windows' output buffer is free again: narrow into it, then order
+  narrow_matches_device(s.out64.as<ws_match64>(), s.out.as<ws_match>(), count, s.stream);
+  read_sorted(s, s.out.as<ws_match>(), count, out);
+}
+
+void read_sorted(Scratch& s, const ws_match* d_res, uint64_t count, ws_match* out) {
+  if (!count) return;
+  const bool on_device = count <= kMaxDeviceSorted;
+  if (on_device && count > 1) {
+    ensure(s.sorted, count * sizeof(ws_match));
+    sort_matches_device(s, d_res, s.sorted.as<ws_match>(), count, s.stream);
+    d_res = s.sorted.as<ws_match>();
+  }
+  check_cuda(cudaMemcpyAsync(out, d_res, count * sizeof(ws_match), cudaMemcpyDeviceToHost, s.stream), "D2H matches");
+  check_cuda(cudaStreamSynchronize(s.stream), "D2H sync");
+  if (!on_device) sort_matches(out, count);
 }
 
 }  // namespace ws
@@ -352,11 +369,7 @@ ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len, ws_match* ou
     check_regex_overflow(m, *s);
     if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
     if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);
-    if (count) {
-      check_cuda(cudaMemcpyAsync(out, s->out.ptr, count * sizeof(ws_match), cudaMemcpyDeviceToHost, s->stream), "D2H matches");
-      check_cuda(cudaStreamSynchronize(s->stream), "D2H sync");
-      sort_matches(out, count);
-    }
+    read_sorted(*s, s->out.as<ws_match>(), count, out);
   });
 }
 

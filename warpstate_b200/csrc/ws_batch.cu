@@ -261,7 +261,13 @@ extern "C" ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t
         check_regex_overflow(m, *s);
         if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one batch launch", 0, count, dcap);
         if (total + count <= cap && count) {
-          check_cuda(cudaMemcpyAsync(out + total, d_tag, count * sizeof(ws_tagged_match), cudaMemcpyDeviceToHost,
+          const ws_tagged_match* res = d_tag;
+          if (count > 1 && count <= kMaxDeviceSorted) {  // this group's matches in their final order
+            ensure(s->sorted, count * sizeof(ws_tagged_match));
+            sort_tagged_device(*s, d_tag, s->sorted.as<ws_tagged_match>(), count, s->stream);
+            res = s->sorted.as<ws_tagged_match>();
+          }
+          check_cuda(cudaMemcpyAsync(out + total, res, count * sizeof(ws_tagged_match), cudaMemcpyDeviceToHost,
                                      s->stream), "D2H tagged matches");
           check_cuda(cudaStreamSynchronize(s->stream), "D2H sync");
         }
@@ -274,11 +280,14 @@ extern "C" ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t
     check_cuda(cudaEventRecord(s->busy, s->stream), "event");
     *n_out = total;
     if (total > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, total, cap);
-    std::sort(out, out + total, [](const ws_tagged_match& a, const ws_tagged_match& b) {
+    // each launch group came back ordered; groups are in source-id order, so
+    // only an id whose items span two groups leaves work for the host
+    auto less = [](const ws_tagged_match& a, const ws_tagged_match& b) {
       if (a.source_id != b.source_id) return a.source_id < b.source_id;
       if (a.start != b.start) return a.start < b.start;
       if (a.pattern_id != b.pattern_id) return a.pattern_id < b.pattern_id;
       return a.end < b.end;
-    });
+    };
+    if (!std::is_sorted(out, out + total, less)) std::sort(out, out + total, less);
   });
 }

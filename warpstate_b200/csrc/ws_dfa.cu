@@ -23,13 +23,26 @@ constexpr uint32_t F_MASK = 0x3FFFFFFFu;
 constexpr uint32_t kCkpt = 256;       // bytes between recorded walk states
 constexpr int kFixRounds = 3;         // parallel fix-up rounds before the serial sweep
 constexpr int kWalkThreads = 1024;    // threads (= chunks) per walk block
+// Reverse walks share a lossy table of visited (position, group, state)
+// triples: a walk that reaches a triple another walk has passed stops there,
+// since the rest of its walk -- and every start it would report -- is the
+// other walk's.  This keeps a long run of match ends (a+ over a run of a's)
+// linear instead of quadratic.  2^kRmarkBits slots of 8 bytes, cleared per scan.
+constexpr uint32_t kRmarkBits = 20;
+constexpr uint32_t kRmarkStateBits = 20;  // states below 2^20, groups below 2^12
+// Leftmost-first walks in the parallel pass stop after kLfCap bytes; the
+// chain kernel finishes such a walk only if it picks that start (picked
+// matches do not overlap, so that work is bounded by the input).
+constexpr uint64_t kLfCap = 1024;
+constexpr uint32_t kLfNone = 0xFFFFFFFFu;  // no match from this start (or a duplicate start)
+constexpr uint32_t kLfLong = 0xFFFFFFFEu;  // the walk reached kLfCap bytes
 
 // ------------------------------------------------------------ scratch layout
 struct RxLayout {
   uint64_t n_chunks = 0, chunk = 0, nck = 0, n_q = 0;
   uint64_t k_cap = 0, ev_cap = 0;
   size_t off_ctr, off_k, off_ev, off_guess, off_used, off_end, off_spec, off_conv, off_round, off_ckpt,
-      off_count, off_offs, off_cursor, off_starts, off_lfend, total;
+      off_count, off_offs, off_cursor, off_starts, off_lfend, off_rmark, total;
 };
 
 struct KCand { uint32_t r, s, e; };
@@ -64,6 +77,7 @@ RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_m
   L.off_cursor = take((size_t)p.n_regex * 4);
   L.off_starts = take(L.k_cap * 4);
   L.off_lfend = take(L.k_cap * 4);
+  L.off_rmark = take(((size_t)1 << kRmarkBits) * 8);
   L.total = o;
   return L;
 }
@@ -104,6 +118,8 @@ struct ScanPtrs {
   uint32_t* cursor;
   uint32_t* starts;
   uint32_t* lfend;
+  unsigned long long* rmark;    // visited reverse-walk triples, or null (state numbers too large, or full K)
+  uint32_t full_k;              // report every (start, end) of K, not only distinct starts (diagnostics)
   uint64_t n_chunks, chunk, nck;
   ws_match* out;
   uint64_t out_cap;
@@ -136,6 +152,8 @@ ScanPtrs make_ptrs(const RxLayout& L, void* base, const RegexLaunch& l) {
   p.cursor = reinterpret_cast<uint32_t*>(b + L.off_cursor);
   p.starts = reinterpret_cast<uint32_t*>(b + L.off_starts);
   p.lfend = reinterpret_cast<uint32_t*>(b + L.off_lfend);
+  p.rmark = reinterpret_cast<unsigned long long*>(b + L.off_rmark);
+  p.full_k = 0;
   p.n_chunks = L.n_chunks;
   p.chunk = L.chunk;
   p.nck = L.nck;
@@ -304,6 +322,10 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
     uint32_t cold_row = 0;
     uint32_t st = state_of(gd.start_anchored, first, rows, lane4, &cold_row);
     const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, (uint32_t)s)) : p.len;
+    // a candidate is (regex, start): the end is recomputed leftmost-first
+    // later, so a match row reported earlier on this walk (a self-loop such
+    // as a+, a short cycle such as (ab)+) adds nothing; the last four are kept
+    uint32_t seen0 = 0xFFFFFFFFu, seen1 = 0xFFFFFFFFu, seen2 = 0xFFFFFFFFu, seen3 = 0xFFFFFFFFu;
     for (uint64_t e = s; e < stop; ++e) {
       uint32_t b = __ldg(p.data + e);
       uint32_t w = WS_STEP_FAST(img, st, b);
@@ -313,9 +335,14 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
       }
       uint32_t m_row;
       bool alive = slow_step(w, b, st, cold_row, first, rows, lane4, cls_s, tab, C, m_row);
-      if (m_row != 0xFFFFFFFFu) {
+      if (m_row != 0xFFFFFFFFu &&
+          (p.full_k || (m_row != seen0 && m_row != seen1 && m_row != seen2 && m_row != seen3))) {
         for (uint32_t j = __ldg(mp + m_row); j < __ldg(mp + m_row + 1); ++j)
           emit_k(p, __ldg(t.mlist + j), (uint32_t)s, (uint32_t)(e + 1));
+        seen3 = seen2;
+        seen2 = seen1;
+        seen1 = seen0;
+        seen0 = m_row;
       }
       if (!alive) break;
     }
@@ -492,6 +519,19 @@ __global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs 
       uint32_t w = __ldg(tab + st * C + __ldg(cm + __ldg(p.data + pos - 1)));
       if (w & F_DEAD) break;
       st = w & F_MASK;
+      if (p.rmark) {
+        // (pos - 1, g, st) fixes the rest of the walk: stop where another
+        // walk has been (it reports these starts), else leave a mark first
+        const uint32_t at = (uint32_t)(pos - 1);
+        const unsigned long long key =
+            ((unsigned long long)at << 32) | ((unsigned long long)g << kRmarkStateBits) | st;
+        // the state is hashed too: walks in different states at the same
+        // position (the two parities of (ab)+) must not evict each other
+        unsigned long long* slot =
+            p.rmark + ((at * 0x9E3779B1u ^ g * 0x7FEB352Du ^ st * 0x2C1B3C6Du) >> (32 - kRmarkBits));
+        if (*(volatile unsigned long long*)slot == key) break;
+        *slot = key;
+      }
       if (w & F_MATCH) {
         for (uint32_t j = __ldg(rmp + st); j < __ldg(rmp + st + 1); ++j)
           emit_k(p, __ldg(t.rmlist + j), (uint32_t)(pos - 1), ev.e);
@@ -535,49 +575,107 @@ __global__ void k_scatter_kernel(ScanPtrs p) {
   }
 }
 
-// Sorts each regex's starts ascending: bitonic sort in shared memory for
-// segments of up to 4096, an in-place block-wide odd-even transposition sort
-// in global memory beyond that.
+// Block-wide bitonic sort of buf[0, m) in shared memory (m a power of two).
+__device__ void bitonic_smem(uint32_t* buf, uint32_t m) {
+  for (uint32_t size = 2; size <= m; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        uint32_t j = k ^ stride;
+        if (j > k) {
+          bool up = (k & size) == 0;
+          uint32_t x = buf[k], y = buf[j];
+          if ((x > y) == up) { buf[k] = y; buf[j] = x; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Sorts src[0, n), n <= 4096, in place through shared memory.
+__device__ void sort_tile(uint32_t* buf, uint32_t* src, uint32_t n) {
+  uint32_t m = 1;
+  while (m < n) m <<= 1;
+  for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) buf[k] = (k < n) ? src[k] : 0xFFFFFFFFu;
+  __syncthreads();
+  bitonic_smem(buf, m);
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) src[k] = buf[k];
+  __syncthreads();
+}
+
+// Number of elements taken from A among the first `diag` of the merge of
+// sorted A and B (ties from A first).
+__device__ uint32_t merge_path(const uint32_t* A, uint32_t na, const uint32_t* B, uint32_t nb, uint32_t diag) {
+  uint32_t lo = diag > nb ? diag - nb : 0, hi = min(diag, na);
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (A[mid] <= B[diag - 1 - mid]) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Sorts each regex's starts ascending: a bitonic sort in shared memory for
+// segments of up to 4096; beyond that, sorted 4096-tiles merged pairwise in
+// global memory (merge-path split of each merge across the block), with the
+// lfend array -- written only after this kernel -- as the other buffer.
 __global__ void __launch_bounds__(512) k_sort_kernel(ScanPtrs p, uint32_t n_regex) {
   __shared__ uint32_t buf[4096];
   for (uint32_t r = blockIdx.x; r < n_regex; r += gridDim.x) {
     const uint32_t a = p.offs[r], n = p.offs[r + 1] - a;
     if (n <= 1) continue;
+    uint32_t* src = p.starts + a;
     if (n <= 4096) {
-      uint32_t m = 1;
-      while (m < n) m <<= 1;
-      for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) buf[k] = (k < n) ? p.starts[a + k] : 0xFFFFFFFFu;
-      __syncthreads();
-      for (uint32_t size = 2; size <= m; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-          for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
-            uint32_t j = k ^ stride;
-            if (j > k) {
-              bool up = (k & size) == 0;
-              uint32_t x = buf[k], y = buf[j];
-              if ((x > y) == up) { buf[k] = y; buf[j] = x; }
-            }
-          }
-          __syncthreads();
-        }
+      sort_tile(buf, src, n);
+      continue;
+    }
+    for (uint32_t t0 = 0; t0 < n; t0 += 4096) sort_tile(buf, src + t0, min(4096u, n - t0));
+    uint32_t* dst = p.lfend + a;
+    for (uint32_t w = 4096; w < n; w <<= 1) {
+      for (uint32_t lo = 0; lo < n; lo += 2 * w) {
+        const uint32_t mid = min(lo + w, n), hi = min(lo + 2 * w, n);
+        const uint32_t* A = src + lo;
+        const uint32_t* B = src + mid;
+        const uint32_t na = mid - lo, nb = hi - mid, total = hi - lo;
+        const uint32_t per = (total + blockDim.x - 1) / blockDim.x;
+        const uint32_t d0 = min(total, threadIdx.x * per), d1 = min(total, d0 + per);
+        uint32_t i = merge_path(A, na, B, nb, d0), j = d0 - i;
+        for (uint32_t d = d0; d < d1; ++d) dst[lo + d] = (j >= nb || (i < na && A[i] <= B[j])) ? A[i++] : B[j++];
       }
-      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) p.starts[a + k] = buf[k];
       __syncthreads();
-    } else {
-      uint32_t* s = p.starts + a;
-      for (uint32_t phase = 0; phase < n; ++phase) {
-        for (uint32_t k = 2 * threadIdx.x + (phase & 1); k + 1 < n; k += 2 * blockDim.x) {
-          uint32_t x = s[k], y = s[k + 1];
-          if (x > y) { s[k] = y; s[k + 1] = x; }
-        }
-        __syncthreads();
-      }
+      uint32_t* t = src;
+      src = dst;
+      dst = t;
+    }
+    if (src != p.starts + a) {
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) p.starts[a + k] = src[k];
+      __syncthreads();
     }
   }
 }
 
-// Leftmost-first end of every distinct candidate start (in parallel): walk the
-// regex's priority DFA from the start, remembering the last match position.
+// Leftmost-first end of a match of regex r from start s: the walk of the
+// regex's priority DFA from s, remembering the last match position, until the
+// DFA dies or the item or input ends.  kLfNone when no match starts at s;
+// kLfLong when the walk was cut off after `cap` bytes.
+__device__ uint32_t lf_walk(const DevTables& t, const ScanPtrs& p, uint32_t r, uint32_t s, uint64_t cap) {
+  const uint4 info = t.lfinfo[r];
+  const uint8_t* cm = t.cls + info.z * 256;
+  const uint32_t* tab = t.lf + info.x;
+  uint32_t st = info.y;
+  int64_t last = -1;
+  const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, s)) : p.len;
+  for (uint64_t pos = s; pos < stop; ++pos) {
+    if (pos - s == cap) return kLfLong;
+    uint32_t w = __ldg(tab + st * info.w + __ldg(cm + __ldg(p.data + pos)));
+    if (w & F_DEAD) break;
+    st = w & F_MASK;
+    if (w & F_MATCH) last = (int64_t)pos + 1;
+  }
+  return last < 0 ? kLfNone : (uint32_t)last;
+}
+
+// Leftmost-first end of every distinct candidate start (in parallel), each
+// walk cut off after kLfCap bytes.
 __global__ void k_lf_kernel(DevTables t, ScanPtrs p, uint32_t n_regex) {
   const uint32_t total = p.offs[n_regex];
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
@@ -589,20 +687,8 @@ __global__ void k_lf_kernel(DevTables t, ScanPtrs p, uint32_t n_regex) {
     }
     const uint32_t r = lo;
     const uint32_t s = p.starts[j];
-    if (j > p.offs[r] && p.starts[j - 1] == s) { p.lfend[j] = 0xFFFFFFFFu; continue; }  // duplicate
-    const uint4 info = t.lfinfo[r];
-    const uint8_t* cm = t.cls + info.z * 256;
-    const uint32_t* tab = t.lf + info.x;
-    uint32_t st = info.y;
-    int64_t last = -1;
-    const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, s)) : p.len;
-    for (uint64_t pos = s; pos < stop; ++pos) {
-      uint32_t w = __ldg(tab + st * info.w + __ldg(cm + __ldg(p.data + pos)));
-      if (w & F_DEAD) break;
-      st = w & F_MASK;
-      if (w & F_MATCH) last = (int64_t)pos + 1;
-    }
-    p.lfend[j] = last < 0 ? 0xFFFFFFFFu : (uint32_t)last;
+    if (j > p.offs[r] && p.starts[j - 1] == s) { p.lfend[j] = kLfNone; continue; }  // duplicate
+    p.lfend[j] = lf_walk(t, p, r, s, kLfCap);
   }
 }
 
@@ -625,17 +711,23 @@ __global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
   for (uint32_t j0 = a; j0 < b; j0 += 32) {
     const uint32_t j = j0 + lane;
     const bool in = j < b;
-    const uint32_t e = in ? p.lfend[j] : 0xFFFFFFFFu;
+    uint32_t e = in ? p.lfend[j] : kLfNone;
     const uint32_t s = in ? p.starts[j] : 0xFFFFFFFFu;
     const bool past = in && (uint64_t)s >= limit;
     bool picked = false;
     while (true) {
-      const bool ok = in && e != 0xFFFFFFFFu && (uint64_t)s >= last_end && !past;
+      const bool ok = in && e != kLfNone && (uint64_t)s >= last_end && !past;
       const unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
       if (!m) break;
       const int k = __ffs(m) - 1;
+      uint32_t ek = __shfl_sync(0xFFFFFFFFu, e, k);
+      if (ek == kLfLong) {  // the parallel walk was cut off: finish it here
+        if ((int)lane == k) e = lf_walk(t, p, r, s, ~0ull);
+        ek = __shfl_sync(0xFFFFFFFFu, e, k);
+        if (ek == kLfNone) continue;  // no match from that start after all
+      }
       picked |= (int)lane == k;
-      last_end = __shfl_sync(0xFFFFFFFFu, e, k);
+      last_end = ek;
     }
     // one output reservation per window of 32 candidates
     const unsigned pm = __ballot_sync(0xFFFFFFFFu, picked);
@@ -1011,6 +1103,7 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
 
   // device layout: reverse and leftmost-first tables, then the forward layout
   P.n_groups = (uint32_t)gbs.size();
+  P.rev_marks = P.n_groups < (1u << (32 - kRmarkStateBits));
   P.groups.assign(P.n_groups, GroupDev{});
   P.rev.clear(); P.lf.clear(); P.rmptr.clear(); P.rmlist.clear(); P.cls.clear();
   P.fdfa.clear(); P.fcls.clear(); P.gregex.clear(); P.nhot_u.clear(); P.nhot_a.clear();
@@ -1023,6 +1116,7 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
     const uint32_t C = (uint32_t)gb.cls.count;
     gd.rev_off = append_trans(gb.rev, P.rev);
     gd.rev_start = gb.rev.start_anchored;
+    if ((uint64_t)gb.rev.n_states >= (1ull << kRmarkStateBits)) P.rev_marks = false;
     gd.cls_off = g * 256;
     gd.rmptr_off = (uint32_t)P.rmptr.size();
     for (int s = 0; s < gb.rev.n_states; ++s) {
@@ -1150,6 +1244,17 @@ void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
 
 namespace {
 
+// Reverse-walk marks start empty in every scan (a stale mark would stop a
+// walk that no other walk continues); plans whose state numbers do not fit
+// the mark key run without them.
+void clear_marks(const RegexPlan& P, ScanPtrs& p, cudaStream_t st) {
+  if (!P.rev_marks || p.full_k) {
+    p.rmark = nullptr;
+    return;
+  }
+  check_cuda(cudaMemsetAsync(p.rmark, 0xFF, ((size_t)1 << kRmarkBits) * 8, st), "memset marks");
+}
+
 void ensure_scratch(DeviceBuffer& scratch, size_t need) {
   if (scratch.bytes >= need) return;
   size_t n = 1;
@@ -1167,6 +1272,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   DevTables t = dev_tables(P);
   uint32_t launches = 0;
+  clear_marks(P, p, st);
   check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");
   check_cuda(cudaMemsetAsync(p.count, 0, (size_t)P.n_regex * 4, st), "memset");
   if (ev) check_cuda(cudaEventRecord(ev[0], st), "event");
@@ -1204,11 +1310,15 @@ void regex_collect_timing(const RegexPlan& P, cudaEvent_t* ev, ws_matcher_info& 
 uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uint32_t mode, cudaStream_t st,
                           DeviceBuffer& scratch, int sm_count, ws_match* host_out, uint64_t cap) {
   if (!P.n_regex || len == 0) return 0;
+  const bool full = (mode & WS_CAND_DISTINCT) == 0;
+  mode &= ~(uint32_t)WS_CAND_DISTINCT;
   RegexLaunch l{d_data, len, nullptr, cap, nullptr, mode};
   RxLayout L = layout(P, len, P.walk_chunk, std::max<uint64_t>(cap, 1));
   ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
+  p.full_k = full ? 1 : 0;
   DevTables t = dev_tables(P);
+  clear_marks(P, p, st);
   check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");
   candidates_phase(P, t, p, mode, st, sm_count, nullptr);
   unsigned long long ctr[16];

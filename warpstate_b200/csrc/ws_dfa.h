@@ -56,6 +56,7 @@ struct RegexPlan {
   uint32_t total_states = 0;
   uint32_t max_classes = 0;
   int64_t max_len = 0;                   // longest match (-1 unbounded)
+  bool rev_marks = false;                // reverse walks may share visited-state marks
   std::vector<GroupDev> groups;
   std::vector<uint32_t> regex_group;     // regex index -> group
   // device tables

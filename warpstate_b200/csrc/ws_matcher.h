@@ -33,6 +33,8 @@ struct Scratch {
   DeviceBuffer lit;          // literal survivor list
   DeviceBuffer aux;          // batch item ends / tagged output
   DeviceBuffer out64;        // ws_match64 output of windowed scans
+  DeviceBuffer sorted;       // matches in their final order, read back from here
+  DeviceBuffer sortbuf;      // radix-sort keys, indices and temporary storage
   void* pinned = nullptr;    // pinned staging for pageable host input
   size_t pinned_bytes = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // [0], [1]: window copies; [2], [3]: staging slots drained
@@ -70,6 +72,20 @@ void ensure(DeviceBuffer& b, size_t need);
 void fill_err(ws_error_info* err, const Failure& f);
 bool is_pinned(const void* p);
 void sort_matches(ws_match* p, uint64_t n);
+
+// Device ordering of results (ws_sort.cu), for counts up to kMaxDeviceSorted;
+// larger counts are ordered on the host.  Input and output must not alias.
+constexpr uint64_t kMaxDeviceSorted = 0x7FFFFFFFull;
+// By (start, pattern_id, end).
+void sort_matches_device(Scratch& s, const ws_match* d_in, ws_match* d_out, uint64_t n, cudaStream_t st);
+// By (source_id, start, pattern_id, end).
+void sort_tagged_device(Scratch& s, const ws_tagged_match* d_in, ws_tagged_match* d_out, uint64_t n,
+                        cudaStream_t st);
+// 64-bit offsets to 32-bit ones (inputs below 4 GiB).
+void narrow_matches_device(const ws_match64* d_in, ws_match* d_out, uint64_t n, cudaStream_t st);
+// Reads `count` device results into host `out` in (start, pattern_id, end)
+// order, through the scratch's stream; returns when they have arrived.
+void read_sorted(Scratch& s, const ws_match* d_res, uint64_t count, ws_match* out);
 
 }  // namespace ws
 

@@ -86,8 +86,7 @@ void finish_window(ws_stream* st) {
   if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one stream piece", 0, count, dcap);
   if (count) {
     st->host.resize(count);
-    check_cuda(cudaMemcpy(st->host.data(), s.out.ptr, count * sizeof(ws_match), cudaMemcpyDeviceToHost), "D2H");
-    sort_matches(st->host.data(), count);
+    read_sorted(s, s.out.as<ws_match>(), count, st->host.data());
     for (const ws_match& mm : st->host) {
       ws_match64 o;
       o.pattern_id = mm.pattern_id;
