@@ -69,6 +69,7 @@ struct LitArgs {
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
   const uint32_t* big;       // stage-1b gram table (2^kBigBits nibbles, L2), or null
+  uint32_t verify_bloom;     // the verify kernel runs stage 1.5 first
 };
 
 __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint32_t bits) {
@@ -528,12 +529,193 @@ __global__ void __launch_bounds__(kBigThreads, 1) literal_filter_big_kernel(LitA
   }
 }
 
+// ------------------------------------------------------------- lean kernel
+// P = 4, 4-byte grams, stage-1b table present, no literals shorter than 4
+// bytes (the large-set layout).  Stage 1.5 moves to the verify kernel, so the
+// filter only hashes, looks up and appends:
+//   - ownership is shifted by 3: the lane with the 16 bytes at `base` owns the
+//     start positions base-3 .. base+12, whose first 4-aligned position is one
+//     of its own four words, so its own four grams decide all of them (bit t of
+//     n0 | n1 << 4 | n2 << 8 | n3 << 12 is position base - 3 + t) and no lane
+//     needs its neighbour's bytes.  The last three positions of the input start
+//     no literal of 4 or more bytes;
+//   - stage 1 and the stage-1b loads run one warp block ahead of the block
+//     being finished, the input two blocks ahead;
+//   - the stage-1b survivors of a warp block (about 0.3 per 512 bytes on
+//     10,000 literals) are appended with one atomic per warp.
+constexpr int kLeanThreads = 1024;
+constexpr int kLeanDepth = 1;  // blocks of stage-1b loads in flight ahead of the one finished
+
+// Bytes [a, a + 4) of the input, zero past its end.
+__device__ __forceinline__ uint32_t word_at(const uint8_t* d, uint32_t len, uint32_t a) {
+  if (a + 4 <= len) return __ldg(reinterpret_cast<const uint32_t*>(d + a));
+  uint32_t x = 0;
+  for (uint32_t k = 0; k < 4; ++k)
+    if (a + k < len) x |= (uint32_t)__ldg(d + a + k) << (8 * k);
+  return x;
+}
+
+struct LeanGrams {
+  uint32_t hf[4], n[4], bw[4];
+};
+
+// Stage 1 of a lane's four aligned grams, stage-1b loads issued.
+__device__ __forceinline__ void lean_issue(const uint32_t* filt, const uint32_t* big, uint32_t bits, const uint4& v,
+                                           LeanGrams& g) {
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    g.hf[q] = w[q] * 0x9E3779B1u;
+    const uint32_t hs = g.hf[q] >> (32 - bits);
+    g.n[q] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
+    g.bw[q] = g.n[q] ? __ldg(big + ((g.hf[q] >> (32 - kBigBits)) >> 3)) : 0u;
+  }
+}
+
+// Candidate mask of positions base-3 .. base+12 inside [0, len).
+__device__ __forceinline__ uint32_t lean_finish(const LeanGrams& g, uint32_t base, uint32_t len) {
+  uint32_t mask = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) mask |= (g.n[q] & (g.bw[q] >> (((g.hf[q] >> (32 - kBigBits)) & 7) << 2))) << (4 * q);
+  if (base == 0) mask &= ~7u;  // positions -3 .. -1
+  if (base + 13 > len) {
+    const uint32_t valid = len + 3 > base ? len + 3 - base : 0;
+    mask &= valid >= 16 ? 0xFFFFu : ((1u << valid) - 1u);
+  }
+  return mask;
+}
+
+// Survivor slots are reserved per warp, kLeanChunk at a time, so that the
+// single global counter sees one atomic per chunk rather than one per warp
+// block; slots a warp reserved but did not fill hold kNoSurvivor.
+constexpr uint32_t kLeanChunk = 32;
+constexpr uint32_t kNoSurvivor = 0xFFFFFFFFu;  // no position: inputs end below 2^32 - 64
+
+struct LeanSlots {
+  unsigned long long next = 0, end = 0;  // the warp's reserved range [next, end)
+};
+
+// Marks the warp's unfilled reserved slots as holes.
+__device__ __forceinline__ void lean_holes(const LitArgs& a, const LeanSlots& r, uint32_t lane) {
+  for (unsigned long long k = r.next + lane; k < r.end && k < a.survivor_cap; k += 32) a.survivors[k] = kNoSurvivor;
+}
+
+__device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, uint32_t mask, uint32_t base,
+                                            uint32_t lane) {
+  if (__ballot_sync(0xFFFFFFFFu, mask != 0) == 0) return;
+  const uint32_t cnt = __popc(mask);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (r.next + total > r.end) {  // warp-uniform: reserve a new chunk
+    lean_holes(a, r, lane);
+    const unsigned long long want = total > kLeanChunk ? total : kLeanChunk;
+    unsigned long long wb = 0;
+    if (lane == 0) wb = atomicAdd(a.survivor_count, want);
+    wb = __shfl_sync(0xFFFFFFFFu, wb, 0);
+    r.next = wb;
+    r.end = wb + want;
+  }
+  unsigned long long slot = r.next + incl - cnt;
+  r.next += total;
+  while (mask) {
+    const uint32_t t = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const uint32_t s = base - 3 + t;
+    if (slot < a.survivor_cap) a.survivors[slot] = s;
+    else verify_position(a, s);  // list full: verify in place
+    ++slot;
+  }
+}
+
+__global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a) {
+  constexpr uint32_t W = kLeanThreads / 32;
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* filt = smem;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.filter);
+    uint4* dst = reinterpret_cast<uint4*>(filt);
+    for (uint32_t k = threadIdx.x; k < a.filter_words / 4; k += kLeanThreads) dst[k] = __ldg(src + k);
+  }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t len = (uint32_t)a.len;
+  const uint32_t nvec = (uint32_t)((a.len + 15) >> 4);
+  const uint32_t full_vecs = len >> 4;
+  const uint32_t nblk = (nvec + 31) >> 5;
+  const uint32_t nw = gridDim.x * W;
+  const uint32_t bits = a.bits;
+  const uint32_t* big = a.big;
+  const uint4 zero = make_uint4(0, 0, 0, 0);
+  auto load = [&](uint32_t blk) -> uint4 {
+    const uint32_t v = blk * 32 + lane;
+    if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
+    return v < nvec ? load_vec(a.data, a.len, v) : zero;
+  };
+  uint32_t b = blockIdx.x * W + warp;
+  LeanSlots slots;
+  if (kLeanDepth == 1) {
+    uint4 vn = b + nw < nblk ? load(b + nw) : zero;
+    LeanGrams gc;
+    if (b < nblk) lean_issue(filt, big, bits, load(b), gc);
+#pragma unroll 2
+    for (; b < nblk; b += nw) {
+      const uint32_t b1 = b + nw, b2 = b1 + nw;
+      const uint4 vn2 = b2 < nblk ? load(b2) : zero;
+      LeanGrams gn;
+      if (b1 < nblk) lean_issue(filt, big, bits, vn, gn);
+      const uint32_t base = b * 512 + lane * 16;
+      lean_append(a, slots, lean_finish(gc, base, len), base, lane);
+      gc = gn;
+      vn = vn2;
+    }
+  } else {
+    // stage 1b of blocks b + nw and b + 2 nw in flight, input of b + 3 nw
+    LeanGrams g0, g1;
+    if (b < nblk) lean_issue(filt, big, bits, load(b), g0);
+    if (b + nw < nblk) lean_issue(filt, big, bits, load(b + nw), g1);
+    uint4 vin = b + 2 * nw < nblk ? load(b + 2 * nw) : zero;
+    for (; b < nblk; b += nw) {
+      const uint32_t b2 = b + 2 * nw, b3 = b2 + nw;
+      const uint4 vnext = b3 < nblk ? load(b3) : zero;
+      LeanGrams g2;
+      if (b2 < nblk) lean_issue(filt, big, bits, vin, g2);
+      const uint32_t base = b * 512 + lane * 16;
+      lean_append(a, slots, lean_finish(g0, base, len), base, lane);
+      g0 = g1;
+      g1 = g2;
+      vin = vnext;
+    }
+  }
+  lean_holes(a, slots, lane);
+}
+
 __global__ void __launch_bounds__(256) literal_verify_kernel(LitArgs a) {
   unsigned long long n = *a.survivor_count;
   if (n > a.survivor_cap) n = a.survivor_cap;
   for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (unsigned long long)gridDim.x * blockDim.x)
-    verify_position(a, a.survivors[k]);
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t s = a.survivors[k];
+    if (s == kNoSurvivor) continue;  // a slot the lean kernel reserved but did not fill
+    if (a.verify_bloom) {  // stage 1.5 for survivors of the lean kernel
+      const uint32_t len = (uint32_t)a.len, w0 = s & ~3u, sh = (s & 3) * 8;
+      const uint32_t x0 = word_at(a.data, len, w0), x1 = word_at(a.data, len, w0 + 4),
+                     x2 = word_at(a.data, len, w0 + 8);
+      const uint32_t lo = __funnelshift_r(x0, x1, sh), hi = __funnelshift_r(x1, x2, sh);
+      bool keep = false;
+      for (uint32_t m = a.parts; m; m &= m - 1) {
+        const uint32_t key = prefix_key(lo, hi, __ffs(m));
+        keep |= (__ldg(a.bloom + (key >> 5)) >> (key & 31)) & 1u;
+      }
+      if (!keep) continue;
+    }
+    verify_position(a, s);
+  }
 }
 
 }  // namespace
@@ -580,6 +762,7 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
   a.big = plan.big.empty() ? nullptr : plan.d_big.as<uint32_t>();
+  a.verify_bloom = 0;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   if (l.len > 0xFFFFFFFFull) raise(WS_ERR_INPUT_TOO_LARGE, "literal scan launch beyond 32-bit offsets", 0, l.len,
                                    0xFFFFFFFFull);
@@ -603,7 +786,14 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   };
   // the pipelined kernel pays off for 4-byte grams (measured); long grams,
   // whose hashing dominates, keep 32 warps per SM
-  if (lg && a.big && plan.period == 4 && plan.gram_len == 4) {
+  if (lg && !sh && a.big && plan.period == 4 && plan.gram_len == 4) {
+    a.verify_bloom = 1;
+    const size_t lsmem = (size_t)a.filter_words * 4;
+    check_cuda(cudaFuncSetAttribute(literal_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
+               "cudaFuncSetAttribute(literal lean)");
+    literal_lean_kernel<<<sm_count, kLeanThreads, lsmem, st>>>(a);
+    check_cuda(cudaGetLastError(), "literal_lean_kernel launch");
+  } else if (lg && a.big && plan.period == 4 && plan.gram_len == 4) {
     sh ? run_big(literal_filter_big_kernel<4, true>) : run_big(literal_filter_big_kernel<4, false>);
   } else if (!lg) {
     run(literal_filter_kernel<4, 4, false, true>);
