@@ -107,15 +107,17 @@ struct LiteralPlan {
   uint32_t parts16 = 0;               // bit i: some literal has a key of i+1 bytes (<= 16)
   std::vector<uint32_t> bloom2;       // 2^kBloom2Bits bits, only when gram_len > 4
   // Large pattern sets fill the shared-memory gram table: a second table of
-  // 2^kBigBits nibbles in L2 (same hashes, more bits) re-checks every gram
-  // that passes it (stage 1b).  Empty when the shared table is sparse enough.
-  std::vector<uint32_t> big;
+  // 2^kBigBits bytes in L2 (same hashes, more bits; each byte holds the P
+  // phase bits of its hash, so a lookup is one byte load) re-checks every
+  // gram that passes it (stage 1b).  Empty when the shared table is sparse
+  // enough.
+  std::vector<uint8_t> big;
   DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2, d_big;
   uint32_t n_buckets = 0;
 };
 
 constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
-constexpr uint32_t kBigBits = 24;     // stage-1b table: 2^24 nibbles, 8 MiB, read through L2
+constexpr uint32_t kBigBits = 24;     // stage-1b table: 2^24 bytes, 16 MiB, read through L2
 
 // Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).
 inline uint32_t gram_hash(uint32_t gram, uint32_t bits) { return (gram * 0x9E3779B1u) >> (32 - bits); }

@@ -207,14 +207,14 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
     }
   }
   // Stage 1b: when more than 0.5% of the shared table's phase bits are set,
-  // a 2^kBigBits-nibble table in L2 (the same full 32-bit gram hashes, more
+  // a 2^kBigBits-byte table in L2 (the same full 32-bit gram hashes, more
   // of their bits) re-checks each passing gram.
   if (plan.has_long && P == 4) {
     uint64_t set = 0;
     for (uint32_t w : plan.filter) set += (uint64_t)__builtin_popcount(w);
     if ((double)set / (double)((uint64_t)plan.filter.size() * 32) > 0.005) {
       const uint32_t G = plan.gram_len;
-      plan.big.assign((size_t)1 << (kBigBits - 3), 0u);
+      plan.big.assign((size_t)1 << kBigBits, 0);
       for (uint32_t li = 0; li < t.n_literals; ++li) {
         const uint32_t len = t.offsets[2 * li + 1];
         const uint8_t* lit = t.packed_bytes + t.offsets[2 * li];
@@ -226,10 +226,10 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
                               : G == 8 ? mix_words(g[0], g[1], 0, 0, 8)
                                        : mix_words(g[0], g[1], g[2], g[3], 16);
           const uint32_t h = hf >> (32 - kBigBits);
-          plan.big[h >> 3] |= (1u << (P - 1 - k)) << ((h & 7) * 4);
+          plan.big[h] |= (uint8_t)(1u << (P - 1 - k));
         }
       }
-      plan.d_big.upload(plan.big.data(), plan.big.size() * 4);
+      plan.d_big.upload(plan.big.data(), plan.big.size());
     }
   }
   plan.n_buckets = t.n_buckets;

@@ -68,7 +68,7 @@ struct LitArgs {
   uint32_t gram_len;        // stage-1 gram bytes: 4, 8 or 16 (8 and 16 with P = 4)
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
-  const uint32_t* big;       // stage-1b gram table (2^kBigBits nibbles, L2), or null
+  const uint8_t* big;        // stage-1b gram table (2^kBigBits bytes, L2), or null
   uint32_t verify_bloom;     // the verify kernel runs stage 1.5 first
 };
 
@@ -80,10 +80,9 @@ __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint
 // Stage 1b: a nibble that passed the shared-memory table is checked again in
 // the larger table in L2 (same gram hash, more bits), only where it is
 // non-zero: one predicated load per passing gram.
-__device__ __forceinline__ uint32_t nib_big(const uint32_t* big, uint32_t h_full, uint32_t n) {
+__device__ __forceinline__ uint32_t nib_big(const uint8_t* big, uint32_t h_full, uint32_t n) {
   if (!n) return 0;
-  const uint32_t h = h_full >> (32 - kBigBits);
-  return n & ((__ldg(big + (h >> 3)) >> ((h & 7) << 2)) & 0xFu);
+  return n & __ldg(big + (h_full >> (32 - kBigBits)));
 }
 
 // Loads the 16 bytes of vector v, zero-filling past the end of the input.
@@ -142,7 +141,7 @@ __device__ void verify_position(const LitArgs& a, uint64_t s) {
 // G = gram bytes, LONG / SHORT = literals of >= 4 / < 4 bytes present).
 template <int P, int G, bool LONG, bool SHORT>
 __device__ __forceinline__ uint32_t stage1(const uint32_t* filt, const uint32_t* shortb, const uint32_t (&w)[8],
-                                           uint32_t lane, uint32_t bits, const uint32_t* big) {
+                                           uint32_t lane, uint32_t bits, const uint8_t* big) {
   uint32_t mask = 0;
   if (LONG) {
     if (G > 4 || P == 4) {
@@ -373,7 +372,7 @@ struct Grams {
 };
 
 template <int G>
-__device__ __forceinline__ void grams_issue(const uint32_t* filt, const uint32_t* big, const uint32_t (&w)[8],
+__device__ __forceinline__ void grams_issue(const uint32_t* filt, const uint8_t* big, const uint32_t (&w)[8],
                                             uint32_t lane, uint32_t bits, Grams& s) {
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
@@ -390,14 +389,14 @@ __device__ __forceinline__ void grams_issue(const uint32_t* filt, const uint32_t
     const uint32_t hs = hf >> (32 - bits);
     s.h[j] = hf;
     s.n[j] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
-    s.bw[j] = s.n[j] ? __ldg(big + ((hf >> (32 - kBigBits)) >> 3)) : 0u;
+    s.bw[j] = s.n[j] ? __ldg(big + (hf >> (32 - kBigBits))) : 0u;
   }
 }
 
 __device__ __forceinline__ uint32_t grams_finish(const Grams& s, uint32_t lane) {
   uint32_t n[5];
 #pragma unroll
-  for (int j = 0; j < 5; ++j) n[j] = s.n[j] & (s.bw[j] >> (((s.h[j] >> (32 - kBigBits)) & 7) << 2));
+  for (int j = 0; j < 5; ++j) n[j] = s.n[j] & s.bw[j];
   const uint32_t n4 = __shfl_down_sync(0xFFFFFFFFu, n[0], 1);
   const uint32_t m = n[0] | (n[1] << 4) | (n[2] << 8) | (n[3] << 12) | ((lane == 31 ? n[4] : n4) << 16);
   return (m >> 3) & 0xFFFFu;
@@ -556,19 +555,21 @@ __device__ __forceinline__ uint32_t word_at(const uint8_t* d, uint32_t len, uint
 }
 
 struct LeanGrams {
-  uint32_t hf[4], n[4], bw[4];
+  uint32_t n[4], bw[4];
 };
 
 // Stage 1 of a lane's four aligned grams, stage-1b loads issued.
-__device__ __forceinline__ void lean_issue(const uint32_t* filt, const uint32_t* big, uint32_t bits, const uint4& v,
-                                           LeanGrams& g) {
+// sh_word = 35 - bits and sh_nib = 30 - bits index the nibble table by the
+// top `bits` bits of the hash: word hf >> sh_word, nibble shift
+// (hf >> sh_nib) & 28.
+__device__ __forceinline__ void lean_issue(const uint32_t* filt, const uint8_t* big, uint32_t sh_word,
+                                           uint32_t sh_nib, const uint4& v, LeanGrams& g) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    g.hf[q] = w[q] * 0x9E3779B1u;
-    const uint32_t hs = g.hf[q] >> (32 - bits);
-    g.n[q] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
-    g.bw[q] = g.n[q] ? __ldg(big + ((g.hf[q] >> (32 - kBigBits)) >> 3)) : 0u;
+    const uint32_t hf = w[q] * 0x9E3779B1u;
+    g.n[q] = (filt[hf >> sh_word] >> ((hf >> sh_nib) & 28u)) & 0xFu;
+    g.bw[q] = g.n[q] ? __ldg(big + (hf >> (32 - kBigBits))) : 0u;
   }
 }
 
@@ -576,7 +577,7 @@ __device__ __forceinline__ void lean_issue(const uint32_t* filt, const uint32_t*
 __device__ __forceinline__ uint32_t lean_finish(const LeanGrams& g, uint32_t base, uint32_t len) {
   uint32_t mask = 0;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) mask |= (g.n[q] & (g.bw[q] >> (((g.hf[q] >> (32 - kBigBits)) & 7) << 2))) << (4 * q);
+  for (int q = 0; q < 4; ++q) mask |= (g.n[q] & g.bw[q]) << (4 * q);
   if (base == 0) mask &= ~7u;  // positions -3 .. -1
   if (base + 13 > len) {
     const uint32_t valid = len + 3 > base ? len + 3 - base : 0;
@@ -649,8 +650,8 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   const uint32_t full_vecs = len >> 4;
   const uint32_t nblk = (nvec + 31) >> 5;
   const uint32_t nw = gridDim.x * W;
-  const uint32_t bits = a.bits;
-  const uint32_t* big = a.big;
+  const uint32_t sh_word = 35 - a.bits, sh_nib = 30 - a.bits;
+  const uint8_t* big = a.big;
   const uint4 zero = make_uint4(0, 0, 0, 0);
   auto load = [&](uint32_t blk) -> uint4 {
     const uint32_t v = blk * 32 + lane;
@@ -662,13 +663,13 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   if (kLeanDepth == 1) {
     uint4 vn = b + nw < nblk ? load(b + nw) : zero;
     LeanGrams gc;
-    if (b < nblk) lean_issue(filt, big, bits, load(b), gc);
+    if (b < nblk) lean_issue(filt, big, sh_word, sh_nib, load(b), gc);
 #pragma unroll 2
     for (; b < nblk; b += nw) {
       const uint32_t b1 = b + nw, b2 = b1 + nw;
       const uint4 vn2 = b2 < nblk ? load(b2) : zero;
       LeanGrams gn;
-      if (b1 < nblk) lean_issue(filt, big, bits, vn, gn);
+      if (b1 < nblk) lean_issue(filt, big, sh_word, sh_nib, vn, gn);
       const uint32_t base = b * 512 + lane * 16;
       lean_append(a, slots, lean_finish(gc, base, len), base, lane);
       gc = gn;
@@ -677,14 +678,14 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   } else {
     // stage 1b of blocks b + nw and b + 2 nw in flight, input of b + 3 nw
     LeanGrams g0, g1;
-    if (b < nblk) lean_issue(filt, big, bits, load(b), g0);
-    if (b + nw < nblk) lean_issue(filt, big, bits, load(b + nw), g1);
+    if (b < nblk) lean_issue(filt, big, sh_word, sh_nib, load(b), g0);
+    if (b + nw < nblk) lean_issue(filt, big, sh_word, sh_nib, load(b + nw), g1);
     uint4 vin = b + 2 * nw < nblk ? load(b + 2 * nw) : zero;
     for (; b < nblk; b += nw) {
       const uint32_t b2 = b + 2 * nw, b3 = b2 + nw;
       const uint4 vnext = b3 < nblk ? load(b3) : zero;
       LeanGrams g2;
-      if (b2 < nblk) lean_issue(filt, big, bits, vin, g2);
+      if (b2 < nblk) lean_issue(filt, big, sh_word, sh_nib, vin, g2);
       const uint32_t base = b * 512 + lane * 16;
       lean_append(a, slots, lean_finish(g0, base, len), base, lane);
       g0 = g1;
@@ -761,7 +762,7 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.gram_len = plan.gram_len;
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
-  a.big = plan.big.empty() ? nullptr : plan.d_big.as<uint32_t>();
+  a.big = plan.big.empty() ? nullptr : plan.d_big.as<uint8_t>();
   a.verify_bloom = 0;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   if (l.len > 0xFFFFFFFFull) raise(WS_ERR_INPUT_TOO_LARGE, "literal scan launch beyond 32-bit offsets", 0, l.len,
