@@ -366,7 +366,11 @@ def main():
     # roofline of the dominant kernel
     peak, peak_kind = load_peaks()
     has_regex = any(k == 1 for k, _ in wl.patterns)
-    kidx, kname = (1, "dfa_walk_kernel") if has_regex else (0, "literal_filter_kernel")
+    # the literal phase (index 0) spans the filter and the verify kernel; the
+    # 10,000-literal set takes the large-set layout (stage-1b table, no literals
+    # under 4 bytes), whose filter is literal_lean_kernel
+    kidx, kname = ((1, "dfa_walk_kernel") if has_regex else
+                   (0, "literal_lean_kernel") if args.config == "literals_large" else (0, "literal_filter_kernel"))
     kms = statistics.mean(i["last_kernel_ms"][kidx] for i in infos) if infos else None
     alg_bytes = n_bytes + 12 * count + (16 * n_items if batch else 0)
     achieved = alg_bytes / (kms * 1e-3) / 1e9 if kms else None
