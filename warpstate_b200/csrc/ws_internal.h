@@ -112,12 +112,18 @@ struct LiteralPlan {
   // gram that passes it (stage 1b).  Empty when the shared table is sparse
   // enough.
   std::vector<uint8_t> big;
-  DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2, d_big;
+  // With the stage-1b table: stage 1 of the lean kernel as bytes, indexed by
+  // the top kFilter8Bits bits of the same hashes (the OR of the 2^7 stage-1b
+  // bytes below each entry), so a lookup needs no nibble extract.
+  std::vector<uint8_t> filter8;
+  DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2, d_big,
+      d_filter8;
   uint32_t n_buckets = 0;
 };
 
 constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
 constexpr uint32_t kBigBits = 24;     // stage-1b table: 2^24 bytes, 16 MiB, read through L2
+constexpr uint32_t kFilter8Bits = 17; // byte-wide stage 1 of the lean kernel: 128 KiB of shared memory
 
 // Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).
 inline uint32_t gram_hash(uint32_t gram, uint32_t bits) { return (gram * 0x9E3779B1u) >> (32 - bits); }

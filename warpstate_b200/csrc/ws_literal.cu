@@ -69,6 +69,7 @@ struct LitArgs {
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
   const uint8_t* big;        // stage-1b gram table (2^kBigBits bytes, L2), or null
+  const uint8_t* filter8;    // byte-wide stage 1 of the lean kernel (2^kFilter8Bits), or null
   uint32_t verify_bloom;     // the verify kernel runs stage 1.5 first
 };
 
@@ -559,16 +560,14 @@ struct LeanGrams {
 };
 
 // Stage 1 of a lane's four aligned grams, stage-1b loads issued.
-// sh_word = 35 - bits and sh_nib = 30 - bits index the nibble table by the
-// top `bits` bits of the hash: word hf >> sh_word, nibble shift
-// (hf >> sh_nib) & 28.
-__device__ __forceinline__ void lean_issue(const uint32_t* filt, const uint8_t* big, uint32_t sh_word,
-                                           uint32_t sh_nib, const uint4& v, LeanGrams& g) {
+// Stage 1 from the byte table in shared memory (top kFilter8Bits bits of the
+// hash), stage 1b from the byte table in L2 (top kBigBits bits).
+__device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint32_t hf = w[q] * 0x9E3779B1u;
-    g.n[q] = (filt[hf >> sh_word] >> ((hf >> sh_nib) & 28u)) & 0xFu;
+    g.n[q] = filt[hf >> (32 - kFilter8Bits)];
     g.bw[q] = g.n[q] ? __ldg(big + (hf >> (32 - kBigBits))) : 0u;
   }
 }
@@ -635,12 +634,12 @@ __device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, uint
 
 __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a) {
   constexpr uint32_t W = kLeanThreads / 32;
-  extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t* filt = smem;
+  extern __shared__ __align__(16) uint8_t smem8[];
+  uint8_t* filt = smem8;
   {
-    const uint4* src = reinterpret_cast<const uint4*>(a.filter);
+    const uint4* src = reinterpret_cast<const uint4*>(a.filter8);
     uint4* dst = reinterpret_cast<uint4*>(filt);
-    for (uint32_t k = threadIdx.x; k < a.filter_words / 4; k += kLeanThreads) dst[k] = __ldg(src + k);
+    for (uint32_t k = threadIdx.x; k < (1u << (kFilter8Bits - 4)); k += kLeanThreads) dst[k] = __ldg(src + k);
   }
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31;
@@ -650,7 +649,6 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   const uint32_t full_vecs = len >> 4;
   const uint32_t nblk = (nvec + 31) >> 5;
   const uint32_t nw = gridDim.x * W;
-  const uint32_t sh_word = 35 - a.bits, sh_nib = 30 - a.bits;
   const uint8_t* big = a.big;
   const uint4 zero = make_uint4(0, 0, 0, 0);
   auto load = [&](uint32_t blk) -> uint4 {
@@ -663,13 +661,13 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   if (kLeanDepth == 1) {
     uint4 vn = b + nw < nblk ? load(b + nw) : zero;
     LeanGrams gc;
-    if (b < nblk) lean_issue(filt, big, sh_word, sh_nib, load(b), gc);
+    if (b < nblk) lean_issue(filt, big, load(b), gc);
 #pragma unroll 2
     for (; b < nblk; b += nw) {
       const uint32_t b1 = b + nw, b2 = b1 + nw;
       const uint4 vn2 = b2 < nblk ? load(b2) : zero;
       LeanGrams gn;
-      if (b1 < nblk) lean_issue(filt, big, sh_word, sh_nib, vn, gn);
+      if (b1 < nblk) lean_issue(filt, big, vn, gn);
       const uint32_t base = b * 512 + lane * 16;
       lean_append(a, slots, lean_finish(gc, base, len), base, lane);
       gc = gn;
@@ -678,14 +676,14 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   } else {
     // stage 1b of blocks b + nw and b + 2 nw in flight, input of b + 3 nw
     LeanGrams g0, g1;
-    if (b < nblk) lean_issue(filt, big, sh_word, sh_nib, load(b), g0);
-    if (b + nw < nblk) lean_issue(filt, big, sh_word, sh_nib, load(b + nw), g1);
+    if (b < nblk) lean_issue(filt, big, load(b), g0);
+    if (b + nw < nblk) lean_issue(filt, big, load(b + nw), g1);
     uint4 vin = b + 2 * nw < nblk ? load(b + 2 * nw) : zero;
     for (; b < nblk; b += nw) {
       const uint32_t b2 = b + 2 * nw, b3 = b2 + nw;
       const uint4 vnext = b3 < nblk ? load(b3) : zero;
       LeanGrams g2;
-      if (b2 < nblk) lean_issue(filt, big, sh_word, sh_nib, vin, g2);
+      if (b2 < nblk) lean_issue(filt, big, vin, g2);
       const uint32_t base = b * 512 + lane * 16;
       lean_append(a, slots, lean_finish(g0, base, len), base, lane);
       g0 = g1;
@@ -763,6 +761,7 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
   a.big = plan.big.empty() ? nullptr : plan.d_big.as<uint8_t>();
+  a.filter8 = plan.filter8.empty() ? nullptr : plan.d_filter8.as<uint8_t>();
   a.verify_bloom = 0;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   if (l.len > 0xFFFFFFFFull) raise(WS_ERR_INPUT_TOO_LARGE, "literal scan launch beyond 32-bit offsets", 0, l.len,
@@ -787,9 +786,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   };
   // the pipelined kernel pays off for 4-byte grams (measured); long grams,
   // whose hashing dominates, keep 32 warps per SM
-  if (lg && !sh && a.big && plan.period == 4 && plan.gram_len == 4) {
+  if (lg && !sh && a.big && a.filter8 && plan.period == 4 && plan.gram_len == 4) {
     a.verify_bloom = 1;
-    const size_t lsmem = (size_t)a.filter_words * 4;
+    const size_t lsmem = (size_t)1 << kFilter8Bits;
     check_cuda(cudaFuncSetAttribute(literal_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
                "cudaFuncSetAttribute(literal lean)");
     literal_lean_kernel<<<sm_count, kLeanThreads, lsmem, st>>>(a);
