@@ -539,12 +539,14 @@ __global__ void __launch_bounds__(kBigThreads, 1) literal_filter_big_kernel(LitA
 //     n0 | n1 << 4 | n2 << 8 | n3 << 12 is position base - 3 + t) and no lane
 //     needs its neighbour's bytes.  The last three positions of the input start
 //     no literal of 4 or more bytes;
-//   - stage 1 and the stage-1b loads run one warp block ahead of the block
-//     being finished, the input two blocks ahead;
+//   - a warp step covers kLeanVecs coalesced 512-byte halves (32 bytes per
+//     lane), so the per-step overhead is paid once per kLeanVecs x 512 bytes;
+//   - stage 1 and the stage-1b loads run one warp step ahead of the step
+//     being finished, the input two steps ahead;
 //   - the stage-1b survivors of a warp block (about 0.3 per 512 bytes on
 //     10,000 literals) are appended with one atomic per warp.
 constexpr int kLeanThreads = 1024;
-constexpr int kLeanDepth = 1;  // blocks of stage-1b loads in flight ahead of the one finished
+constexpr int kLeanVecs = 2;  // 16-byte vectors per lane per warp step (a step covers kLeanVecs x 512 bytes)
 
 // Bytes [a, a + 4) of the input, zero past its end.
 __device__ __forceinline__ uint32_t word_at(const uint8_t* d, uint32_t len, uint32_t a) {
@@ -600,10 +602,16 @@ __device__ __forceinline__ void lean_holes(const LitArgs& a, const LeanSlots& r,
   for (unsigned long long k = r.next + lane; k < r.end && k < a.survivor_cap; k += 32) a.survivors[k] = kNoSurvivor;
 }
 
-__device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, uint32_t mask, uint32_t base,
-                                            uint32_t lane) {
-  if (__ballot_sync(0xFFFFFFFFu, mask != 0) == 0) return;
-  const uint32_t cnt = __popc(mask);
+template <int V>
+__device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, const uint32_t (&mask)[V],
+                                            const uint32_t (&base)[V], uint32_t lane) {
+  uint32_t any = 0, cnt = 0;
+#pragma unroll
+  for (int h = 0; h < V; ++h) {
+    any |= mask[h];
+    cnt += __popc(mask[h]);
+  }
+  if (__ballot_sync(0xFFFFFFFFu, any != 0) == 0) return;
   uint32_t incl = cnt;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
@@ -622,18 +630,19 @@ __device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, uint
   }
   unsigned long long slot = r.next + incl - cnt;
   r.next += total;
-  while (mask) {
-    const uint32_t t = __ffs(mask) - 1;
-    mask &= mask - 1;
-    const uint32_t s = base - 3 + t;
-    if (slot < a.survivor_cap) a.survivors[slot] = s;
-    else verify_position(a, s);  // list full: verify in place
-    ++slot;
+#pragma unroll
+  for (int h = 0; h < V; ++h) {
+    for (uint32_t m = mask[h]; m; m &= m - 1) {
+      const uint32_t s = base[h] - 3 + (__ffs(m) - 1);
+      if (slot < a.survivor_cap) a.survivors[slot] = s;
+      else verify_position(a, s);  // list full: verify in place
+      ++slot;
+    }
   }
 }
 
 __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a) {
-  constexpr uint32_t W = kLeanThreads / 32;
+  constexpr uint32_t W = kLeanThreads / 32, V = kLeanVecs;
   extern __shared__ __align__(16) uint8_t smem8[];
   uint8_t* filt = smem8;
   {
@@ -647,48 +656,44 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   const uint32_t len = (uint32_t)a.len;
   const uint32_t nvec = (uint32_t)((a.len + 15) >> 4);
   const uint32_t full_vecs = len >> 4;
-  const uint32_t nblk = (nvec + 31) >> 5;
+  const uint32_t nblk = (nvec + 32 * V - 1) / (32 * V);  // warp steps of V * 512 bytes
   const uint32_t nw = gridDim.x * W;
   const uint8_t* big = a.big;
   const uint4 zero = make_uint4(0, 0, 0, 0);
-  auto load = [&](uint32_t blk) -> uint4 {
-    const uint32_t v = blk * 32 + lane;
+  // half h of warp step blk: the 512 coalesced bytes at (blk * V + h) * 512
+  auto load = [&](uint32_t blk, uint32_t h) -> uint4 {
+    const uint32_t v = (blk * V + h) * 32 + lane;
     if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
     return v < nvec ? load_vec(a.data, a.len, v) : zero;
   };
   uint32_t b = blockIdx.x * W + warp;
   LeanSlots slots;
-  if (kLeanDepth == 1) {
-    uint4 vn = b + nw < nblk ? load(b + nw) : zero;
-    LeanGrams gc;
-    if (b < nblk) lean_issue(filt, big, load(b), gc);
-#pragma unroll 2
-    for (; b < nblk; b += nw) {
-      const uint32_t b1 = b + nw, b2 = b1 + nw;
-      const uint4 vn2 = b2 < nblk ? load(b2) : zero;
-      LeanGrams gn;
-      if (b1 < nblk) lean_issue(filt, big, vn, gn);
-      const uint32_t base = b * 512 + lane * 16;
-      lean_append(a, slots, lean_finish(gc, base, len), base, lane);
-      gc = gn;
-      vn = vn2;
+  // stage 1 and the stage-1b loads of step b + nw run while step b finishes;
+  // the input is loaded two steps ahead
+  uint4 vn[V];
+  LeanGrams gc[V];
+#pragma unroll
+  for (uint32_t h = 0; h < V; ++h) {
+    vn[h] = b + nw < nblk ? load(b + nw, h) : zero;
+    if (b < nblk) lean_issue(filt, big, load(b, h), gc[h]);
+  }
+  for (; b < nblk; b += nw) {
+    const uint32_t b1 = b + nw, b2 = b1 + nw;
+    uint4 vn2[V];
+    LeanGrams gn[V];
+    uint32_t mask[V], base[V];
+#pragma unroll
+    for (uint32_t h = 0; h < V; ++h) {
+      vn2[h] = b2 < nblk ? load(b2, h) : zero;
+      if (b1 < nblk) lean_issue(filt, big, vn[h], gn[h]);
+      base[h] = (b * V + h) * 512 + lane * 16;
+      mask[h] = lean_finish(gc[h], base[h], len);
     }
-  } else {
-    // stage 1b of blocks b + nw and b + 2 nw in flight, input of b + 3 nw
-    LeanGrams g0, g1;
-    if (b < nblk) lean_issue(filt, big, load(b), g0);
-    if (b + nw < nblk) lean_issue(filt, big, load(b + nw), g1);
-    uint4 vin = b + 2 * nw < nblk ? load(b + 2 * nw) : zero;
-    for (; b < nblk; b += nw) {
-      const uint32_t b2 = b + 2 * nw, b3 = b2 + nw;
-      const uint4 vnext = b3 < nblk ? load(b3) : zero;
-      LeanGrams g2;
-      if (b2 < nblk) lean_issue(filt, big, vin, g2);
-      const uint32_t base = b * 512 + lane * 16;
-      lean_append(a, slots, lean_finish(g0, base, len), base, lane);
-      g0 = g1;
-      g1 = g2;
-      vin = vnext;
+    lean_append<V>(a, slots, mask, base, lane);
+#pragma unroll
+    for (uint32_t h = 0; h < V; ++h) {
+      gc[h] = gn[h];
+      vn[h] = vn2[h];
     }
   }
   lean_holes(a, slots, lane);
