@@ -813,7 +813,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   } else {
     sh ? run(literal_filter_kernel<1, 4, true, true>) : run(literal_filter_kernel<1, 4, true, false>);
   }
-  literal_verify_kernel<<<sm_count * 4, 256, 0, st>>>(a);
+  // the verify pass is a chain of dependent loads per survivor: the lean
+  // path's longer survivor list (stage 1.5 runs here) gets more threads
+  literal_verify_kernel<<<sm_count * (a.verify_bloom ? 16 : 4), 256, 0, st>>>(a);
   check_cuda(cudaGetLastError(), "literal_verify_kernel launch");
 }
 
