@@ -18,6 +18,8 @@
 //   survivors are appended to a compact position list with one atomic per warp
 //             (ballot + popc).  If the list is full, the position is verified in
 //             place instead, so results never depend on the list's capacity.
+// Kernel 1 for large sets, literal_lean_kernel (see its comment): stages 1 and
+//             1b only, no compaction; stage 1.5 moves to kernel 2.
 // Kernel 2, literal_verify_kernel: the reference's per-position algorithm on the
 //             surviving positions only: FNV-1a probe of the LiteralPrefilterTable
 //             partition at each non-empty prefix length (shader.rs:59-98) and an
