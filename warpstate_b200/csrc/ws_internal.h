@@ -109,9 +109,10 @@ struct LiteralPlan {
   // Large pattern sets fill the shared-memory gram table: a second table of
   // 2^kBigBits bytes in L2 (same hashes, more bits; each byte holds the P
   // phase bits of its hash, so a lookup is one byte load) re-checks every
-  // gram that passes it (stage 1b).  Empty when the shared table is sparse
-  // enough.
+  // gram that passes it (stage 1b).  Not built when the shared table is
+  // sparse enough; the host copy is released once uploaded (has_big).
   std::vector<uint8_t> big;
+  bool has_big = false;
   // With the stage-1b table: stage 1 of the lean kernel as bytes, indexed by
   // the top kFilter8Bits bits of the same hashes (the OR of the 2^7 stage-1b
   // bytes below each entry), so a lookup needs no nibble extract.
@@ -122,7 +123,7 @@ struct LiteralPlan {
 };
 
 constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
-constexpr uint32_t kBigBits = 24;     // stage-1b table: 2^24 bytes, 16 MiB, read through L2
+constexpr uint32_t kBigBits = 25;     // stage-1b table: 2^25 bytes, 32 MiB, read through L2
 constexpr uint32_t kFilter8Bits = 17; // byte-wide stage 1 of the lean kernel: 128 KiB of shared memory
 
 // Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).

@@ -233,6 +233,8 @@ void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
       plan.filter8.assign((size_t)1 << kFilter8Bits, 0);
       for (size_t h = 0; h < plan.big.size(); ++h) plan.filter8[h >> (kBigBits - kFilter8Bits)] |= plan.big[h];
       plan.d_filter8.upload(plan.filter8.data(), plan.filter8.size());
+      plan.has_big = true;
+      std::vector<uint8_t>().swap(plan.big);
     }
   }
   plan.n_buckets = t.n_buckets;

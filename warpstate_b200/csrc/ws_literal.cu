@@ -767,8 +767,8 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.gram_len = plan.gram_len;
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
-  a.big = plan.big.empty() ? nullptr : plan.d_big.as<uint8_t>();
-  a.filter8 = plan.filter8.empty() ? nullptr : plan.d_filter8.as<uint8_t>();
+  a.big = plan.has_big ? plan.d_big.as<uint8_t>() : nullptr;
+  a.filter8 = plan.has_big ? plan.d_filter8.as<uint8_t>() : nullptr;
   a.verify_bloom = 0;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   if (l.len > 0xFFFFFFFFull) raise(WS_ERR_INPUT_TOO_LARGE, "literal scan launch beyond 32-bit offsets", 0, l.len,
