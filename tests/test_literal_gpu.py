@@ -161,3 +161,86 @@ def test_concurrent_scans_share_one_matcher():
     [t.start() for t in th]
     [t.join() for t in th]
     assert not errs
+
+
+# ------------------------------------------- large sets (the lean kernel)
+# 10,000 literals of 8-32 bytes fill the shared-memory gram table, so these
+# scans take the large-set layout: stage 1 + 1b in the filter, each lane owning
+# the start positions whose first 4-aligned position is one of its own words,
+# 32 bytes per lane per warp step, survivors in per-warp chunks, stage 1.5 in
+# the verify kernel.
+def _large_set_matcher(extra=(), **cfg):
+    ws = _ws()
+    wl = w.literals_large(size=1 << 20, seed=11)
+    pats = list(wl.patterns) + [(0, p) for p in extra]
+    b = ws.PatternSet.builder()
+    for _, p in pats:
+        b = b.literal_bytes(p)
+    c = ws.AutoMatcherConfig()
+    for k, v in cfg.items():
+        getattr(c, k)(v)
+    return ws.GpuMatcher.with_config(b.build(), c), pats, wl.data
+
+
+def _plant(data, lits, positions, seed):
+    r = np.random.default_rng(seed)
+    d = data.copy()
+    for p in positions:
+        lit = lits[int(r.integers(0, len(lits)))]
+        if 0 <= p and p + len(lit) <= len(d):
+            d[p:p + len(lit)] = np.frombuffer(lit, dtype=np.uint8)
+    return d
+
+
+def test_large_set_edges_and_ragged_ends():
+    # matches at positions 0-3 (the shifted ownership masks positions before
+    # the input), across 512-byte halves and 1 KiB warp steps, and ending at
+    # the last byte of inputs of every length mod 16
+    m, pats, base = _large_set_matcher()
+    lits = [p for _, p in pats]
+    for n in (1 << 20, (1 << 20) - 1, (1 << 20) - 5, 100_003, 4099, 1027, 515, 64, 17, 9):
+        ends = [n - len(lits[k]) for k in (0, 1, 2)]
+        pos = [0, 1, 2, 3, 509, 510, 511, 512, 513, 1021, 1022, 1023, 1024, 1025, 2045, 2048] + ends
+        d = _plant(base[:n], lits, pos, seed=n)
+        # the last literal ends exactly at the last byte
+        tail = lits[3]
+        if len(tail) <= n:
+            d[n - len(tail):] = np.frombuffer(tail, dtype=np.uint8)
+        got = m.scan_array(d)
+        exp = oracle.scan_patterns(pats, d)
+        assert np.array_equal(got, exp), n
+
+
+def test_large_set_every_position_survives():
+    # a run of one byte that starts a literal at every position: the survivor
+    # list overflows and the filter verifies the rest in place
+    m, pats, _ = _large_set_matcher(extra=[b"zzzzzzzz", b"zzzzzzzzzzzz"], max_matches=8 << 20)
+    d = np.full((2 << 20) + 7, ord("z"), dtype=np.uint8)
+    d[::4093] = ord("q")
+    got = m.scan_array(d)
+    exp = oracle.scan_patterns(pats, d)
+    assert len(exp) > (3 << 20) and np.array_equal(got, exp)
+
+
+def test_large_set_batch_items_and_stream_windows():
+    # batch: item ends bound every match (literals planted across item ends
+    # must not match); stream: 1 MiB windows with exact carry
+    ws = _ws()
+    m, pats, base = _large_set_matcher(window_mib=1)
+    lits = [p for _, p in pats]
+    r = np.random.default_rng(3)
+    lens = r.integers(1, 6000, size=400)
+    total = int(lens.sum())
+    data = np.concatenate([base] * (total // len(base) + 1))[:total]
+    ends = np.cumsum(lens)
+    data = _plant(data, lits, list(ends[:-1] - 5) + list(ends[:-1] - 40), seed=4)
+    items, off = [], 0
+    for ln in lens:
+        items.append((off, int(ln)))
+        off += int(ln)
+    got = ws.scan_batch_packed(m, data, lens.astype(np.uint64))
+    exp = oracle.batch_scan(pats, data, items)
+    assert len(exp) > 50 and np.array_equal(got, exp)
+    big = np.concatenate([base, base, base[: (1 << 19) + 333]])
+    sp = ws.StreamPipeline(m).scan_array(big, block=(1 << 20) + 4095)
+    assert np.array_equal(sp, oracle.scan_patterns(pats, big).astype(np.uint64))
