@@ -791,8 +791,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
     kernel<<<grid, kBigThreads, smem, st>>>(a);
     check_cuda(cudaGetLastError(), "literal_filter_big_kernel launch");
   };
-  // the pipelined kernel pays off for 4-byte grams (measured); long grams,
-  // whose hashing dominates, keep 32 warps per SM
+  // large sets with 4-byte grams: the lean kernel, or with literals shorter
+  // than 4 bytes the pipelined compacting kernel; long grams, whose hashing
+  // dominates, keep 32 warps per SM
   if (lg && !sh && a.big && a.filter8 && plan.period == 4 && plan.gram_len == 4) {
     a.verify_bloom = 1;
     const size_t lsmem = (size_t)1 << kFilter8Bits;
@@ -800,8 +801,8 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
                "cudaFuncSetAttribute(literal lean)");
     literal_lean_kernel<<<sm_count, kLeanThreads, lsmem, st>>>(a);
     check_cuda(cudaGetLastError(), "literal_lean_kernel launch");
-  } else if (lg && a.big && plan.period == 4 && plan.gram_len == 4) {
-    sh ? run_big(literal_filter_big_kernel<4, true>) : run_big(literal_filter_big_kernel<4, false>);
+  } else if (lg && sh && a.big && plan.period == 4 && plan.gram_len == 4) {
+    run_big(literal_filter_big_kernel<4, true>);
   } else if (!lg) {
     run(literal_filter_kernel<4, 4, false, true>);
   } else if (plan.gram_len == 16) {
