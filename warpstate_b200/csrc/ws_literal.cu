@@ -545,8 +545,9 @@ __global__ void __launch_bounds__(kBigThreads, 1) literal_filter_big_kernel(LitA
 //     lane), so the per-step overhead is paid once per kLeanVecs x 512 bytes;
 //   - stage 1 and the stage-1b loads run one warp step ahead of the step
 //     being finished, the input two steps ahead;
-//   - the stage-1b survivors of a warp block (about 0.3 per 512 bytes on
-//     10,000 literals) are appended with one atomic per warp.
+//   - the stage-1b survivors of a warp step (about 0.15 per 512 bytes on
+//     10,000 literals) are appended into the warp's reserved slots of the
+//     list, one atomic per kLeanChunk slots (see lean_append).
 constexpr int kLeanThreads = 1024;
 constexpr int kLeanVecs = 2;  // 16-byte vectors per lane per warp step (a step covers kLeanVecs x 512 bytes)
 
@@ -563,9 +564,9 @@ struct LeanGrams {
   uint32_t n[4], bw[4];
 };
 
-// Stage 1 of a lane's four aligned grams, stage-1b loads issued.
-// Stage 1 from the byte table in shared memory (top kFilter8Bits bits of the
-// hash), stage 1b from the byte table in L2 (top kBigBits bits).
+// Stage 1 of a lane's four aligned grams from the byte table in shared memory
+// (top kFilter8Bits bits of the hash); the stage-1b loads from the byte table
+// in L2 (top kBigBits bits) are issued for the grams that pass.
 __device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
