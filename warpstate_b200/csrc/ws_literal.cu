@@ -101,14 +101,31 @@ __device__ __forceinline__ uint4 load_vec(const uint8_t* data, uint64_t len, uin
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// The reference's per-position probe and exact verify (stage 2).
-__device__ void verify_position(const LitArgs& a, uint64_t s) {
-  if (s >= a.max_start) return;
+// Bytes [a, a + 4) of the input for a 4-aligned a, zero past its end.
+__device__ __forceinline__ uint32_t word_at(const uint8_t* d, uint32_t len, uint32_t a) {
+  if (a + 4 <= len) return __ldg(reinterpret_cast<const uint32_t*>(d + a));
+  uint32_t x = 0;
+  for (uint32_t k = 0; k < 4; ++k)
+    if (a + k < len) x |= (uint32_t)__ldg(d + a + k) << (8 * k);
+  return x;
+}
+
+// The reference's per-position probe and exact verify (stage 2).  Inputs of
+// one launch are below 4 GiB.  The hashed bytes come from two words read
+// once, and a candidate literal is compared a word at a time (literal bytes
+// start 4-aligned in a buffer padded to 16 bytes).
+__device__ void verify_position(const LitArgs& a, uint64_t s64) {
+  if (s64 >= a.max_start) return;
+  const uint32_t s = (uint32_t)s64, len = (uint32_t)a.len;
+  const uint32_t w0 = s & ~3u, sh = (s & 3) * 8;
+  const uint32_t x0 = word_at(a.data, len, w0), x1 = word_at(a.data, len, w0 + 4),
+                 x2 = word_at(a.data, len, w0 + 8);
+  const uint32_t lo = __funnelshift_r(x0, x1, sh), hi = __funnelshift_r(x1, x2, sh);
   uint32_t h = 2166136261u;
-  uint64_t rem = a.len - s;
-  uint32_t maxp = (uint32_t)(rem < a.window ? rem : a.window);
+  const uint32_t rem = len - s;
+  const uint32_t maxp = rem < a.window ? rem : a.window;
   for (uint32_t i = 0; i < maxp; ++i) {
-    h = (h ^ (uint32_t)__ldg(a.data + s + i)) * 16777619u;
+    h = (h ^ (((i < 4 ? lo : hi) >> (8 * (i & 3))) & 0xFFu)) * 16777619u;
     if (!((a.parts >> i) & 1u)) continue;
     uint4 m = __ldg(a.meta + i);
     uint2 r = __ldg(a.ranges + m.x + (h & m.y));
@@ -117,10 +134,16 @@ __device__ void verify_position(const LitArgs& a, uint64_t s) {
       if (ent.x != h) continue;
       uint4 info = __ldg(a.info + ent.y);  // {offset, len, pattern id, 0}
       if (info.y > rem) continue;
-      const uint8_t* lit = a.lit_bytes + info.x;
+      const uint32_t* lit = reinterpret_cast<const uint32_t*>(a.lit_bytes + info.x);
       bool eq = true;
-      for (uint32_t k = 0; k < info.y; ++k) {
-        if (__ldg(lit + k) != __ldg(a.data + s + k)) { eq = false; break; }
+      uint32_t cur = x0;
+      for (uint32_t k = 0; k < info.y; k += 4) {
+        const uint32_t nxt = word_at(a.data, len, w0 + k + 4);
+        const uint32_t dw = __funnelshift_r(cur, nxt, sh);
+        const uint32_t left = info.y - k;
+        const uint32_t m = left >= 4 ? 0xFFFFFFFFu : ((1u << (8 * left)) - 1u);
+        if ((__ldg(lit + (k >> 2)) ^ dw) & m) { eq = false; break; }
+        cur = nxt;
       }
       if (!eq) continue;
       if (s + info.y <= a.min_end) continue;
@@ -550,15 +573,6 @@ __global__ void __launch_bounds__(kBigThreads, 1) literal_filter_big_kernel(LitA
 //     list, one atomic per kLeanChunk slots (see lean_append).
 constexpr int kLeanThreads = 1024;
 constexpr int kLeanVecs = 2;  // 16-byte vectors per lane per warp step (a step covers kLeanVecs x 512 bytes)
-
-// Bytes [a, a + 4) of the input, zero past its end.
-__device__ __forceinline__ uint32_t word_at(const uint8_t* d, uint32_t len, uint32_t a) {
-  if (a + 4 <= len) return __ldg(reinterpret_cast<const uint32_t*>(d + a));
-  uint32_t x = 0;
-  for (uint32_t k = 0; k < 4; ++k)
-    if (a + k < len) x |= (uint32_t)__ldg(d + a + k) << (8 * k);
-  return x;
-}
 
 struct LeanGrams {
   uint32_t n[4], bw[4];
