@@ -170,6 +170,48 @@ def cpu_baseline(wl, seconds: float = 12.0):
             "sample": f"first {n} bytes of the same input ({n / dt / 1e6:.1f} MB/s over {dt:.1f} s)"}
 
 
+# ----------------------------------------------------------------- parity
+MATCH64 = np.dtype([("pid", "<u4"), ("res", "<u4"), ("start", "<u8"), ("end", "<u8")])
+TAGGED = np.dtype([("sid", "<u8"), ("pid", "<u4"), ("start", "<u4"), ("end", "<u4"), ("res", "<u4")])
+
+
+def device_rows(d_out, count: int, kind: str) -> np.ndarray:
+    """The device output of one scan as rows in the oracle's canonical order:
+    (pattern_id, start, end) by (start, pattern_id, end), or for batches
+    (source_id, pattern_id, start, end) by (source_id, start, pattern_id, end)."""
+    import oracle
+    if kind == "match":
+        a = d_out.view(-1).view(__import__("torch").int32)[: count * 3].cpu().numpy().view(np.uint32)
+        return oracle.sort_matches(a.reshape(-1, 3).copy())
+    raw = d_out.view(-1).view(__import__("torch").uint8)[: count * 24].cpu().numpy()
+    if kind == "match64":
+        o = raw.view(MATCH64)
+        a = np.empty((count, 3), dtype=np.uint64)
+        a[:, 0], a[:, 1], a[:, 2] = o["pid"], o["start"], o["end"]
+        return a[np.lexsort((a[:, 2], a[:, 0], a[:, 1]))]
+    o = raw.view(TAGGED)
+    a = np.empty((count, 4), dtype=np.uint64)
+    a[:, 0], a[:, 1], a[:, 2], a[:, 3] = o["sid"], o["pid"], o["start"], o["end"]
+    return a[np.lexsort((a[:, 3], a[:, 1], a[:, 2], a[:, 0]))]
+
+
+def mismatches(a: np.ndarray, b: np.ndarray) -> int:
+    """Size of the symmetric difference of two match multisets."""
+    if a.shape == b.shape and np.array_equal(a, b):
+        return 0
+    from collections import Counter
+    ca = Counter(map(tuple, a.astype(np.uint64).tolist()))
+    cb = Counter(map(tuple, b.astype(np.uint64).tolist()))
+    return sum(((ca - cb) + (cb - ca)).values())
+
+
+def oracle_rows(wl, nbytes: int, threads: int) -> np.ndarray:
+    import oracle
+    if wl.items is not None:
+        return oracle.batch_scan(wl.patterns, wl.data, wl.items, threads=threads)
+    return oracle.scan_patterns(wl.patterns, wl.data[:nbytes], threads)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -216,7 +258,7 @@ def build_matchers(ws, wl, config, walk_chunk=None, proposer=True, dfa_max_state
     return m, plain, tune
 
 
-def main():
+def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -227,11 +269,199 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison of the full match set")
+    ap.add_argument("--no-literal", action="store_true",
+                    help="skip the literals_large sub-record of the regex configuration")
+    ap.add_argument("--no-arms", action="store_true", help="skip the second boundary-guess arm of the regex walk")
+    ap.add_argument("--parity-bytes", type=int, default=512 << 20,
+                    help="dna: bytes of the input prefix compared with the oracle")
     ap.add_argument("--walk-chunk", type=int, default=None, help="speculative walk chunk bytes")
     ap.add_argument("--no-proposer", action="store_true", help="guess the unanchored start at every boundary")
     ap.add_argument("--dfa-max-states", type=int, default=None, help="states per merged group DFA")
-    args = ap.parse_args()
+    return ap.parse_args()
 
+
+class Runner:
+    """Device-resident inputs and outputs of one configuration and the timed
+    step over them (one scan of the whole input by the full pattern set)."""
+
+    def __init__(self, wl, config, dev, stream, dist, torch):
+        self.wl, self.config, self.dev, self.stream, self.dist, self.torch = wl, config, dev, stream, dist, torch
+        self.batch = wl.items is not None
+        self.big = config == "dna" or wl.data.nbytes > 0xFFFFFFFF
+        if self.batch:
+            self.lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+            self.n_bytes = int(self.lens.sum())
+            self.n_items = len(self.lens)
+            self.d_in = torch.from_numpy(wl.data[: self.n_bytes]).to(dev)
+            self.d_ends = torch.from_numpy(np.cumsum(self.lens).astype(np.uint32).view(np.int32)).to(dev)
+            self.d_ids = torch.arange(self.n_items, dtype=torch.int64, device=dev)
+        else:
+            self.n_bytes = int(wl.data.nbytes)
+            self.n_items = 1
+            self.d_in = torch.from_numpy(wl.data).to(dev)
+        # ws_match (12 B), ws_match64 or ws_tagged_match (24 B)
+        self.d_out = torch.empty(CAP * 3, dtype=torch.int64, device=dev)
+        self.d_cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.kind = "tagged" if self.batch else "match64" if self.big else "match"
+        # inputs smaller than L2 are re-read cold: a 512 MiB write between steps
+        self.flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev) if self.n_bytes < (256 << 20) else None
+
+    def step(self, matcher, n_bytes=None):
+        s = self.stream.cuda_stream
+        if self.batch:
+            matcher.scan_batch_device(self.d_in.data_ptr(), self.n_bytes, self.d_ends.data_ptr(),
+                                      self.d_ids.data_ptr(), self.n_items, self.d_out.data_ptr(), CAP,
+                                      self.d_cnt.data_ptr(), s)
+        elif self.big:
+            matcher.scan_device64(self.d_in.data_ptr(), n_bytes or self.n_bytes, self.d_out.data_ptr(), CAP,
+                                  self.d_cnt.data_ptr(), s)
+        else:
+            matcher.scan_device(self.d_in.data_ptr(), n_bytes or self.n_bytes, self.d_out.data_ptr(), CAP,
+                                self.d_cnt.data_ptr(), s)
+
+    def count(self) -> int:
+        c = int(self.d_cnt.item()) & 0xFFFFFFFFFFFFFFFF
+        if c > CAP:
+            raise SystemExit(f"match overflow or unknown count ({c} > {CAP})")
+        return c
+
+    def timed_steps(self, matcher, steps, warmup):
+        torch, dist = self.torch, self.dist
+        for _ in range(warmup):
+            self.step(matcher)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total, infos = 0.0, []
+        torch.cuda.nvtx.range_push("timed")  # lets a profiler capture only the timed steps
+        for _ in range(steps):
+            if self.flush is not None:
+                self.flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            self.step(matcher)
+            e1.record(self.stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            infos.append(matcher.info())
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return total / steps, infos
+
+    def parity(self, matcher, parity_bytes: int):
+        """One more scan (untimed), its full match set against the oracle's on
+        the same input: the whole input, or for the 4 GiB nucleotide input a
+        prefix (the oracle's offsets are 32-bit)."""
+        import oracle
+        n = self.n_bytes
+        if self.big:
+            n = min(n, parity_bytes)
+        self.step(matcher, n_bytes=n)
+        self.torch.cuda.synchronize()
+        got = device_rows(self.d_out, self.count(), self.kind)
+        t = time.perf_counter()
+        exp = oracle_rows(self.wl, n, oracle.hw_threads())
+        dt = time.perf_counter() - t
+        rec = {"mismatches": mismatches(got, exp), "compared_matches": int(len(exp)), "gpu_matches": int(len(got)),
+               "compared_bytes": n, "oracle_s": round(dt, 2), "oracle_threads": oracle.hw_threads()}
+        if n < self.n_bytes:
+            rec["scope"] = f"first {n} bytes of the {self.n_bytes}-byte input"
+        return rec
+
+
+def build_matchers(ws, wl, config, walk_chunk=None, proposer=True, dfa_max_states=None, plain_too=True):
+    ps = ws.PatternSet.builder()
+    for kind, p in wl.patterns:
+        ps = ps.literal_bytes(p) if kind == 0 else ps.regex(p.decode())
+    ps = ps.build()
+    cfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_SPECULATIVE)
+    if walk_chunk:
+        cfg.walk_chunk(walk_chunk)
+    if dfa_max_states:
+        cfg.dfa_max_states(dfa_max_states)
+    if not proposer:
+        cfg.proposer(ws.PROPOSER_NONE)
+    m = ws.GpuMatcher.with_config(ps, cfg)
+    plain = None
+    has_regex = any(k == 1 for k, _ in wl.patterns)
+    if plain_too and has_regex and config in ("regex", "batch", "dna"):
+        pcfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_PLAIN)
+        plain = ws.GpuMatcher.with_config(ps, pcfg)
+    tune = None
+    if has_regex:
+        # a separately seeded 256 MiB corpus of the same distribution: the
+        # autotuner picks group size, hot rows, proposer and chunk on it (knobs
+        # given on the command line stay fixed)
+        corpus = W.dna_training_corpus() if config == "dna" else W.regex_training_corpus()
+        flags = (0 if dfa_max_states else ws.GpuMatcher.TUNE_GROUPS) | (0 if walk_chunk else ws.GpuMatcher.TUNE_CHUNK)
+        tune = m.tune(corpus, flags=flags)
+        del corpus
+    return m, plain, tune
+
+
+def roofline_of(config, infos, n_bytes, count, n_items, batch, has_regex, peak, peak_kind):
+    """The dominant kernel's achieved algorithmic bandwidth against the
+    measured HBM peak (N input bytes + 12 B per match + 16 B per item)."""
+    # the literal phase (index 0) spans the filter and the verify kernel; the
+    # 10,000-literal set takes the large-set layout (stage-1b table, no literals
+    # under 4 bytes), whose filter is literal_lean_kernel
+    kidx, kname = ((1, "dfa_walk_kernel") if has_regex else
+                   (0, "literal_lean_kernel") if config == "literals_large" else (0, "literal_filter_kernel"))
+    kms = statistics.mean(i["last_kernel_ms"][kidx] for i in infos) if infos else None
+    alg_bytes = n_bytes + 12 * count + (16 * n_items if batch else 0)
+    achieved = alg_bytes / (kms * 1e-3) / 1e9 if kms else None
+    return {"bound": "hbm", "achieved": round(achieved, 2) if achieved else None, "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4) if achieved else None,
+            "traffic": read_traffic(kname, config), "kernel": kname,
+            "kernel_ms": round(kms, 4) if kms else None,
+            "peak_source": (f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                            else "fallback 6.65 TB/s"),
+            "algorithmic_bytes_per_launch": alg_bytes}
+
+
+def walk_record(info, n_bytes, ms):
+    """Counters of the speculative walk of one profiled scan."""
+    g = info["n_groups"]
+    walk_ms = info["last_kernel_ms"][1]
+    guesses = info["last_guesses"]
+    return {"gbs": round(n_bytes / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 4),
+            "walk_ms": round(walk_ms, 4),
+            "lookups_per_s": round(g * n_bytes / (walk_ms * 1e-3), 1) if walk_ms else None,
+            "guess_hit_rate": round(info["last_guess_hits"] / guesses, 5) if guesses else None,
+            "fixup_chunks": info["last_fixup_chunks"], "chunks": info["last_chunks"],
+            "rewalk_bytes": info["last_rewalk_bytes"],
+            "rewalk_frac": round(info["last_rewalk_bytes"] / (g * n_bytes), 6) if g else None,
+            "events": info["last_events"], "candidates": info["last_kcandidates"],
+            "phase_ms": [round(x, 4) for x in info["last_kernel_ms"]]}
+
+
+def literal_subrecord(ws, args, dev, stream, dist, torch, peak, peak_kind):
+    """The literal prefilter + verify path (10,000 literals over 1 GiB) timed
+    in the same run, with its own roofline and oracle comparison."""
+    wl = make_workload("literals_large", None)
+    m, _, _ = build_matchers(ws, wl, "literals_large", plain_too=False)
+    r = Runner(wl, "literals_large", dev, stream, dist, torch)
+    ms, infos = r.timed_steps(m, args.steps, args.warmup)
+    count = r.count()
+    rec = {"workload": "literals_large", "description": CONFIGS["literals_large"],
+           "value": round(r.n_bytes / (ms * 1e-3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
+           "matches": count,
+           "roofline": roofline_of("literals_large", infos, r.n_bytes, count, 1, False, False, peak, peak_kind)}
+    if not args.no_parity:
+        rec["parity"] = r.parity(m, args.parity_bytes)
+    m.close()
+    del r, wl
+    torch.cuda.empty_cache()
+    return rec
+
+
+def main():
+    args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -253,65 +483,10 @@ def main():
 
     wl = make_workload(args.config, args.size)
     m, plain, tune = build_matchers(ws, wl, args.config, args.walk_chunk, not args.no_proposer,
-                                       args.dfa_max_states)
-    if args.no_plain:
-        plain = None
+                                    args.dfa_max_states, plain_too=not args.no_plain)
     stream = torch.cuda.current_stream()
-    batch = wl.items is not None
-    big = args.config == "dna" or wl.data.nbytes > 0xFFFFFFFF
-
-    # device-resident inputs and outputs
-    if batch:
-        lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
-        n_bytes = int(lens.sum())
-        n_items = len(lens)
-        d_in = torch.from_numpy(wl.data[:n_bytes]).to(dev)
-        d_ends = torch.from_numpy(np.cumsum(lens).astype(np.uint32).view(np.int32)).to(dev)
-        d_ids = torch.arange(n_items, dtype=torch.int64, device=dev)
-        d_out = torch.empty(CAP * 3, dtype=torch.int64, device=dev)  # ws_tagged_match = 24 B
-    else:
-        n_bytes = int(wl.data.nbytes)
-        n_items = 1
-        d_in = torch.from_numpy(wl.data).to(dev)
-        d_out = torch.empty(CAP * 3, dtype=torch.int64, device=dev)  # ws_match (12 B) or ws_match64 (24 B)
-    d_cnt = torch.zeros(1, dtype=torch.int64, device=dev)
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev) if n_bytes < (256 << 20) else None
-
-    def step(matcher):
-        s = stream.cuda_stream
-        if batch:
-            matcher.scan_batch_device(d_in.data_ptr(), n_bytes, d_ends.data_ptr(), d_ids.data_ptr(), n_items,
-                                      d_out.data_ptr(), CAP, d_cnt.data_ptr(), s)
-        elif big:
-            matcher.scan_device64(d_in.data_ptr(), n_bytes, d_out.data_ptr(), CAP, d_cnt.data_ptr(), s)
-        else:
-            matcher.scan_device(d_in.data_ptr(), n_bytes, d_out.data_ptr(), CAP, d_cnt.data_ptr(), s)
-
-    def timed_steps(matcher, steps, warmup):
-        for _ in range(warmup):
-            step(matcher)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        total, infos = 0.0, []
-        torch.cuda.nvtx.range_push("timed")  # lets a profiler capture only the timed steps
-        for _ in range(steps):
-            if flush is not None:
-                flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            step(matcher)
-            e1.record(stream)
-            e1.synchronize()
-            total += e0.elapsed_time(e1)
-            infos.append(matcher.info())
-        torch.cuda.nvtx.range_pop()
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        return total / steps, infos
+    r = Runner(wl, args.config, dev, stream, dist, torch)
+    n_bytes, n_items, batch = r.n_bytes, r.n_items, r.batch
 
     def max_over_ranks(x):
         t = torch.tensor([x], dtype=torch.float64, device=dev)
@@ -321,20 +496,34 @@ def main():
 
     # the speculative (or only) path
     with ClockSampler(local) as clk:
-        ms, infos = timed_steps(m, args.steps, args.warmup)
+        ms, infos = r.timed_steps(m, args.steps, args.warmup)
     clocks = clk.summary()
-    count = int(d_cnt.item())
-    if count > CAP:
-        raise SystemExit(f"match overflow ({count} > {CAP})")
+    count = r.count()
     ms_max = max_over_ranks(ms)
     value = world * n_bytes / (ms_max * 1e-3) / 1e9
+    has_regex = any(k == 1 for k, _ in wl.patterns)
+
+    # the other boundary guess of the speculative walk, timed the same way:
+    # the trained proposer when the tuner chose the unanchored start, and the
+    # reverse; same chunk, same matches
+    arms = None
+    if has_regex and tune and not args.no_arms and not args.no_proposer and tune["proposer_top1"] > 0:
+        used = tune["proposer_used"]
+        arms = {("proposer" if used else "unanchored"): walk_record(infos[-1], n_bytes, ms)}
+        m.set_walk(0, ws.PROPOSER_NONE if used else ws.PROPOSER_MLP)
+        ams, ainfos = r.timed_steps(m, args.steps, args.warmup)
+        acount = r.count()
+        if acount != count:
+            raise SystemExit(f"match counts differ between boundary guesses: {acount} vs {count}")
+        arms[("unanchored" if used else "proposer")] = walk_record(ainfos[-1], n_bytes, max_over_ranks(ams))
+        m.set_walk(0, ws.PROPOSER_MLP if used else ws.PROPOSER_NONE)
 
     plain_gbs = plain_ms = None
     if plain is not None:
-        pms, _ = timed_steps(plain, max(1, min(2, args.steps)), 1)
+        pms, _ = r.timed_steps(plain, max(1, min(2, args.steps)), 1)
         plain_ms = max_over_ranks(pms)
         plain_gbs = world * n_bytes / (plain_ms * 1e-3) / 1e9
-        plain_count = int(d_cnt.item())
+        plain_count = r.count()
         if plain_count != count:
             raise SystemExit(f"plain/speculative match counts differ: {plain_count} vs {count}")
 
@@ -346,6 +535,7 @@ def main():
         import ctypes
         import warpstate_b200._native as N
         k = min(n_items, 2000)
+        lens = r.lens
         offs = np.concatenate([[0], np.cumsum(lens[:k])]).astype(np.int64)
         host = np.ascontiguousarray(wl.data[: int(offs[k])])
         out1 = (N.WsMatch * (1 << 20))()
@@ -362,25 +552,12 @@ def main():
         per_item = {"items": k, "bytes": int(offs[k]), "ms": round(dt_items * 1e3, 3),
                     "gbs": round(int(offs[k]) / dt_items / 1e9, 4),
                     "api": "GpuMatcher.scan (ws_scan), plain kernel, one call per item from host memory"}
+    if plain is not None:
+        plain.close()
 
     # roofline of the dominant kernel
     peak, peak_kind = load_peaks()
-    has_regex = any(k == 1 for k, _ in wl.patterns)
-    # the literal phase (index 0) spans the filter and the verify kernel; the
-    # 10,000-literal set takes the large-set layout (stage-1b table, no literals
-    # under 4 bytes), whose filter is literal_lean_kernel
-    kidx, kname = ((1, "dfa_walk_kernel") if has_regex else
-                   (0, "literal_lean_kernel") if args.config == "literals_large" else (0, "literal_filter_kernel"))
-    kms = statistics.mean(i["last_kernel_ms"][kidx] for i in infos) if infos else None
-    alg_bytes = n_bytes + 12 * count + (16 * n_items if batch else 0)
-    achieved = alg_bytes / (kms * 1e-3) / 1e9 if kms else None
-    roofline = {"bound": "hbm", "achieved": round(achieved, 2) if achieved else None, "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4) if achieved else None,
-                "traffic": read_traffic(kname, args.config), "kernel": kname,
-                "kernel_ms": round(kms, 4) if kms else None,
-                "peak_source": (f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
-                                else "fallback 6.65 TB/s"),
-                "algorithmic_bytes_per_launch": alg_bytes}
+    roofline = roofline_of(args.config, infos, n_bytes, count, n_items, batch, has_regex, peak, peak_kind)
 
     # end to end through the public API from pinned host memory
     e2e = None
@@ -389,10 +566,12 @@ def main():
         pinned.numpy()[:] = wl.data[:n_bytes]
         hv = pinned.numpy()
         if batch:
+            lens = r.lens
+
             def call():
                 return ws.scan_batch_packed(m, pinned, lens)
             d2h = lambda n: 24 * n + 8  # noqa: E731
-        elif big:
+        elif r.big:
             sp = ws.StreamPipeline(m)
 
             def call():
@@ -413,22 +592,27 @@ def main():
         if len(res) != count:
             raise SystemExit(f"e2e count {len(res)} != device count {count}")
         # the link ceiling: a plain pinned host-to-device copy of the same bytes
-        dev = torch.empty(n_bytes, dtype=torch.uint8, device="cuda")
-        dev.copy_(pinned, non_blocking=True)
+        dbuf = torch.empty(n_bytes, dtype=torch.uint8, device=dev)
+        dbuf.copy_(pinned, non_blocking=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(k):
-            dev.copy_(pinned, non_blocking=True)
+            dbuf.copy_(pinned, non_blocking=True)
         e1.record()
         torch.cuda.synchronize()
         h2d_gbs = n_bytes * k / (e0.elapsed_time(e1) * 1e-3) / 1e9
-        del dev
+        del dbuf
         e2e = {"value": round(world * n_bytes / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": n_bytes,
                "d2h_bytes_per_step": d2h(count), "ms_per_step": round(dt * 1e3, 3),
                "h2d_copy_gbs": round(h2d_gbs, 2),
                "api": ("scan_batch_packed (ws_scan_batch)" if batch else
-                       "StreamPipeline.scan (ws_stream_*)" if big else "GpuMatcher.scan (ws_scan)")}
+                       "StreamPipeline.scan (ws_stream_*)" if r.big else "GpuMatcher.scan (ws_scan)")}
         del pinned, hv
+
+    # the full match set of one more scan against the oracle on the same input
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = r.parity(m, args.parity_bytes)
 
     base = None
     if rank == 0 and not args.no_cpu:
@@ -450,28 +634,36 @@ def main():
         "data": "synthetic",
         "config": {"workload": args.config, "description": CONFIGS[args.config], "bytes_per_rank": n_bytes,
                    "items": n_items if batch else None, "patterns": len(wl.patterns), "matches": count,
-                   "l2": "input larger than L2" if flush is None else "L2 flushed (512 MiB write) between steps",
+                   "l2": "input larger than L2" if r.flush is None else "L2 flushed (512 MiB write) between steps",
                    "parallelism": f"replicas x{world}"},
         "roofline": roofline,
         "cpu_baseline": base,
         "e2e": e2e,
         "gpu_launches": int(launches) * args.steps,
         "clocks": clocks,
+        "parity": parity,
     }
     if has_regex:
         last = infos[-1]
-        line["regex"] = {"speculative_gbs": round(value, 3),
-                         "plain_gbs": round(plain_gbs, 3) if plain_gbs else None,
-                         "speedup_vs_plain": round(value / plain_gbs, 3) if plain_gbs else None,
-                         "plain_ms_per_step": round(plain_ms, 4) if plain_ms else None,
-                         "proposer_top1": last["proposer_top1"], "proposer_top4": last["proposer_top4"],
-                         "tune": tune,
-                         "fixup_chunks": last["last_fixup_chunks"], "chunks": last["last_chunks"],
-                         "groups": last["n_groups"], "states": last["total_states"],
-                         "phase_ms": [round(x, 4) for x in last["last_kernel_ms"]]}
+        rec = {"speculative_gbs": round(value, 3),
+               "plain_gbs": round(plain_gbs, 3) if plain_gbs else None,
+               "speedup_vs_plain": round(value / plain_gbs, 3) if plain_gbs else None,
+               "plain_ms_per_step": round(plain_ms, 4) if plain_ms else None,
+               "boundary_guess": ("learned proposer (top-1)" if tune and tune["proposer_used"]
+                                  else "unanchored start state (the autotuner turned the proposer off)"),
+               "proposer_top1_heldout": last["proposer_top1"], "proposer_top4_heldout": last["proposer_top4"],
+               "tune": tune, "groups": last["n_groups"], "states": last["total_states"]}
+        rec.update(walk_record(last, n_bytes, ms_max))
+        if arms:
+            rec["arms"] = arms
+        line["regex"] = rec
     if per_item is not None:
         line["batch"] = {"per_item_plain_dispatch": per_item,
                          "batched_gbs": round(value, 3)}
+    del r
+    torch.cuda.empty_cache()
+    if args.config == "regex" and not args.no_literal and rank == 0 and world == 1:
+        line["literal"] = literal_subrecord(ws, args, dev, stream, dist, torch, peak, peak_kind)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -168,12 +168,25 @@ void ws_matcher_destroy(ws_matcher* m);
 ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len,
                   ws_match* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
 
+/* Match count a device-resident scan reports when its regex candidate buffers
+ * (library scratch, sized from the input length and max_matches) overflowed:
+ * the true count is not known.  The matcher records how many candidates the
+ * scan needed, so the same call made again succeeds.  The synchronous entry
+ * points (ws_scan, ws_scan_batch, ws_stream_*) repeat such a scan themselves
+ * and always return the true count. */
+#define WS_COUNT_UNKNOWN UINT64_MAX
+/* Match count a device-resident scan reports when one of its bounded
+ * device-side waits ran out (it should not; the synchronous entry points
+ * return WS_ERR_TIMEOUT for it). */
+#define WS_COUNT_TIMEOUT (UINT64_MAX - 1)
+
 /* Device-resident variant: d_data is a 16-byte aligned device pointer, d_out a
  * device buffer of cap matches, d_count a device u64 that receives the true
  * match count (only min(count, cap) matches are written; count > cap means
- * overflow).  Nothing is copied to the host and the output is unsorted.  All
- * work is enqueued on `stream` (a cudaStream_t, 0 = legacy default stream) and
- * the call returns without synchronising. */
+ * overflow), or WS_COUNT_UNKNOWN or WS_COUNT_TIMEOUT (see above).  Nothing is copied to the host
+ * and the output is unsorted.  All work is enqueued on `stream` (a
+ * cudaStream_t, 0 = legacy default stream) and the call returns without
+ * synchronising.  The device-resident calls below report counts the same way. */
 ws_status ws_scan_device(ws_matcher* m, const uint8_t* d_data, uint64_t len,
                          ws_match* d_out, uint64_t cap, uint64_t* d_count,
                          void* stream, ws_error_info* err);
@@ -186,10 +199,13 @@ ws_status ws_scan_device(ws_matcher* m, const uint8_t* d_data, uint64_t len,
  * scratch in a static device array inside the library (about 8 MiB, held on
  * every GPU that loads the library until the process exits) instead of an
  * allocation.  Accepts at most 128 MiB per call (WS_ERR_INPUT_TOO_LARGE
- * beyond).  The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the one array: calls whose work overlaps on the GPU race,
- * so serialise them (one stream, or events). */
+ * beyond).  Every call looks up the array's device address
+ * (cudaGetSymbolAddress); the first call on a device loads the library's
+ * device code there, so make that first call before any stream capture.  A
+ * device reset (cudaDeviceReset) discards the array with everything else on
+ * the device, including the results of earlier calls.  All calls share the
+ * one array: calls whose work overlaps on the GPU race, so serialise them (one
+ * stream, or events). */
 ws_status ws_scan_literals_noalloc(ws_matcher* m, const uint8_t* d_data, uint64_t len,
                                    ws_match* d_out, uint64_t cap, uint64_t* d_count,
                                    void* stream, ws_error_info* err);
@@ -279,6 +295,13 @@ typedef struct {
 ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint64_t len, uint64_t seed,
                           uint32_t flags, ws_tune_report* report, ws_error_info* err);
 
+/* Pins the speculative walk's chunk (bytes, a multiple of 256; 0 keeps the
+ * current one) and whether the trained proposer (WS_PROPOSER_MLP) or the
+ * unanchored start (WS_PROPOSER_NONE) supplies each chunk's start state,
+ * overriding the autotuner's choice.  Matches never change.  No counterpart in
+ * the reference.  Call it between scans, not while scans run. */
+ws_status ws_matcher_set_walk(ws_matcher* m, uint32_t walk_chunk, uint32_t proposer, ws_error_info* err);
+
 /* Introspection for tests and the benchmark. */
 typedef struct {
   uint32_t n_literals, n_regex, n_groups;
@@ -286,12 +309,18 @@ typedef struct {
   uint32_t max_classes;
   uint32_t filter_q, filter_period, filter_bits;
   double proposer_top1, proposer_top4;  /* held-out hit rates after training */
-  uint64_t last_fixup_chunks, last_chunks;
-  uint64_t last_kcandidates;
+  uint64_t last_fixup_chunks;     /* chunk re-walks of the fix-up (profiled scans) */
+  uint64_t last_chunks;           /* (group, chunk) walks of the last scan */
+  uint64_t last_kcandidates;      /* regex candidates of the last profiled scan */
   double last_kernel_ms[8];      /* literal, walk, propose, fixup, reverse, resolve, plain, total */
   uint32_t last_launches;
   uint32_t max_literal_len;      /* longest literal (bytes) */
   int64_t max_regex_len;         /* longest regex match (bytes), -1 unbounded */
+  /* Counters of the last profiled speculative scan (WS_FLAG_PROFILE): */
+  uint64_t last_events;          /* match events of the chunked walk */
+  uint64_t last_rewalk_bytes;    /* bytes re-walked by the fix-up (over all groups) */
+  uint64_t last_guess_hits;      /* chunk boundaries whose guessed start state was the true one */
+  uint64_t last_guesses;         /* chunk boundaries guessed (chunks - 1, per group) */
 } ws_matcher_info;
 ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
 

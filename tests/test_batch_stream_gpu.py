@@ -135,6 +135,19 @@ def test_batch_scaled_vs_oracle(mode):
     assert got.shape == exp.shape and np.array_equal(got, exp)
 
 
+def test_batch_config_mix_20000_items_vs_oracle():
+    # the batch configuration's pattern mix (1,500 literals + 500 regexes) and
+    # item-size distribution, on 20,000 items
+    ws = _ws()
+    wl = w.batch(n_items=20_000)
+    m = matcher(wl.patterns, max_matches=1 << 21)
+    lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+    got = ws.scan_batch_packed(m, wl.data, lens)
+    exp = oracle.batch_scan(wl.patterns, wl.data, wl.items)
+    assert len(exp) > 1000
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
 def test_batch_launch_groups_and_planner_agree():
     # a 1 MiB launch budget splits the batch into several launch sequences;
     # the reference planner's grouping (scan_batch) gives the same result

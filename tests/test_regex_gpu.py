@@ -35,9 +35,38 @@ def matcher(patterns, mode=SPEC, proposer=None, **cfg):
     return ws.GpuMatcher.with_config(b.build(), c)
 
 
+def _outside_classes(pattern: str) -> str:
+    """The pattern with bracket expressions removed (a ^ there negates a class)."""
+    out, i = [], 0
+    while i < len(pattern):
+        c = pattern[i]
+        if c == "\\":
+            out.append(pattern[i:i + 2])
+            i += 2
+        elif c == "[":
+            j = i + 1
+            if j < len(pattern) and pattern[j] == "^":
+                j += 1
+            if j < len(pattern) and pattern[j] == "]":
+                j += 1
+            while j < len(pattern) and pattern[j] != "]":
+                j += 2 if pattern[j] == "\\" else 1
+            i = j + 1
+        else:
+            out.append(c)
+            i += 1
+    return "".join(out)
+
+
 def supported(pattern: str) -> bool:
     r = oracle.Regex(pattern)
-    return not r.nullable and not any(a in pattern for a in ("^", "$", "\\b", "\\B", "\\A", "\\z"))
+    bare = _outside_classes(pattern)
+    return not r.nullable and not any(a in bare for a in ("^", "$", "\\b", "\\B", "\\A", "\\z"))
+
+
+def test_negated_classes_are_run():
+    # [^a-z] style goldens are not look-around: they must reach the GPU
+    assert supported("[^a-z]+") and supported("x[^\\]]y") and not supported("^abc")
 
 
 def test_golden_regex_cases(golden):
@@ -177,3 +206,57 @@ def test_distinct_candidates_hold_the_starts_of_full_k():
         d = m.regex_candidates(data, md, distinct=True)
         assert set(map(tuple, d[:, :2].tolist())) == starts, md
         assert len(d) * 20 < len(full[md]), (md, len(d), len(full[md]))
+
+
+def test_candidate_overflow_is_retried_exactly():
+    # [a-z]{1,8}q over lowercase text: every q ends a match from up to 8
+    # starts, so the candidates far exceed a small max_matches while the
+    # leftmost-first result still fits.  The candidate buffers overflow on the
+    # first scan; the synchronous scan repeats it with the capacity the first
+    # one needed and returns the exact result.
+    rng = np.random.default_rng(5)
+    data = rng.integers(ord("a"), ord("z") + 1, size=6 << 20, dtype=np.uint8).tobytes()
+    pats = [(1, b"[a-z]{1,8}q"), (1, b"[a-m]{2,6}[xyz]")]
+    exp = oracle.scan_patterns(pats, data)
+    cap = len(exp) + 10
+    for mode in (PLAIN, SPEC):
+        m = matcher(pats, mode=mode, max_matches=cap)
+        got = m.scan_array(data)
+        assert np.array_equal(got, exp), mode
+        got2 = m.scan_array(data)  # the recorded capacity is kept
+        assert np.array_equal(got2, exp), mode
+
+
+def test_candidate_overflow_device_reports_unknown_then_succeeds():
+    import torch
+    rng = np.random.default_rng(6)
+    data = rng.integers(ord("a"), ord("z") + 1, size=6 << 20, dtype=np.uint8)
+    pats = [(1, b"[a-z]{1,8}q")]
+    exp = oracle.scan_patterns(pats, data.tobytes())
+    cap = len(exp) + 10
+    m = matcher(pats, mode=SPEC, max_matches=cap)
+    d = torch.from_numpy(data).cuda()
+    out = torch.zeros((cap, 3), dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    counts = []
+    for _ in range(2):
+        m.scan_device(d.data_ptr(), d.numel(), out.data_ptr(), cap, cnt.data_ptr())
+        torch.cuda.synchronize()
+        counts.append(int(cnt.item()) & 0xFFFFFFFFFFFFFFFF)
+    assert counts[0] == 0xFFFFFFFFFFFFFFFF  # WS_COUNT_UNKNOWN: the candidates overflowed
+    assert counts[1] == len(exp)
+    got = oracle.sort_matches(out[:counts[1]].cpu().numpy().astype(np.uint32))
+    assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_nucleotide_config_scaled_vs_oracle(mode):
+    # the nucleotide configuration (k-mer literals plus IUPAC-degenerate
+    # regexes over ACGT with N runs) at 64 MiB, both regex paths
+    wl = w.dna(size=64 << 20)
+    m = matcher(wl.patterns, mode=mode, max_matches=1 << 20)
+    got = m.scan_array(wl.data)
+    exp = oracle.scan_patterns(wl.patterns, wl.data)
+    rx_ids = {i for i, (k, _) in enumerate(wl.patterns) if k == 1}
+    assert sum(1 for p in exp[:, 0].tolist() if p in rx_ids) >= 20  # regex matches are part of the check
+    assert got.shape == exp.shape and np.array_equal(got, exp)

@@ -508,6 +508,12 @@ class GpuMatcher:
                 "proposer_top1": rep.proposer_top1, "proposer_top4": rep.proposer_top4,
                 "tune_seconds": round(rep.tune_seconds, 2)}
 
+    def set_walk(self, walk_chunk: int = 0, proposer: int = PROPOSER_MLP):
+        """Pins the speculative walk's chunk (0 keeps it) and its boundary
+        guess: the trained proposer (PROPOSER_MLP) or the unanchored start
+        (PROPOSER_NONE), overriding the autotuner.  Matches never change."""
+        _call(N.lib().ws_matcher_set_walk, self._h, int(walk_chunk), int(proposer))
+
     def regex_candidates(self, data, mode: int, distinct: bool = False) -> np.ndarray:
         """K candidates (pattern_id, start, end), unsorted: every anchored match
         end, or with ``distinct`` the candidates a scan works from (the same

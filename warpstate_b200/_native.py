@@ -72,7 +72,9 @@ class WsMatcherInfo(ctypes.Structure):
                 ("proposer_top4", ctypes.c_double), ("last_fixup_chunks", ctypes.c_uint64),
                 ("last_chunks", ctypes.c_uint64), ("last_kcandidates", ctypes.c_uint64),
                 ("last_kernel_ms", ctypes.c_double * 8), ("last_launches", ctypes.c_uint32),
-                ("max_literal_len", ctypes.c_uint32), ("max_regex_len", ctypes.c_int64)]
+                ("max_literal_len", ctypes.c_uint32), ("max_regex_len", ctypes.c_int64),
+                ("last_events", ctypes.c_uint64), ("last_rewalk_bytes", ctypes.c_uint64),
+                ("last_guess_hits", ctypes.c_uint64), ("last_guesses", ctypes.c_uint64)]
 
 
 class WsTuneReport(ctypes.Structure):
@@ -123,6 +125,8 @@ SIGNATURES = {
                                                  ctypes.POINTER(WsErrorInfo)]),
     "ws_matcher_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                        ctypes.c_uint32, ctypes.POINTER(WsTuneReport), ctypes.POINTER(WsErrorInfo)]),
+    "ws_matcher_set_walk": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(WsErrorInfo)]),
     "ws_matcher_get_info":(ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatcherInfo)]),
     "ws_regex_candidates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
                                            ctypes.POINTER(WsMatch), ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),

@@ -133,6 +133,15 @@ uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t*
     rl.cursor = x.cursor;
     rl.base = x.base;
     rl.frontier = x.frontier;
+    rl.need = m->need_dev;
+    if (m->need_host) {
+      // a quarter more than was needed: the reverse walks' shared marks are
+      // lossy, so a repeated scan can append a few more candidates
+      const volatile unsigned long long* need = m->need_host;
+      const uint64_t k = need[0], e = need[1];
+      rl.k_min = k ? k + k / 4 : 0;
+      rl.ev_min = e ? e + e / 4 : 0;
+    }
     launches += run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
   }
   if (prof) check_cuda(cudaEventRecord(m->pev[2], st), "event");
@@ -155,12 +164,17 @@ void read_phases(ws_matcher* m, double* ms) {
   for (int k = 0; k < 8; ++k) ms[k] = tmp.last_kernel_ms[k];
 }
 
-void check_regex_overflow(ws_matcher* m, Scratch& s) {
-  if (!m->rx.n_regex || !s.rx.ptr) return;
-  unsigned long long flag = 0;
-  check_cuda(cudaMemcpy(&flag, static_cast<uint8_t*>(s.rx.ptr) + kRegexErrorFlagOffset, 8, cudaMemcpyDeviceToHost),
-             "D2H flag");
-  if (flag) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow (raise max_matches)", 0, 0, m->cfg.max_matches);
+void raise_candidates_unknown(ws_matcher* m) {
+  const uint64_t need = m->need_host ? std::max(m->need_host[0], m->need_host[1]) : 0;
+  raise(WS_ERR_OVERFLOW, "regex candidates exceed what the device buffers can hold", 0, need,
+        std::min<uint64_t>(need, 0x7FFFFFFFull));
+}
+
+bool repeat_scan(ws_matcher* m, unsigned long long count, int attempt) {
+  if (count == kCountTimeout) raise(WS_ERR_TIMEOUT, "a device-side wait of the scan ran out");
+  if (count != kCountUnknown) return false;
+  if (attempt + 1 >= kCandidateRetries) raise_candidates_unknown(m);
+  return true;
 }
 
 // The windowed form of ws_scan for a large pinned host input (see ws_scan).
@@ -189,11 +203,14 @@ void scan_overlapped(ws_matcher* m, Scratch& s, const uint8_t* data, uint64_t le
   try {
     check_cuda(cudaMemsetAsync(d + len, 0, 64, s.stream), "memset pad");
     ensure(s.out64, dcap * sizeof(ws_match64));
-    enqueue_windows(m, s, s.stream, d, len, W, s.out64.as<ws_match64>(), dcap, d_counter, [&](uint64_t end) {
-      check_cuda(cudaStreamWaitEvent(s.stream, arrived[(end - 1) / W], 0), "wait window");
-    });
-    check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
-    check_cuda(cudaStreamSynchronize(s.stream), "scan");
+    for (int attempt = 0;; ++attempt) {
+      enqueue_windows(m, s, s.stream, d, len, W, s.out64.as<ws_match64>(), dcap, d_counter, [&](uint64_t end) {
+        check_cuda(cudaStreamWaitEvent(s.stream, arrived[(end - 1) / W], 0), "wait window");
+      });
+      check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s.stream), "D2H count");
+      check_cuda(cudaStreamSynchronize(s.stream), "scan");
+      if (!repeat_scan(m, count, attempt)) break;
+    }
   } catch (...) {
     cudaStreamSynchronize(s.copy);  // no copy may still read the caller's input
     throw;
@@ -323,6 +340,13 @@ ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_co
     m->info.filter_period = m->lit.period;
     m->info.filter_bits = m->lit.table_bits;
     regex_fill_info(m->rx, m->info);
+    if (t->n_regex) {
+      check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&m->need_host), 2 * sizeof(unsigned long long),
+                               cudaHostAllocMapped), "cudaHostAlloc(mapped)");
+      m->need_host[0] = m->need_host[1] = 0;
+      check_cuda(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->need_dev), m->need_host, 0),
+                 "cudaHostGetDevicePointer");
+    }
     m->profile = (m->cfg.flags & WS_FLAG_PROFILE) != 0;
     if (m->profile) {
       for (auto& e : m->pev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
@@ -361,12 +385,14 @@ ws_status ws_scan(ws_matcher* m, const uint8_t* data, uint64_t len, ws_match* ou
     }
     stage_input(m, *s, data, len);
     ensure(s->out, dcap * sizeof(ws_match));
-    enqueue_scan(m, *s, s->stream, s->input.as<uint8_t>(), len, s->out.as<ws_match>(), dcap, d_counter);
     unsigned long long count = 0;
-    check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");
-    check_cuda(cudaStreamSynchronize(s->stream), "scan");
+    for (int attempt = 0;; ++attempt) {
+      enqueue_scan(m, *s, s->stream, s->input.as<uint8_t>(), len, s->out.as<ws_match>(), dcap, d_counter);
+      check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream), "D2H count");
+      check_cuda(cudaStreamSynchronize(s->stream), "scan");
+      if (!repeat_scan(m, count, attempt)) break;
+    }
     *n_out = count;
-    check_regex_overflow(m, *s);
     if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches", 0, count, dcap);
     if (count > cap) raise(WS_ERR_OVERFLOW, "too many matches for the output buffer", 0, count, cap);
     read_sorted(*s, s->out.as<ws_match>(), count, out);

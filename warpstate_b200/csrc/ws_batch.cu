@@ -245,20 +245,22 @@ extern "C" ws_status ws_scan_batch(ws_matcher* m, const ws_item* items, uint64_t
         ScanExtras x;
         x.item_end = reinterpret_cast<const uint32_t*>(aux + ends_off);
         x.n_items = (uint32_t)ni;
-        enqueue_scan(m, *s, s->stream, inbuf[gi & 1]->as<uint8_t>(), G.bytes, s->out.as<ws_match>(), dcap,
-                     d_counter, x);
         auto* d_tag = reinterpret_cast<ws_tagged_match*>(aux + tag_off);
-        tag_kernel<<<m->ctx->sm_count * 4, 256, 0, s->stream>>>(s->out.as<ws_match>(), d_counter, dcap,
-                                                                  reinterpret_cast<const uint32_t*>(aux + ends_off),
-                                                                  reinterpret_cast<const uint64_t*>(aux + ids_off),
-                                                                  (uint32_t)ni, d_tag);
-        check_cuda(cudaGetLastError(), "tag_kernel");
-        if (gi + 1 < groups.size()) gather(gi + 1);
         unsigned long long count = 0;
-        check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream),
-                   "D2H count");
-        check_cuda(cudaStreamSynchronize(s->stream), "batch scan");
-        check_regex_overflow(m, *s);
+        for (int attempt = 0;; ++attempt) {
+          enqueue_scan(m, *s, s->stream, inbuf[gi & 1]->as<uint8_t>(), G.bytes, s->out.as<ws_match>(), dcap,
+                       d_counter, x);
+          tag_kernel<<<m->ctx->sm_count * 4, 256, 0, s->stream>>>(s->out.as<ws_match>(), d_counter, dcap,
+                                                                    reinterpret_cast<const uint32_t*>(aux + ends_off),
+                                                                    reinterpret_cast<const uint64_t*>(aux + ids_off),
+                                                                    (uint32_t)ni, d_tag);
+          check_cuda(cudaGetLastError(), "tag_kernel");
+          if (attempt == 0 && gi + 1 < groups.size()) gather(gi + 1);
+          check_cuda(cudaMemcpyAsync(&count, d_counter, sizeof(count), cudaMemcpyDeviceToHost, s->stream),
+                     "D2H count");
+          check_cuda(cudaStreamSynchronize(s->stream), "batch scan");
+          if (!repeat_scan(m, count, attempt)) break;  // else the regex candidates overflowed: scan again
+        }
         if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one batch launch", 0, count, dcap);
         if (total + count <= cap && count) {
           const ws_tagged_match* res = d_tag;

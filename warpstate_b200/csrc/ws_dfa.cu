@@ -50,16 +50,29 @@ struct Event { uint32_t e, state, q, tag; };
 
 // counters block (unsigned long long[16]):
 //  [0] K count  [1] event count  [2] error flags  [3..3+kFixRounds] round-changed flags
-enum { C_K = 0, C_EV = 1, C_ERR = 2, C_ROUND = 3 };
+//  [8] chunk re-walks of the fix-up  [9] bytes those re-walks stepped
+//  [10] boundary guesses that were the true state  [11] boundary guesses
+enum { C_K = 0, C_EV = 1, C_ERR = 2, C_ROUND = 3, C_FIX = 8, C_REWALK = 9, C_HITS = 10, C_GUESSES = 11 };
+// error bits in ctr[C_ERR]: 1 candidate overflow, 2 event overflow, 4 a
+// bounded device-side wait ran out
+constexpr unsigned long long kErrTimeout = 4;
+static_assert(C_ROUND + kFixRounds < C_FIX, "counter slots overlap");
 
-RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_matches) {
+// Candidate and event buffers hold at most this many entries (the per-regex
+// offsets of the resolution are 32-bit).
+constexpr uint64_t kMaxCandidates = 0x7FFFFFFFull;
+
+// k_min / ev_min: capacities an earlier scan of this matcher found it needed.
+RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_matches, uint64_t k_min = 0,
+                uint64_t ev_min = 0) {
   RxLayout L;
   L.chunk = chunk;
   L.n_chunks = (len + chunk - 1) / chunk;
   L.nck = chunk / kCkpt;
   L.n_q = L.n_chunks * p.n_groups;
-  L.k_cap = std::max<uint64_t>(2 * max_matches, len / 256 + 65536);
-  L.ev_cap = L.k_cap;
+  const uint64_t base = std::max<uint64_t>(2 * max_matches, len / 256 + 65536);
+  L.k_cap = std::min(kMaxCandidates, std::max(base, k_min));
+  L.ev_cap = std::min(kMaxCandidates, std::max(base, ev_min));
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t r = o; o = (o + bytes + 255) & ~(size_t)255; return r; };
   L.off_ctr = take(16 * 8);
@@ -235,12 +248,13 @@ __device__ __forceinline__ uint32_t state_of(uint32_t row, uint32_t first, uint3
   return kTrapByte;
 }
 
-// Stages the image (when the group has one) and the class map.
 // Stages a group's hot-row image (224 KiB) and byte-class map into shared
-// memory with two bulk (TMA) copies completing on one mbarrier; a wait that
-// runs out (it should not) falls back to copying with the threads.
-__device__ __forceinline__ void stage_hot(const DevTables& t, uint32_t g, uint32_t off, uint32_t rows,
-                                          uint32_t* img, uint8_t* cls_s) {
+// memory with two bulk (TMA) copies completing on one mbarrier.  The wait is
+// bounded: when it runs out (it should not), the block records a timeout in
+// `err`, waits once more (again bounded) for the copies it issued, and the
+// caller returns without walking (false); the scan then reports the timeout.
+__device__ __forceinline__ bool stage_hot(const DevTables& t, uint32_t g, uint32_t off, uint32_t rows,
+                                          uint32_t* img, uint8_t* cls_s, unsigned long long* err) {
   uint64_t* bar = reinterpret_cast<uint64_t*>(cls_s + 256);
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
@@ -254,15 +268,12 @@ __device__ __forceinline__ void stage_hot(const DevTables& t, uint32_t g, uint32
   }
   bool ok = false;
   for (uint32_t it = 0; it < (1u << 22) && !ok; ++it) ok = mbar_try(bar, 0);
-  if (!__syncthreads_and(ok)) {
-    if (rows) {
-      const uint4* src = reinterpret_cast<const uint4*>(t.hot + off);
-      uint4* dst = reinterpret_cast<uint4*>(img);
-      for (uint32_t k = threadIdx.x; k < kImgWords / 4; k += blockDim.x) dst[k] = __ldg(src + k);
-    }
-    for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cls_s[k] = t.cls[g * 256 + k];
-    __syncthreads();
-  }
+  if (__syncthreads_and(ok)) return true;
+  if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+  ok = false;
+  for (uint32_t it = 0; it < (1u << 22) && !ok; ++it) ok = mbar_try(bar, 0);
+  __syncthreads();
+  return false;
 }
 
 // Slow path of one transition: handles match / cold / dead and returns false
@@ -312,7 +323,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
   uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.ahot_rows);
-  stage_hot(t, g, gd.ahot_off, gd.ahot_rows, img, cls_s);
+  if (!stage_hot(t, g, gd.ahot_off, gd.ahot_rows, img, cls_s, &p.ctr[C_ERR])) return;
   const uint32_t* tab = t.fwd + gd.fwd_off;
   const uint32_t* mp = t.mptr + gd.mptr_off;
   const uint32_t C = gd.n_classes, first = gd.ahot_base, rows = gd.ahot_rows;
@@ -361,7 +372,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
   uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.hot_rows);
-  stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s);
+  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR])) return;
   const uint64_t i = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
   if (i >= p.n_chunks) return;
   const uint32_t* tab = t.fwd + gd.fwd_off;
@@ -473,6 +484,8 @@ __device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uin
   p.used[q] = S;
   p.round[q] = tag;
   p.conv[q] = (uint32_t)conv;
+  atomicAdd(&p.ctr[C_FIX], 1ull);
+  atomicAdd(&p.ctr[C_REWALK], (unsigned long long)(conv - c0));
   uint32_t new_end = converged ? p.spec[q] : st;
   if (new_end != endv[q]) {
     endv[q] = new_end;
@@ -755,12 +768,45 @@ __global__ void k_export_kernel(DevTables t, ScanPtrs p, ws_match* out, uint64_t
   }
 }
 
-// A candidate or event buffer overflow makes the scan's match count exceed the
-// output capacity, so every caller sees MatchBufferOverflow.
-__global__ void finalize_kernel(ScanPtrs p) {
-  if (p.ctr[C_ERR]) {
-    unsigned long long c = *p.out_counter;
-    if (c <= p.out_cap) atomicMax(p.out_counter, (unsigned long long)p.out_cap + 1);
+// After a candidate or event buffer overflow the scan's match count is not
+// known: the count becomes kCountUnknown (larger than any capacity), and the
+// capacities the scan would have needed are recorded in `need` (host-mapped
+// memory of the matcher, read by the next launch), so the same scan run again
+// fits.  One thread, after every other kernel of the scan.
+__global__ void finalize_kernel(ScanPtrs p, unsigned long long* need) {
+  if (p.ctr[C_ERR] & kErrTimeout) {
+    *p.out_counter = kCountTimeout;
+  } else if (p.ctr[C_ERR]) {
+    *p.out_counter = kCountUnknown;
+    if (need) {
+      volatile unsigned long long* v = need;
+      if (p.ctr[C_K] > v[0]) v[0] = p.ctr[C_K];
+      if (p.ctr[C_EV] > v[1]) v[1] = p.ctr[C_EV];
+    }
+  }
+}
+
+// Counts the chunk boundaries whose guess (the proposer's, or the unanchored
+// start) was the true state: the predecessor's end state after the fix-up.
+__global__ void guess_hits_kernel(DevTables t, ScanPtrs p) {
+  const uint32_t g = blockIdx.y;
+  const GroupDev gd = t.groups[g];
+  unsigned long long hits = 0, total = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < p.n_chunks;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t q = (uint64_t)g * p.n_chunks + i;
+    uint32_t guess = p.guess[q];
+    if (guess >= gd.n_states) guess = gd.start_unanchored;
+    hits += guess == p.end[q - 1];
+    total += 1;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    hits += __shfl_down_sync(0xFFFFFFFFu, hits, o);
+    total += __shfl_down_sync(0xFFFFFFFFu, total, o);
+  }
+  if ((threadIdx.x & 31) == 0 && total) {
+    atomicAdd(&p.ctr[C_HITS], hits);
+    atomicAdd(&p.ctr[C_GUESSES], total);
   }
 }
 
@@ -1267,7 +1313,7 @@ void ensure_scratch(DeviceBuffer& scratch, size_t need) {
 uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch, int sm_count,
                         cudaEvent_t* ev) {
   if (!P.n_regex || l.len == 0) return 0;
-  RxLayout L = layout(P, l.len, P.walk_chunk, l.cap);
+  RxLayout L = layout(P, l.len, P.walk_chunk, l.cap, l.k_min, l.ev_min);
   ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   DevTables t = dev_tables(P);
@@ -1286,17 +1332,33 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   k_chain_kernel<<<(P.n_regex + 3) / 4, 128, 0, st>>>(t, p);  // a warp per regex
   check_cuda(cudaGetLastError(), "resolution kernels");
   launches += 6;
-  finalize_kernel<<<1, 1, 0, st>>>(p);
+  finalize_kernel<<<1, 1, 0, st>>>(p, l.need);
   check_cuda(cudaGetLastError(), "finalize_kernel");
   launches += 1;
-  if (ev) check_cuda(cudaEventRecord(ev[5], st), "event");
+  if (ev) {
+    // profiled scans also count the boundary guesses that held and read the
+    // counters back for ws_matcher_get_info
+    if (l.mode != WS_REGEX_PLAIN && L.n_chunks > 1) {
+      dim3 hg2((unsigned)std::min<uint64_t>((L.n_chunks + 255) / 256, 1024), P.n_groups);
+      guess_hits_kernel<<<hg2, 256, 0, st>>>(t, p);
+      check_cuda(cudaGetLastError(), "guess_hits_kernel");
+      launches += 1;
+    }
+    if (!P.prof_ctr) {
+      unsigned long long* h = nullptr;
+      check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&h), 16 * 8, cudaHostAllocDefault), "cudaHostAlloc");
+      std::memset(h, 0, 16 * 8);
+      P.prof_ctr.reset(h);
+    }
+    check_cuda(cudaMemcpyAsync(P.prof_ctr.get(), p.ctr, 16 * 8, cudaMemcpyDeviceToHost, st), "D2H counters");
+    check_cuda(cudaEventRecord(ev[5], st), "event");
+  }
   P.last_chunks = L.n_q;
   P.last_launches = launches;
   return launches;
 }
 
 void regex_collect_timing(const RegexPlan& P, cudaEvent_t* ev, ws_matcher_info& info) {
-  (void)P;
   float ms = 0;
   // [2] proposer, [1] walk or plain, [3] fix-up, [4] reverse, [5] resolution, [6] regex total
   if (cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) info.last_kernel_ms[2] = ms;
@@ -1305,6 +1367,15 @@ void regex_collect_timing(const RegexPlan& P, cudaEvent_t* ev, ws_matcher_info& 
   if (cudaEventElapsedTime(&ms, ev[3], ev[4]) == cudaSuccess) info.last_kernel_ms[4] = ms;
   if (cudaEventElapsedTime(&ms, ev[4], ev[5]) == cudaSuccess) info.last_kernel_ms[5] = ms;
   if (cudaEventElapsedTime(&ms, ev[0], ev[5]) == cudaSuccess) info.last_kernel_ms[6] = ms;
+  if (P.prof_ctr) {
+    const unsigned long long* c = P.prof_ctr.get();
+    info.last_kcandidates = c[C_K];
+    info.last_events = c[C_EV];
+    info.last_fixup_chunks = c[C_FIX];
+    info.last_rewalk_bytes = c[C_REWALK];
+    info.last_guess_hits = c[C_HITS];
+    info.last_guesses = c[C_GUESSES];
+  }
 }
 
 uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uint32_t mode, cudaStream_t st,
@@ -1313,7 +1384,8 @@ uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uin
   const bool full = (mode & WS_CAND_DISTINCT) == 0;
   mode &= ~(uint32_t)WS_CAND_DISTINCT;
   RegexLaunch l{d_data, len, nullptr, cap, nullptr, mode};
-  RxLayout L = layout(P, len, P.walk_chunk, std::max<uint64_t>(cap, 1));
+  // every candidate must fit: the buffers are sized for the caller's capacity
+  RxLayout L = layout(P, len, P.walk_chunk, std::max<uint64_t>(cap, 1), cap, cap);
   ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   p.full_k = full ? 1 : 0;
@@ -1324,7 +1396,9 @@ uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uin
   unsigned long long ctr[16];
   check_cuda(cudaMemcpyAsync(ctr, p.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st), "D2H");
   check_cuda(cudaStreamSynchronize(st), "sync");
-  if (ctr[C_ERR]) raise(WS_ERR_OVERFLOW, "regex candidate buffer overflow", 0, ctr[C_K], L.k_cap);
+  if (ctr[C_ERR] & kErrTimeout) raise(WS_ERR_TIMEOUT, "a device-side wait of the regex walk ran out");
+  if (ctr[C_ERR])  // at least cap + 1 candidates (an event overflow leaves the count short)
+    raise(WS_ERR_OVERFLOW, "too many regex candidates", 0, std::max<uint64_t>(ctr[C_K], cap + 1), cap);
   uint64_t n = std::min<uint64_t>(ctr[C_K], L.k_cap);
   if (n > cap) raise(WS_ERR_OVERFLOW, "too many regex candidates", 0, n, cap);
   if (n) {

@@ -76,8 +76,15 @@ struct RegexPlan {
   double top1 = 0, top4 = 0, start_rate = 0;
   uint32_t walk_chunk = 4096;            // speculative chunk bytes (multiple of 256)
   // last scan
-  uint64_t last_chunks = 0, last_fixup = 0, last_k = 0;
+  uint64_t last_chunks = 0;
   uint32_t last_launches = 0;
+  // profiled scans: the scan's counters (K candidates, events, fix-up
+  // re-walks and bytes, boundary guesses and hits), read back into pinned
+  // memory behind the scan's last phase event
+  struct PinnedDeleter {
+    void operator()(unsigned long long* p) const { cudaFreeHost(p); }
+  };
+  std::unique_ptr<unsigned long long, PinnedDeleter> prof_ctr;
 };
 
 struct RegexLaunch {
@@ -98,7 +105,19 @@ struct RegexLaunch {
   // max(last match end, frontier).
   unsigned long long* cursor = nullptr;
   uint64_t base = 0, frontier = 0;
+  // Candidate-buffer sizing: `need` (device address of two host-mapped
+  // words) receives the candidate and event counts of a scan whose buffers
+  // overflowed; k_min and ev_min are the capacities to reserve (what an
+  // earlier scan needed).
+  unsigned long long* need = nullptr;
+  uint64_t k_min = 0, ev_min = 0;
 };
+
+// Match count of a scan whose regex candidate buffers overflowed: the true
+// count is unknown (repeating the scan succeeds, sized by what it needed).
+constexpr unsigned long long kCountUnknown = ~0ull;
+// Match count of a scan in which a bounded device-side wait ran out.
+constexpr unsigned long long kCountTimeout = ~0ull - 1;
 
 void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, RegexPlan& plan);
 // Re-ranks the forward DFA states of every group by how often a walk over
@@ -110,9 +129,6 @@ void regex_fill_info(const RegexPlan& plan, ws_matcher_info& info);
 // when phase timing is wanted.  Returns the number of kernel launches.
 uint32_t run_regex_scan(RegexPlan& plan, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch,
                         int sm_count, cudaEvent_t* events);
-// Byte offset, inside the regex scratch, of the error-flag word (non-zero after
-// a scan whose candidate or event buffer overflowed).
-constexpr size_t kRegexErrorFlagOffset = 16;
 void regex_collect_timing(const RegexPlan& plan, cudaEvent_t* events, ws_matcher_info& info);
 // K candidates only (diagnostic entry point), copied to host_out.
 uint64_t regex_candidates(RegexPlan& plan, const uint8_t* d_data, uint64_t len, uint32_t mode, cudaStream_t st,

@@ -110,9 +110,15 @@ struct ws_matcher {
   // phase times summed over the windows of the last multi-window scan
   bool use_summed = false;
   double summed_ms[8] = {};
+  // Two host-mapped words (regex candidates, match events) where a scan whose
+  // candidate buffers overflowed records how many it needed; later scans
+  // reserve that much (need_dev is their device address).
+  unsigned long long* need_host = nullptr;
+  unsigned long long* need_dev = nullptr;
   ~ws_matcher() {
     for (auto e : pev) if (e) cudaEventDestroy(e);
     for (auto e : rx_events) if (e) cudaEventDestroy(e);
+    if (need_host) cudaFreeHost(need_host);
   }
 
   std::unique_ptr<ws::Scratch> take();
@@ -167,8 +173,17 @@ uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t*
 // Waits for the last profiled scan and reads its phase times (ms[8], the
 // layout of ws_matcher_info.last_kernel_ms).
 void read_phases(ws_matcher* m, double* ms);
-// Raises MatchBufferOverflow when a regex scratch buffer overflowed.
-void check_regex_overflow(ws_matcher* m, Scratch& s);
+// Scans whose regex candidate buffers overflow report kCountUnknown; the
+// synchronous entry points repeat them (sized by what they needed) up to this
+// many times before giving up with MatchBufferOverflow.
+constexpr int kCandidateRetries = 4;
+// Raises MatchBufferOverflow for a count that stayed unknown.
+[[noreturn]] void raise_candidates_unknown(ws_matcher* m);
+// After a synchronous scan: true when it must be repeated (its regex
+// candidates overflowed; attempt counts from 0), false when `count` is a match
+// count; raises Timeout for a scan whose device-side wait ran out and
+// MatchBufferOverflow once the retries are used up.
+bool repeat_scan(ws_matcher* m, unsigned long long count, int attempt);
 
 // One window of a scan in steps (stream feeds, ws_scan_device64): the bytes
 // seen so far are [0, seen), the previous window started at win_base, regex

@@ -14,7 +14,6 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "ws_internal.h"
 
@@ -31,24 +30,18 @@ static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes]
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
 // Device address of g_noalloc_scratch on the current device.  In host code the
-// array's name is only a host-side stand-in, so the address is looked up once
-// per device with cudaGetSymbolAddress.
-void* scratch_address(int device) {
-  std::lock_guard<std::mutex> g(g_setup_mu);
-  if (device < 0 || device >= kMaxDevices) raise(WS_ERR_DEVICE, "device index out of range for the no-alloc scan");
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      raise(WS_ERR_DEVICE, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
-    g_scratch_addr[device] = p;
-  }
-  return g_scratch_addr[device];
+// array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, with the scan's device current.  It is looked up on
+// every call (a table lookup once the module is loaded) rather than cached:
+// after cudaDeviceReset the module, and with it the array, is loaded again at
+// another address.  The first lookup on a device loads the module.
+void* scratch_address() {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    raise(WS_ERR_DEVICE, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
+  return p;
 }
 
 }  // namespace
@@ -81,7 +74,7 @@ extern "C" ws_status ws_scan_literals_noalloc(ws_matcher* m, const uint8_t* d_da
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(d_count);
     check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st), "memset count");
     if (len == 0 || plan->n_literals == 0) return WS_OK;
-    void* scratch = scratch_address(device);
+    void* scratch = scratch_address();
     uint64_t scap = literal_survivor_cap(len);  // <= the array's capacity for len <= kNoAllocMaxInput
     LiteralLaunch ll{d_data, len, d_out, cap, counter, scratch, scap};
     launch_literal_scan(*plan, ll, st, sm_count);  // clears the survivor counter first

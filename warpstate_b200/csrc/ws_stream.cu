@@ -36,6 +36,7 @@ struct ws_stream {
   uint64_t seen = 0;        // bytes fed so far
   uint64_t frontier = 0;    // regex starts below it are decided
   DeviceBuffer cursor;      // per-regex find_iter position (u64)
+  DeviceBuffer cursor_bak;  // the cursors before the window scan in flight (restored to repeat it)
   std::vector<ws_match64> pending;  // decided, not yet delivered
   size_t delivered = 0;
   std::vector<ws_match> host;       // per-step readback
@@ -69,19 +70,33 @@ bool enqueue_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t
   x.base = st->win_base;
   x.frontier = frontier;
   if (!literals && !m->rx.n_regex) return false;
+  if (m->rx.n_regex)
+    check_cuda(cudaMemcpyAsync(st->cursor_bak.ptr, st->cursor.ptr, (size_t)m->rx.n_regex * 8,
+                               cudaMemcpyDeviceToDevice, s.stream), "D2D cursor");
   enqueue_scan(m, s, s.stream, st->win[st->cur].as<uint8_t>(), st->win_len, s.out.as<ws_match>(), dcap, d_counter, x);
   check_cuda(cudaMemcpyAsync(&st->count, d_counter, sizeof(st->count), cudaMemcpyDeviceToHost, s.stream),
              "D2H count");
   return true;
 }
 
-// Waits for the window scan just enqueued and appends the decided matches.
+// Waits for the window scan just enqueued; false when its regex candidates
+// overflowed (the cursors are then back where the scan found them, so the
+// window can be scanned again).
+bool window_done(ws_stream* st, int attempt) {
+  ws_matcher* m = st->m;
+  Scratch& s = *st->s;
+  check_cuda(cudaStreamSynchronize(s.stream), "stream scan");
+  if (!repeat_scan(m, st->count, attempt)) return true;
+  check_cuda(cudaMemcpyAsync(st->cursor.ptr, st->cursor_bak.ptr, (size_t)m->rx.n_regex * 8,
+                             cudaMemcpyDeviceToDevice, s.stream), "D2D cursor");
+  return false;
+}
+
+// Appends the decided matches of the window scan that window_done accepted.
 void finish_window(ws_stream* st) {
   ws_matcher* m = st->m;
   Scratch& s = *st->s;
   const uint64_t dcap = device_capacity(m);
-  check_cuda(cudaStreamSynchronize(s.stream), "stream scan");
-  check_regex_overflow(m, s);
   const unsigned long long count = st->count;
   if (count > dcap) raise(WS_ERR_OVERFLOW, "too many matches in one stream piece", 0, count, dcap);
   if (count) {
@@ -100,7 +115,11 @@ void finish_window(ws_stream* st) {
 
 // Runs one scan of the current window and appends the decided matches.
 void scan_window(ws_stream* st, bool literals, uint64_t lit_min_end, uint64_t frontier) {
-  if (enqueue_window(st, literals, lit_min_end, frontier)) finish_window(st);
+  for (int attempt = 0;; ++attempt) {
+    if (!enqueue_window(st, literals, lit_min_end, frontier)) return;
+    if (window_done(st, attempt)) break;
+  }
+  finish_window(st);
 }
 
 }  // namespace
@@ -216,6 +235,10 @@ __global__ void __launch_bounds__(1024) widen_kernel(const ws_match* in, const u
                                                      unsigned long long* total) {
   const unsigned long long n = *step_count;
   const unsigned long long at = *total;
+  if (n >= kCountTimeout || at >= kCountTimeout) {  // a timeout or an unknown count stays in the total
+    if (threadIdx.x == 0) *total = (n == kCountTimeout || at == kCountTimeout) ? kCountTimeout : kCountUnknown;
+    return;
+  }
   const unsigned long long avail = n < step_cap ? n : step_cap;
   for (unsigned long long k = threadIdx.x; k < avail; k += blockDim.x) {
     if (at + k >= cap) break;
@@ -319,6 +342,7 @@ ws_status ws_stream_begin(ws_matcher* m, ws_stream** out, ws_error_info* err) {
     check_cuda(cudaStreamWaitEvent(st->s->stream, st->s->busy, 0), "wait");
     if (m->rx.n_regex) {
       st->cursor.alloc((size_t)m->rx.n_regex * 8);
+      st->cursor_bak.alloc((size_t)m->rx.n_regex * 8);
       check_cuda(cudaMemsetAsync(st->cursor.ptr, 0, (size_t)m->rx.n_regex * 8, st->s->stream), "memset cursor");
     }
     *out = st.release();

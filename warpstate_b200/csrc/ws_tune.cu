@@ -176,3 +176,19 @@ extern "C" ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint6
     if (report) *report = rep;
   });
 }
+
+extern "C" ws_status ws_matcher_set_walk(ws_matcher* m, uint32_t walk_chunk, uint32_t proposer, ws_error_info* err) {
+  return guarded(err, [&] {
+    if (!m) raise(WS_ERR_INVALID_ARGUMENT, "null argument");
+    if (walk_chunk && (walk_chunk % 256 != 0 || walk_chunk > (1u << 24)))
+      raise(WS_ERR_INVALID_ARGUMENT, "walk chunk must be a multiple of 256 bytes, at most 16 MiB");
+    if (proposer != WS_PROPOSER_MLP && proposer != WS_PROPOSER_NONE) raise(WS_ERR_INVALID_ARGUMENT, "unknown proposer");
+    if (proposer == WS_PROPOSER_MLP && m->rx.n_regex && !m->rx.proposer)
+      raise(WS_ERR_INVALID_ARGUMENT, "no trained proposer (call ws_matcher_train_proposer or ws_matcher_tune first)");
+    if (walk_chunk) {
+      m->rx.walk_chunk = walk_chunk;
+      m->cfg.walk_chunk = walk_chunk;
+    }
+    m->rx.use_proposer = proposer == WS_PROPOSER_MLP;
+  });
+}
