@@ -125,6 +125,33 @@ typedef struct {
 
 ws_status ws_ir_tables(const ws_ir* ir, ws_pattern_tables* out);
 
+/* Pattern names (PatternSetBuilder::named_literal / named_regex,
+ * core/src/pattern/compiler.rs:50-93), kept with the IR so that a compiled
+ * index carries them.  ws_ir_name writes the name's UTF-8 bytes (not
+ * NUL-terminated) and sets *n_out to its length, or to UINT64_MAX when the
+ * pattern has no name. */
+ws_status ws_ir_set_name(ws_ir* ir, uint64_t pattern_id, const char* name, uint64_t len);
+ws_status ws_ir_name(const ws_ir* ir, uint64_t pattern_id, char* out, uint64_t cap, uint64_t* n_out);
+
+/* ----------------------------------------------------------- compiled index */
+/* CompiledPatternIndex::load (core/src/compiled_index/mod.rs:58-260): parses
+ * the reference's on-disk index (magic WPSIDX01, versions 1-3, CRC-32 of
+ * version 3) into an IR, with the reference's own validation and errors
+ * (PatternCompilationFailed for a corrupt, truncated or inconsistent file,
+ * InputTooLarge above 512 MiB).  The literal tables -- packed bytes, offsets,
+ * ids and the LiteralPrefilterTable -- are used as stored (after bounds
+ * checks); regexes come from their stored sources (version 2 and later), and
+ * the stored regex-automata DFAs are checked for shape and not used. */
+ws_status ws_index_load(const uint8_t* bytes, uint64_t len, ws_ir** out, ws_error_info* err);
+
+/* CompiledPatternIndex::build (core/src/compiled_index/builder.rs:8-64):
+ * serializes an IR in the version 3 format, with names, regex sources and the
+ * literal tables, and no serialized regex-automata DFAs (the regex section is
+ * rebuilt from the sources on load, here and by the reference's
+ * to_pattern_set).  *n_out receives the size; WS_ERR_OVERFLOW when it exceeds
+ * cap (call again with a larger buffer). */
+ws_status ws_index_save(const ws_ir* ir, uint8_t* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
+
 /* ------------------------------------------------------------------ matcher */
 /* AutoMatcherConfig (core/src/config.rs:39-173) plus the B200 plan knobs. */
 typedef struct {

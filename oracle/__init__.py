@@ -196,25 +196,32 @@ def sort_matches(a: np.ndarray) -> np.ndarray:
     return a[idx]
 
 
-def scan_patterns(patterns: list[tuple[int, bytes]], data, threads: int = 0) -> np.ndarray:
+_FOLD = np.arange(256, dtype=np.uint8)
+_FOLD[ord("A"):ord("Z") + 1] |= 0x20
+
+
+def ascii_fold(data) -> np.ndarray:
+    """A-Z mapped to a-z, every other byte unchanged: the byte equivalence of
+    an Aho-Corasick automaton built with ascii_case_insensitive(true), which
+    PatternSetBuilder::case_insensitive selects for the literal patterns
+    (core/src/pattern/compiler.rs:66-76,247-281)."""
+    a = np.frombuffer(data, dtype=np.uint8) if isinstance(data, (bytes, bytearray)) else np.asarray(data)
+    return _FOLD[a.view(np.uint8).reshape(-1)]
+
+
+def scan_patterns(patterns: list[tuple[int, bytes]], data, threads: int = 0,
+                  case_insensitive: bool = False) -> np.ndarray:
     """The full parity contract of a pattern list: literal patterns (and regexes
     the reference demotes to literals) under L, the other regexes under R,
-    sorted by (start, pattern_id, end)."""
-    lits, lit_ids, rxs, rx_ids = [], [], [], []
-    for i, (kind, b) in enumerate(patterns):
-        if kind == 0:
-            lits.append(bytes(b))
-            lit_ids.append(i)
-        else:
-            src = b.decode() if isinstance(b, (bytes, bytearray)) else b
-            lit = regex_literal(src)
-            if lit:
-                lits.append(lit)
-                lit_ids.append(i)
-            else:
-                rxs.append(Regex(src))
-                rx_ids.append(i)
-    parts = [literal_scan(lits, lit_ids, data, threads), regex_scan(rxs, rx_ids, data, threads)]
+    sorted by (start, pattern_id, end).  With ``case_insensitive`` the
+    literals match ASCII case-insensitively (L over case-folded bytes);
+    regexes are unaffected."""
+    lits, lit_ids, rxs, rx_ids = split_patterns(patterns)
+    if case_insensitive:
+        lit_part = literal_scan([bytes(ascii_fold(l)) for l in lits], lit_ids, ascii_fold(data), threads)
+    else:
+        lit_part = literal_scan(lits, lit_ids, data, threads)
+    parts = [lit_part, regex_scan(rxs, rx_ids, data, threads)]
     return sort_matches(np.concatenate(parts, axis=0))
 
 
@@ -241,12 +248,26 @@ def split_patterns(patterns: list[tuple[int, bytes]]):
 TAGGED = np.dtype([("sid", "<u8"), ("pid", "<u4"), ("start", "<u4"), ("end", "<u4"), ("res", "<u4")])
 
 
-def batch_scan(patterns: list[tuple[int, bytes]], data, items, ids=None, threads: int = 0) -> np.ndarray:
+def batch_scan(patterns: list[tuple[int, bytes]], data, items, ids=None, threads: int = 0,
+               case_insensitive: bool = False) -> np.ndarray:
     """Batch contract (scan_batch_cpu, core/src/batch.rs:170-195): items are
     (offset, length) slices of ``data``, each scanned on its own; returns an
     (n, 4) uint64 array (source_id, pattern_id, start, end) sorted by
-    (source_id, start, pattern_id, end)."""
+    (source_id, start, pattern_id, end).  ``case_insensitive`` as in
+    scan_patterns."""
+    if case_insensitive:
+        # literal part on folded bytes, regex part on the bytes as they are
+        lits, lit_ids, rxs, rx_ids = split_patterns(patterns)
+        a = _batch_scan_split([bytes(ascii_fold(l)) for l in lits], lit_ids, [], [], ascii_fold(data), items, ids,
+                              threads)
+        b = _batch_scan_split([], [], rxs, rx_ids, data, items, ids, threads)
+        r = np.concatenate([a, b], axis=0)
+        return r[np.lexsort((r[:, 3], r[:, 1], r[:, 2], r[:, 0]))]
     lits, lit_ids, rxs, rx_ids = split_patterns(patterns)
+    return _batch_scan_split(lits, lit_ids, rxs, rx_ids, data, items, ids, threads)
+
+
+def _batch_scan_split(lits, lit_ids, rxs, rx_ids, data, items, ids, threads) -> np.ndarray:
     packed = b"".join(lits)
     offs, o = [], 0
     for l in lits:

@@ -36,6 +36,7 @@ __all__ = [
     "MatchBufferOverflow", "PathologicalRegex", "PatternSet", "PatternSetBuilder", "AutoMatcherConfig",
     "GpuMatcher", "WarpStateer", "GpuScanner", "AutoMatcher", "ScanItem", "TaggedMatch", "BatchConfig",
     "scan_batch", "scan_batch_gpu", "scan_batch_auto", "StreamPipeline", "REGEX_SPECULATIVE", "REGEX_PLAIN",
+    "CompiledPatternIndex",
 ]
 
 REGEX_SPECULATIVE = 0
@@ -228,6 +229,10 @@ class PatternSetBuilder:
             specs[i].len = len(b)
         h = ctypes.c_void_p()
         _call(L.ws_ir_build, specs, n, 1 if self._ci else 0, ctypes.byref(h))
+        for i, (_, _, name) in enumerate(self._patterns):
+            if name is not None:
+                nb = name.encode("utf-8")
+                _call_noerr(L.ws_ir_set_name, h, i, nb, len(nb))
         return PatternSet(h, [p[2] for p in self._patterns], self._dfa_size_limit)
 
 
@@ -236,11 +241,21 @@ class PatternSet:
 
     def __init__(self, handle, names, dfa_size_limit):
         self._h = handle
-        self.names = names
         self.dfa_size_limit = dfa_size_limit
         t = N.WsPatternTables()
         _call_noerr(N.lib().ws_ir_tables, self._h, ctypes.byref(t))
         self._tables = t
+        if names is None:  # names stored with the IR (a loaded index)
+            names = []
+            n = ctypes.c_uint64()
+            buf = ctypes.create_string_buffer(4096)
+            for i in range(t.n_patterns):
+                st = N.lib().ws_ir_name(self._h, i, buf, 4096, ctypes.byref(n))
+                if st == 11:
+                    buf = ctypes.create_string_buffer(n.value)
+                    st = N.lib().ws_ir_name(self._h, i, buf, n.value, ctypes.byref(n))
+                names.append(None if st != 0 or n.value == 0xFFFFFFFFFFFFFFFF else buf.raw[: n.value].decode())
+        self.names = names
 
     @staticmethod
     def builder() -> PatternSetBuilder:
@@ -288,6 +303,75 @@ class PatternSet:
             except Exception:
                 pass
             self._h = None
+
+
+class CompiledPatternIndex:
+    """CompiledPatternIndex (core/src/compiled_index/mod.rs:22-260): the
+    reference's on-disk pattern index.  ``load`` parses and validates it
+    (magic, version, CRC-32, consistency) into a pattern set whose literal
+    tables are the stored ones; ``scan`` runs it on the GPU."""
+
+    MAX_BYTES = 512 * 1024 * 1024  # mod.rs:19
+
+    def __init__(self, serialized: bytes):
+        self._bytes = bytes(serialized)
+        self._ps = self._parse()
+        self._matcher = None
+
+    def _parse(self) -> "PatternSet":
+        buf = ctypes.create_string_buffer(self._bytes, len(self._bytes)) if self._bytes else None
+        h = ctypes.c_void_p()
+        _call(N.lib().ws_index_load, ctypes.cast(buf, ctypes.c_void_p).value if buf is not None else None,
+              len(self._bytes), ctypes.byref(h))
+        return PatternSet(h, None, 50_000_000)
+
+    @staticmethod
+    def build(patterns: "PatternSet") -> bytes:
+        """Serialized index image of a pattern set (builder.rs:8-64)."""
+        n = ctypes.c_uint64()
+        err = N.WsErrorInfo()
+        st = N.lib().ws_index_save(patterns._h, None, 0, ctypes.byref(n), ctypes.byref(err))
+        if st not in (0, 11):
+            _raise(st, err)
+        out = ctypes.create_string_buffer(max(n.value, 1))
+        _call(N.lib().ws_index_save, patterns._h, out, n.value, ctypes.byref(n))
+        return out.raw[: n.value]
+
+    @classmethod
+    def load(cls, data: bytes) -> "CompiledPatternIndex":
+        return cls(data)
+
+    @classmethod
+    def load_from_file(cls, path) -> "CompiledPatternIndex":
+        import os
+        size = os.path.getsize(path)
+        if size > cls.MAX_BYTES:
+            raise InputTooLarge(size, cls.MAX_BYTES)
+        with open(path, "rb") as f:
+            return cls(f.read())
+
+    def save_to_file(self, path) -> None:
+        with open(path, "wb") as f:
+            f.write(self._bytes)
+
+    def to_bytes(self) -> bytes:
+        return self._bytes
+
+    def names(self) -> list:
+        return self._ps.names
+
+    def literal_count(self) -> int:
+        return int(self._ps.tables().n_literals)
+
+    def to_pattern_set(self) -> "PatternSet":
+        """A pattern set equal to the one the index was built from."""
+        return self._parse()
+
+    def scan(self, data) -> list[Match]:
+        """Scan on the GPU with the index's pattern set (sorted matches)."""
+        if self._matcher is None:
+            self._matcher = GpuMatcher(self._ps)
+        return self._matcher.scan(data)
 
 
 def _call_noerr(fn, *args):

@@ -94,6 +94,12 @@ SIGNATURES = {
                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),
     "ws_ir_destroy": (None, [ctypes.c_void_p]),
     "ws_ir_tables": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsPatternTables)]),
+    "ws_ir_set_name": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64]),
+    "ws_ir_name": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64, c_u64p]),
+    "ws_index_load": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p),
+                                     ctypes.POINTER(WsErrorInfo)]),
+    "ws_index_save": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, c_u64p,
+                                     ctypes.POINTER(WsErrorInfo)]),
     "ws_config_default": (None, [ctypes.POINTER(WsConfig)]),
     "ws_matcher_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsPatternTables), ctypes.POINTER(WsConfig),
                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <numeric>
@@ -361,9 +362,22 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
 }
 
 // ------------------------------------------------------- speculative walk
+// 16 input bytes of a chunk (global loads that do not allocate in L1, which
+// keeps L1 for the class-indexed rows of cold states).
+__device__ __forceinline__ uint4 load_stream16(const uint8_t* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
 // Thread per (group, chunk): unanchored walk from the proposed start state,
 // recording the state every kCkpt bytes, the end state and every match event.
 // blockIdx.y = group; the group's hottest rows sit in shared memory.
+// V bit 0: slow words handled at the byte (else a careful re-walk of the
+// 16-byte block); V bit 1: input loads bypass L1.
+template <int V>
 __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, ScanPtrs p) {
   extern __shared__ __align__(16) uint32_t smem[];
   // blockIdx.x = group (fastest), so the groups' blocks over the same chunks
@@ -390,36 +404,28 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
   uint32_t cold_row = 0;
   uint32_t st = state_of(start, 0, H, (uint32_t)lane4, &cold_row);
   const uint64_t nfull = (c1 - c0) / 16;
+  auto load16 = [&](uint64_t k) -> uint4 {
+    const uint8_t* a = p.data + c0 + k * 16;
+    if (V & 2) return load_stream16(a);
+    return __ldg(reinterpret_cast<const uint4*>(a));
+  };
   // four 16-byte vectors in flight ahead of the walk
   constexpr int kAhead = 4;
   uint4 ring[kAhead];
 #pragma unroll
-  for (int a = 0; a < kAhead; ++a)
-    ring[a] = (uint64_t)a < nfull ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + a * 16)) : make_uint4(0, 0, 0, 0);
+  for (int a = 0; a < kAhead; ++a) ring[a] = (uint64_t)a < nfull ? load16(a) : make_uint4(0, 0, 0, 0);
   for (uint64_t k16 = 0; k16 < nfull; ++k16) {
     const uint4 cur = ring[0];
     const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
     for (int a = 0; a < kAhead - 1; ++a) ring[a] = ring[a + 1];
-    ring[kAhead - 1] = (k16 + kAhead < nfull) ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + (k16 + kAhead) * 16))
-                                              : make_uint4(0, 0, 0, 0);
-    // optimistic pass: fast entries only; a slow word (negative) sends the walk
-    // to the first row (in bounds) and marks the block for the careful pass
-    const uint32_t st0 = st, cold0 = cold_row;
-    uint32_t acc = 0;
+    ring[kAhead - 1] = (k16 + kAhead < nfull) ? load16(k16 + kAhead) : make_uint4(0, 0, 0, 0);
+    if (V & 1) {
+      // every byte: a fast entry (the next row's column) or, rarely, the slow
+      // path for a match, cold or dead transition
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
-      uint32_t w = WS_STEP_FAST(img, st, b);
-      acc |= w;
-      st = (uint32_t)max((int32_t)w, lane4);
-    }
-    if ((int32_t)acc < 0) {
-      // careful pass over the same 16 bytes: match events, cold rows
-      st = st0;
-      cold_row = cold0;
       for (int k = 0; k < 16; ++k) {
-        uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+        uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
         uint32_t w = WS_STEP_FAST(img, st, b);
         if ((int32_t)w >= 0) {
           st = (uint32_t)max((int32_t)w, lane4);
@@ -427,6 +433,35 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
           uint32_t m_row;
           slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
           if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(c0 + k16 * 16 + k + 1), m_row, (uint32_t)q, 0);
+        }
+      }
+    } else {
+      // optimistic pass: fast entries only; a slow word (negative) sends the
+      // walk to the first row (in bounds) and marks the block for the careful
+      // pass
+      const uint32_t st0 = st, cold0 = cold_row;
+      uint32_t acc = 0;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
+        uint32_t w = WS_STEP_FAST(img, st, b);
+        acc |= w;
+        st = (uint32_t)max((int32_t)w, lane4);
+      }
+      if ((int32_t)acc < 0) {
+        // careful pass over the same 16 bytes: match events, cold rows
+        st = st0;
+        cold_row = cold0;
+        for (int k = 0; k < 16; ++k) {
+          uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+          uint32_t w = WS_STEP_FAST(img, st, b);
+          if ((int32_t)w >= 0) {
+            st = (uint32_t)max((int32_t)w, lane4);
+          } else {
+            uint32_t m_row;
+            slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
+            if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(c0 + k16 * 16 + k + 1), m_row, (uint32_t)q, 0);
+          }
         }
       }
     }
@@ -878,8 +913,16 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
   }
   mark(1);
   size_t smem = hot_smem_bytes(max_rows(P, false));
-  set_smem(dfa_walk_kernel, smem, "smem(walk)");
-  dfa_walk_kernel<<<cgrid, kWalkThreads, smem, st>>>(t, p);
+  static const int variant = getenv("WS_WALK_VARIANT") ? atoi(getenv("WS_WALK_VARIANT")) : 0;
+  switch (variant) {
+#define WS_WALK_CASE(v)                                                    \
+    case v:                                                                \
+      set_smem(dfa_walk_kernel<v>, smem, "smem(walk)");                    \
+      dfa_walk_kernel<v><<<cgrid, kWalkThreads, smem, st>>>(t, p);         \
+      break;
+    WS_WALK_CASE(1) WS_WALK_CASE(2) WS_WALK_CASE(3)
+    default: WS_WALK_CASE(0)
+  }
   check_cuda(cudaGetLastError(), "dfa_walk_kernel");
   launches++;
   mark(2);

@@ -52,7 +52,19 @@ struct IrData {
   std::vector<const char*> regex_ptrs;        // views for ws_pattern_tables
   uint32_t n_patterns = 0;
   bool case_insensitive = false;
+  // optional pattern names (a CompiledPatternIndex carries them)
+  std::vector<std::string> names;
+  std::vector<uint8_t> named;
 };
+
+}  // namespace ws
+
+// The handle behind ws_ir (a built pattern set or a loaded compiled index).
+struct ws_ir {
+  ws::IrData d;
+};
+
+namespace ws {
 
 // LiteralPrefilterTable::build (core/src/literal_prefilter.rs:23-88).
 void build_prefilter_table(const std::vector<uint32_t>& offsets, const std::vector<uint32_t>& hashes,
@@ -120,7 +132,23 @@ struct LiteralPlan {
   DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2, d_big,
       d_filter8;
   uint32_t n_buckets = 0;
+  // ASCII case-insensitive: the tables hold folded literals and the kernels
+  // fold the input (A-Z to a-z) before hashing and comparing.
+  bool fold = false;
 };
+
+// ASCII case folding of the case-insensitive literal scan: A-Z to a-z.
+__host__ __device__ inline uint8_t ascii_fold(uint8_t c) { return (c >= 'A' && c <= 'Z') ? (uint8_t)(c | 0x20) : c; }
+
+// The same for the four bytes of a word at once: a byte is an upper-case
+// letter when its low seven bits are at least 0x41 and below 0x5B and its top
+// bit is clear; adding 0x3F and 0x25 to the low seven bits sets bit 7 exactly
+// at those bounds (no carry leaves a byte), and 0x80 >> 2 is the case bit.
+__host__ __device__ inline uint32_t ascii_fold4(uint32_t w) {
+  const uint32_t x = w & 0x7F7F7F7Fu;
+  const uint32_t upper = (x + 0x3F3F3F3Fu) & ~(x + 0x25252525u) & ~w & 0x80808080u;
+  return w | (upper >> 2);
+}
 
 constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
 constexpr uint32_t kBigBits = 25;     // stage-1b table: 2^25 bytes, 32 MiB, read through L2

@@ -5,10 +5,6 @@
 
 #include "ws_internal.h"
 
-struct ws_ir {
-  ws::IrData d;
-};
-
 namespace ws {
 
 void raise(ws_status s, const std::string& msg, uint64_t index, uint64_t count, uint64_t max) {
@@ -97,9 +93,32 @@ void DeviceBuffer::upload(const void* src, size_t n) {
   if (n) check_cuda(cudaMemcpy(ptr, src, n, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
 }
 
-void plan_literals(const ws_pattern_tables& t, LiteralPlan& plan) {
-  plan.n_literals = t.n_literals;
-  if (t.n_literals == 0) return;
+void plan_literals(const ws_pattern_tables& given, LiteralPlan& plan) {
+  plan.n_literals = given.n_literals;
+  if (given.n_literals == 0) return;
+  // ASCII case-insensitive sets (PatternSetBuilder::case_insensitive,
+  // core/src/pattern/compiler.rs:66-76, an Aho-Corasick automaton with
+  // ascii_case_insensitive): every table below is planned on the literals
+  // with A-Z folded to a-z, the prefilter table rebuilt on their FNV-1a
+  // hashes, and the kernels fold the input the same way.
+  ws_pattern_tables t = given;
+  std::vector<uint8_t> folded;
+  std::vector<uint32_t> foffsets, fhashes, fmeta, franges, fentries;
+  plan.fold = given.case_insensitive != 0;
+  if (plan.fold) {
+    folded.assign(given.packed_bytes, given.packed_bytes + given.packed_len);
+    for (uint8_t& c : folded) c = ascii_fold(c);
+    foffsets.assign(given.offsets, given.offsets + 2 * (size_t)given.n_literals);
+    for (uint32_t li = 0; li < given.n_literals; ++li)
+      fhashes.push_back(fnv1a(folded.data() + foffsets[2 * li], foffsets[2 * li + 1], HASH_WINDOW));
+    build_prefilter_table(foffsets, fhashes, HASH_WINDOW, fmeta, franges, fentries);
+    t.packed_bytes = folded.data();
+    t.hash_window_len = HASH_WINDOW;
+    t.prefix_meta = fmeta.data();
+    t.bucket_ranges = franges.data();
+    t.n_buckets = (uint32_t)(franges.size() / 2);
+    t.entries = fentries.data();
+  }
   uint32_t min_long = UINT32_MAX;
   plan.max_len = 0;
   for (uint32_t li = 0; li < t.n_literals; ++li) {

@@ -28,6 +28,8 @@
 // The output is contract L: every overlapping occurrence of every literal.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "ws_internal.h"
 
 namespace ws {
@@ -73,7 +75,12 @@ struct LitArgs {
   const uint8_t* big;        // stage-1b gram table (2^kBigBits bytes, L2), or null
   const uint8_t* filter8;    // byte-wide stage 1 of the lean kernel (2^kFilter8Bits), or null
   uint32_t verify_bloom;     // the verify kernel runs stage 1.5 first
+  uint32_t fold;             // ASCII case-insensitive: input bytes A-Z read as a-z
 };
+
+__device__ __forceinline__ uint4 fold16(uint4 v) {
+  return make_uint4(ascii_fold4(v.x), ascii_fold4(v.y), ascii_fold4(v.z), ascii_fold4(v.w));
+}
 
 __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint32_t bits) {
   uint32_t h = (gram * 0x9E3779B1u) >> (32 - bits);
@@ -110,6 +117,12 @@ __device__ __forceinline__ uint32_t word_at(const uint8_t* d, uint32_t len, uint
   return x;
 }
 
+// word_at for the scan's input, case-folded for case-insensitive sets.
+__device__ __forceinline__ uint32_t input_word(const LitArgs& a, uint32_t len, uint32_t at) {
+  const uint32_t w = word_at(a.data, len, at);
+  return a.fold ? ascii_fold4(w) : w;
+}
+
 // The reference's per-position probe and exact verify (stage 2).  Inputs of
 // one launch are below 4 GiB.  The hashed bytes come from two words read
 // once, and a candidate literal is compared a word at a time (literal bytes
@@ -118,8 +131,7 @@ __device__ void verify_position(const LitArgs& a, uint64_t s64) {
   if (s64 >= a.max_start) return;
   const uint32_t s = (uint32_t)s64, len = (uint32_t)a.len;
   const uint32_t w0 = s & ~3u, sh = (s & 3) * 8;
-  const uint32_t x0 = word_at(a.data, len, w0), x1 = word_at(a.data, len, w0 + 4),
-                 x2 = word_at(a.data, len, w0 + 8);
+  const uint32_t x0 = input_word(a, len, w0), x1 = input_word(a, len, w0 + 4), x2 = input_word(a, len, w0 + 8);
   const uint32_t lo = __funnelshift_r(x0, x1, sh), hi = __funnelshift_r(x1, x2, sh);
   uint32_t h = 2166136261u;
   const uint32_t rem = len - s;
@@ -138,7 +150,7 @@ __device__ void verify_position(const LitArgs& a, uint64_t s64) {
       bool eq = true;
       uint32_t cur = x0;
       for (uint32_t k = 0; k < info.y; k += 4) {
-        const uint32_t nxt = word_at(a.data, len, w0 + k + 4);
+        const uint32_t nxt = input_word(a, len, w0 + k + 4);
         const uint32_t dw = __funnelshift_r(cur, nxt, sh);
         const uint32_t left = info.y - k;
         const uint32_t m = left >= 4 ? 0xFFFFFFFFu : ((1u << (8 * left)) - 1u);
@@ -345,8 +357,9 @@ __global__ void __launch_bounds__(kThreads, 1) literal_filter_kernel(LitArgs a) 
   const uint32_t nwarps = gridDim.x * kWarps;
   const uint32_t bits = a.bits;
   auto load = [&](uint32_t v) -> uint4 {
-    if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
-    return v < nvec ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
+    const uint4 x = v < full_vecs ? __ldg(reinterpret_cast<const uint4*>(a.data) + v)
+                    : v < nvec ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
+    return a.fold ? fold16(x) : x;
   };
 
   uint32_t b = blockIdx.x * kWarps + warp;
@@ -492,8 +505,9 @@ __global__ void __launch_bounds__(kBigThreads, 1) literal_filter_big_kernel(LitA
   const uint32_t nwarps = gridDim.x * kBigWarps;
   const uint32_t bits = a.bits;
   auto load = [&](uint32_t v) -> uint4 {
-    if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
-    return v < nvec ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
+    const uint4 x = v < full_vecs ? __ldg(reinterpret_cast<const uint4*>(a.data) + v)
+                    : v < nvec ? load_vec(a.data, a.len, v) : make_uint4(0, 0, 0, 0);
+    return a.fold ? fold16(x) : x;
   };
   const uint4 zero = make_uint4(0, 0, 0, 0);
 
@@ -578,16 +592,46 @@ struct LeanGrams {
   uint32_t n[4], bw[4];
 };
 
+// L2 eviction policies: the input streams through L2 once (evict first), the
+// stage-1b table should stay (evict last).
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// 16 input bytes, not kept in L1, evict-first in L2.
+__device__ __forceinline__ uint4 ld_stream16(const void* ptr, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(ptr), "l"(pol));
+  return v;
+}
+// One byte of a table that should stay in L2.
+__device__ __forceinline__ uint32_t ld_keep8(const uint8_t* ptr, uint64_t pol) {
+  unsigned short v;
+  asm volatile("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(ptr), "l"(pol));
+  return v;
+}
+
 // Stage 1 of a lane's four aligned grams from the byte table in shared memory
 // (top kFilter8Bits bits of the hash); the stage-1b loads from the byte table
 // in L2 (top kBigBits bits) are issued for the grams that pass.
-__device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g) {
+template <bool kHint>
+__device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g,
+                                           uint64_t keep) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint32_t hf = w[q] * 0x9E3779B1u;
     g.n[q] = filt[hf >> (32 - kFilter8Bits)];
-    g.bw[q] = g.n[q] ? __ldg(big + (hf >> (32 - kBigBits))) : 0u;
+    const uint8_t* at = big + (hf >> (32 - kBigBits));
+    g.bw[q] = g.n[q] ? (kHint ? ld_keep8(at, keep) : (uint32_t)__ldg(at)) : 0u;
   }
 }
 
@@ -658,6 +702,7 @@ __device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, cons
   }
 }
 
+template <bool kHint>
 __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a) {
   constexpr uint32_t W = kLeanThreads / 32, V = kLeanVecs;
   extern __shared__ __align__(16) uint8_t smem8[];
@@ -677,11 +722,14 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   const uint32_t nw = gridDim.x * W;
   const uint8_t* big = a.big;
   const uint4 zero = make_uint4(0, 0, 0, 0);
+  const uint64_t stream_pol = kHint ? l2_evict_first() : 0, keep_pol = kHint ? l2_evict_last() : 0;
   // half h of warp step blk: the 512 coalesced bytes at (blk * V + h) * 512
   auto load = [&](uint32_t blk, uint32_t h) -> uint4 {
     const uint32_t v = (blk * V + h) * 32 + lane;
-    if (v < full_vecs) return __ldg(reinterpret_cast<const uint4*>(a.data) + v);
-    return v < nvec ? load_vec(a.data, a.len, v) : zero;
+    const uint4 x = v < full_vecs ? (kHint ? ld_stream16(reinterpret_cast<const uint4*>(a.data) + v, stream_pol)
+                                           : __ldg(reinterpret_cast<const uint4*>(a.data) + v))
+                    : v < nvec ? load_vec(a.data, a.len, v) : zero;
+    return a.fold ? fold16(x) : x;
   };
   uint32_t b = blockIdx.x * W + warp;
   LeanSlots slots;
@@ -692,7 +740,7 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
 #pragma unroll
   for (uint32_t h = 0; h < V; ++h) {
     vn[h] = b + nw < nblk ? load(b + nw, h) : zero;
-    if (b < nblk) lean_issue(filt, big, load(b, h), gc[h]);
+    if (b < nblk) lean_issue<kHint>(filt, big, load(b, h), gc[h], keep_pol);
   }
   for (; b < nblk; b += nw) {
     const uint32_t b1 = b + nw, b2 = b1 + nw;
@@ -702,7 +750,7 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
 #pragma unroll
     for (uint32_t h = 0; h < V; ++h) {
       vn2[h] = b2 < nblk ? load(b2, h) : zero;
-      if (b1 < nblk) lean_issue(filt, big, vn[h], gn[h]);
+      if (b1 < nblk) lean_issue<kHint>(filt, big, vn[h], gn[h], keep_pol);
       base[h] = (b * V + h) * 512 + lane * 16;
       mask[h] = lean_finish(gc[h], base[h], len);
     }
@@ -725,8 +773,7 @@ __global__ void __launch_bounds__(256) literal_verify_kernel(LitArgs a) {
     if (s == kNoSurvivor) continue;  // a slot the lean kernel reserved but did not fill
     if (a.verify_bloom) {  // stage 1.5 for survivors of the lean kernel
       const uint32_t len = (uint32_t)a.len, w0 = s & ~3u, sh = (s & 3) * 8;
-      const uint32_t x0 = word_at(a.data, len, w0), x1 = word_at(a.data, len, w0 + 4),
-                     x2 = word_at(a.data, len, w0 + 8);
+      const uint32_t x0 = input_word(a, len, w0), x1 = input_word(a, len, w0 + 4), x2 = input_word(a, len, w0 + 8);
       const uint32_t lo = __funnelshift_r(x0, x1, sh), hi = __funnelshift_r(x1, x2, sh);
       bool keep = false;
       for (uint32_t m = a.parts; m; m &= m - 1) {
@@ -785,6 +832,7 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.big = plan.has_big ? plan.d_big.as<uint8_t>() : nullptr;
   a.filter8 = plan.has_big ? plan.d_filter8.as<uint8_t>() : nullptr;
   a.verify_bloom = 0;
+  a.fold = plan.fold ? 1 : 0;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
   if (l.len > 0xFFFFFFFFull) raise(WS_ERR_INPUT_TOO_LARGE, "literal scan launch beyond 32-bit offsets", 0, l.len,
                                    0xFFFFFFFFull);
@@ -812,9 +860,11 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   if (lg && !sh && a.big && a.filter8 && plan.period == 4 && plan.gram_len == 4) {
     a.verify_bloom = 1;
     const size_t lsmem = (size_t)1 << kFilter8Bits;
-    check_cuda(cudaFuncSetAttribute(literal_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
+    static const int variant = getenv("WS_LIT_VARIANT") ? atoi(getenv("WS_LIT_VARIANT")) : 0;
+    auto lean = variant & 1 ? literal_lean_kernel<true> : literal_lean_kernel<false>;
+    check_cuda(cudaFuncSetAttribute(lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
                "cudaFuncSetAttribute(literal lean)");
-    literal_lean_kernel<<<sm_count, kLeanThreads, lsmem, st>>>(a);
+    lean<<<sm_count, kLeanThreads, lsmem, st>>>(a);
     check_cuda(cudaGetLastError(), "literal_lean_kernel launch");
   } else if (lg && sh && a.big && plan.period == 4 && plan.gram_len == 4) {
     run_big(literal_filter_big_kernel<4, true>);
