@@ -291,6 +291,37 @@ ws_status ws_stream_end(ws_stream* s, ws_match64* out, uint64_t cap, uint64_t* n
                         ws_error_info* err);
 void ws_stream_destroy(ws_stream* s);
 
+/* Zero-copy scan session: StreamPipeline::scan_zero_copy / ZeroCopyScan
+ * (core/src/pipeline.rs:31-83) over DmaStagingBuffer (core/src/dma.rs:17-141).
+ * ws_zero_copy_begin returns in *mapped a writable buffer of input_len bytes
+ * of pinned, device-mapped host memory owned by the library; the caller fills
+ * it and calls ws_zero_copy_finish, which scans it exactly as ws_scan does
+ * (same output, sorting and errors) with the device copies reading the
+ * caller's bytes in place, and ends the session (the buffer returns to a
+ * per-matcher pool and must not be touched afterwards).  ws_zero_copy_abort
+ * ends a session without scanning.  Staging buffers are freed with the
+ * matcher; end every session before destroying its matcher. */
+typedef struct ws_zero_copy ws_zero_copy;
+ws_status ws_zero_copy_begin(ws_matcher* m, uint64_t input_len, ws_zero_copy** out, uint8_t** mapped,
+                             ws_error_info* err);
+ws_status ws_zero_copy_finish(ws_zero_copy* z, ws_match* out, uint64_t cap, uint64_t* n_out, ws_error_info* err);
+void ws_zero_copy_abort(ws_zero_copy* z);
+
+/* HotSwapPatternSet (core/src/pattern/mod.rs:17-70): a handle whose active
+ * matcher can be replaced while other threads scan through it.
+ * ws_hotswap_create and ws_hotswap_swap take ownership of the matcher they
+ * are given.  ws_hotswap_swap returns 1 when the active matcher changed, 0
+ * when `next` is already active (the reference's swap_arc result), -1 for a
+ * null argument; the matcher it replaces is destroyed once no scan that
+ * started with it is running.  ws_hotswap_scan is ws_scan with the matcher
+ * active when the call starts. */
+typedef struct ws_hotswap ws_hotswap;
+ws_status ws_hotswap_create(ws_matcher* initial, ws_hotswap** out, ws_error_info* err);
+int ws_hotswap_swap(ws_hotswap* h, ws_matcher* next);
+ws_status ws_hotswap_scan(ws_hotswap* h, const uint8_t* data, uint64_t len, ws_match* out, uint64_t cap,
+                          uint64_t* n_out, ws_error_info* err);
+void ws_hotswap_destroy(ws_hotswap* h);
+
 /* Trains the learned boundary-state proposer of the speculative regex walk on
  * a corpus drawn from the same distribution as the inputs to be scanned (host
  * memory, at least 64 KiB; 256 MiB is the intended size).  No counterpart in

@@ -402,3 +402,58 @@ def test_batch_order_ties_on_end_and_ids_spanning_groups():
     m = matcher(pats, batch_mib=1, max_matches=1 << 21)
     got = tagged_rows(ws.scan_batch_gpu(m, [ws.ScanItem(5, d) for d in big]))
     assert got == exp
+
+
+# ------------------------------------------------------ zero copy, hot swap
+def test_zero_copy_session_vs_oracle():
+    # StreamPipeline::scan_zero_copy (core/src/pipeline.rs:31-83): the caller
+    # fills the library's mapped staging buffer, finish() scans it in place
+    ws = _ws()
+    wl = w.regex(size=8 << 20, n=100, seed=41)
+    m = matcher(wl.patterns, max_matches=1 << 20)
+    sp = ws.StreamPipeline(m)
+    for _ in range(2):  # the second session reuses the pooled buffer
+        z = sp.scan_zero_copy(wl.data.size)
+        z.mapped_mut()[:] = wl.data
+        got = z.finish_array()
+        assert np.array_equal(got, oracle.scan_patterns(wl.patterns, wl.data))
+    # a large input takes the windowed copy/scan path
+    big = w.literals_small(size=300 << 20, n=100, seed=42)
+    mb = matcher(big.patterns, max_matches=1 << 22)
+    z = ws.StreamPipeline(mb).scan_zero_copy(big.data.size)
+    z.mapped_mut()[:] = big.data
+    got = z.finish_array()
+    assert np.array_equal(got, oracle.scan_patterns(big.patterns, big.data))
+    with pytest.raises(ValueError):
+        z.mapped_mut()
+
+
+def test_hot_swap_pattern_set():
+    # HotSwapPatternSet (core/src/pattern/mod.rs:17-70)
+    import threading
+    ws = _ws()
+    data = (b"alpha beta gamma " * 4000) + b"needle"
+    a = ws.PatternSet.builder().literal("alpha").regex("b[a-z]+a").build()
+    b = ws.PatternSet.builder().literal("gamma").literal("needle").build()
+    hs = ws.HotSwapPatternSet(a)
+    ra = hs.scan_array(data)
+    assert np.array_equal(ra, oracle.scan_patterns([(0, b"alpha"), (1, b"b[a-z]+a")], data))
+    rb_exp = oracle.scan_patterns([(0, b"gamma"), (0, b"needle")], data)
+    results, stop = [], threading.Event()
+
+    def scanner():
+        while not stop.is_set():
+            results.append(hs.scan_array(data))
+
+    threads = [threading.Thread(target=scanner) for _ in range(3)]
+    for t in threads:
+        t.start()
+    assert hs.swap(b) is True
+    assert hs.swap(b) is False  # already active
+    stop.set()
+    for t in threads:
+        t.join()
+    assert np.array_equal(hs.scan_array(data), rb_exp)
+    for r in results:  # every scan saw one whole pattern set
+        assert np.array_equal(r, ra) or np.array_equal(r, rb_exp)
+    assert hs.swap(a) is True and np.array_equal(hs.scan_array(data), ra)

@@ -36,7 +36,7 @@ __all__ = [
     "MatchBufferOverflow", "PathologicalRegex", "PatternSet", "PatternSetBuilder", "AutoMatcherConfig",
     "GpuMatcher", "WarpStateer", "GpuScanner", "AutoMatcher", "ScanItem", "TaggedMatch", "BatchConfig",
     "scan_batch", "scan_batch_gpu", "scan_batch_auto", "StreamPipeline", "REGEX_SPECULATIVE", "REGEX_PLAIN",
-    "CompiledPatternIndex",
+    "CompiledPatternIndex", "HotSwapPatternSet", "ZeroCopyScan",
 ]
 
 REGEX_SPECULATIVE = 0
@@ -945,6 +945,111 @@ class StreamPipeline:
 
     def scan(self, data) -> list[Match]:
         return [Match(int(p), int(s), int(e)) for p, s, e in self.scan_array(data).tolist()]
+
+
+class ZeroCopyScan:
+    """Two-phase zero-copy scan session (core/src/pipeline.rs:48-83): fill
+    ``mapped_mut()`` (pinned, device-mapped memory the library owns), then
+    ``finish()`` scans it in place."""
+
+    def __init__(self, matcher: "GpuMatcher", input_len: int):
+        self._m = matcher
+        self._len = int(input_len)
+        h, p = ctypes.c_void_p(), ctypes.c_void_p()
+        _call(N.lib().ws_zero_copy_begin, matcher._h, self._len, ctypes.byref(h), ctypes.byref(p))
+        self._h = h
+        self._view = (np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_uint8)), shape=(self._len,))
+                      if self._len else np.empty(0, dtype=np.uint8))
+
+    def mapped_mut(self) -> np.ndarray:
+        """The writable input region (a uint8 view; valid until finish())."""
+        if self._h is None:
+            raise ValueError("session already finished")
+        return self._view
+
+    def finish_array(self) -> np.ndarray:
+        if self._h is None:
+            raise ValueError("session already finished")
+        cap = max(int(self._m.config.c.max_matches), 1)
+        out = np.empty((cap, 3), dtype=np.uint32)
+        cnt = ctypes.c_uint64()
+        h, self._h = self._h, None
+        self._view = None
+        _call(N.lib().ws_zero_copy_finish, h, out.ctypes.data_as(ctypes.POINTER(N.WsMatch)), cap, ctypes.byref(cnt))
+        return out[: cnt.value].copy()
+
+    def finish(self) -> list[Match]:
+        return [Match(int(p), int(s), int(e)) for p, s, e in self.finish_array().tolist()]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                N.lib().ws_zero_copy_abort(h)
+            except Exception:
+                pass
+
+
+def _stream_pipeline_scan_zero_copy(self, input_len: int) -> ZeroCopyScan:
+    """StreamPipeline::scan_zero_copy (core/src/pipeline.rs:31-46)."""
+    return ZeroCopyScan(self.backend, input_len)
+
+
+StreamPipeline.scan_zero_copy = _stream_pipeline_scan_zero_copy
+
+
+class HotSwapPatternSet:
+    """HotSwapPatternSet (core/src/pattern/mod.rs:17-70) on the GPU: the
+    active pattern set's device tables are replaced atomically by ``swap``
+    while other threads scan; each scan uses the set active when it began."""
+
+    def __init__(self, pattern_set: PatternSet, config: AutoMatcherConfig | None = None, device: int = 0):
+        self.config = config or AutoMatcherConfig()
+        self._device = device
+        m = GpuMatcher(pattern_set, self.config, device)
+        h = ctypes.c_void_p()
+        _call(N.lib().ws_hotswap_create, m._h, ctypes.byref(h))
+        m._h = None  # the handle owns the matcher now
+        self._h = h
+        self._active = pattern_set
+
+    @classmethod
+    def new(cls, pattern_set: PatternSet) -> "HotSwapPatternSet":
+        return cls(pattern_set)
+
+    def swap(self, next_set: PatternSet) -> bool:
+        """Makes ``next_set`` active; False when it already is."""
+        if next_set is self._active:
+            return False
+        m = GpuMatcher(next_set, self.config, self._device)
+        r = N.lib().ws_hotswap_swap(self._h, m._h)
+        m._h = None
+        if r < 0:
+            raise ValueError("hot swap failed")
+        self._active = next_set
+        return r == 1
+
+    def scan_array(self, data) -> np.ndarray:
+        ptr, n, keep = _buffer(data)
+        cap = max(int(self.config.c.max_matches), 1)
+        out = np.empty((cap, 3), dtype=np.uint32)
+        cnt = ctypes.c_uint64()
+        _call(N.lib().ws_hotswap_scan, self._h, ptr, n, out.ctypes.data_as(ctypes.POINTER(N.WsMatch)), cap,
+              ctypes.byref(cnt))
+        del keep
+        return out[: cnt.value].copy()
+
+    def scan(self, data) -> list[Match]:
+        return [Match(int(p), int(s), int(e)) for p, s, e in self.scan_array(data).tolist()]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                N.lib().ws_hotswap_destroy(h)
+            except Exception:
+                pass
+            self._h = None
 
 
 class Stream:

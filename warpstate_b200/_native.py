@@ -127,6 +127,17 @@ SIGNATURES = {
     "ws_stream_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatch64), ctypes.c_uint64, c_u64p,
                                      ctypes.POINTER(WsErrorInfo)]),
     "ws_stream_destroy": (None, [ctypes.c_void_p]),
+    "ws_zero_copy_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(WsErrorInfo)]),
+    "ws_zero_copy_finish": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WsMatch), ctypes.c_uint64, c_u64p,
+                                           ctypes.POINTER(WsErrorInfo)]),
+    "ws_zero_copy_abort": (None, [ctypes.c_void_p]),
+    "ws_hotswap_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(WsErrorInfo)]),
+    "ws_hotswap_swap": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "ws_hotswap_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(WsMatch),
+                                       ctypes.c_uint64, c_u64p, ctypes.POINTER(WsErrorInfo)]),
+    "ws_hotswap_destroy": (None, [ctypes.c_void_p]),
     "ws_matcher_train_proposer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                                  ctypes.POINTER(WsErrorInfo)]),
     "ws_matcher_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,

@@ -359,6 +359,7 @@ ws_status ws_matcher_create(ws_ctx* ctx, const ws_pattern_tables* t, const ws_co
 void ws_matcher_destroy(ws_matcher* m) {
   if (!m) return;
   cudaSetDevice(m->ctx->device);
+  release_staging(m);
   delete m;
 }
 

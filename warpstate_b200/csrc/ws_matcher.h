@@ -83,6 +83,8 @@ void sort_tagged_device(Scratch& s, const ws_tagged_match* d_in, ws_tagged_match
                         cudaStream_t st);
 // 64-bit offsets to 32-bit ones (inputs below 4 GiB).
 void narrow_matches_device(const ws_match64* d_in, ws_match* d_out, uint64_t n, cudaStream_t st);
+// Frees the zero-copy staging buffers pooled for a matcher (ws_session.cu).
+void release_staging(const ws_matcher* m);
 // Reads `count` device results into host `out` in (start, pattern_id, end)
 // order, through the scratch's stream; returns when they have arrived.
 void read_sorted(Scratch& s, const ws_match* d_res, uint64_t count, ws_match* out);
