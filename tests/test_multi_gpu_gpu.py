@@ -41,3 +41,23 @@ def test_shards_regex_workload():
     assert len(whole) > 100
     for n in (2, 4):
         assert np.array_equal(mg.sharded_scan_local(m, wl.data, n), whole), n
+
+
+def test_multi_gpu_matcher_concurrent_shards():
+    # MultiGpuMatcher (core/src/multi_gpu.rs:33-160): shards scanned at the
+    # same time from host threads, then the cursor exchange; here every shard
+    # is on device 0 (each thread its own stream), which is how one GPU runs
+    # the multi-device driver without any kernel waiting for another
+    import warpstate_b200 as ws
+    from warpstate_b200 import multi_gpu as mg
+    data = _data()
+    b = ws.PatternSet.builder()
+    for kind, p in PATTERNS:
+        b = b.literal_bytes(p) if kind == 0 else b.regex(p.decode() if isinstance(p, bytes) else p)
+    ps = b.build()
+    whole = oracle.scan_patterns(PATTERNS, data).astype(np.uint64)
+    for n in (1, 2, 4):
+        mm = mg.MultiGpuMatcher(ps, devices=[0] * n)
+        assert mm.device_count() == n
+        assert np.array_equal(mm.scan_array(data), whole), n
+        assert np.array_equal(mm.scan_array(data), whole), n  # scanners are reused

@@ -249,3 +249,96 @@ def run_local_protocol(world: int, n_regex: int, shards: list[ScanShard],
         if not any(redo):
             break
     return [m for m, _ in res]
+
+
+class MultiGpuMatcher:
+    """MultiGpuMatcher (core/src/multi_gpu.rs:33-160) in one process: one
+    matcher per device, the shards of an input scanned at the same time (one
+    host thread per shard, each on its device's own stream), then the cursor
+    exchange of ``resolve_chains`` with the rescans of a round run at once
+    too.  The reference awaits its shards one after another
+    (multi_gpu.rs:142-156) and leaves regex chains near shard boundaries to an
+    overlapped rescan; here the result equals one scan of the whole input.
+    ``devices`` may repeat an index (several shards on one GPU)."""
+
+    def __init__(self, patterns, devices: Sequence[int] | None = None, config=None):
+        import torch
+        from . import GpuMatcher
+        if devices is None:
+            devices = list(range(torch.cuda.device_count()))
+        if not devices:
+            from . import NoGpuAdapter
+            raise NoGpuAdapter("no CUDA device")
+        self.devices = list(devices)
+        self.matchers = {}
+        for d in sorted(set(self.devices)):
+            with torch.cuda.device(d):
+                self.matchers[d] = GpuMatcher(patterns, config, device=d)
+        self._scanners = {}
+
+    def device_count(self) -> int:
+        return len(self.devices)
+
+    def _scanner(self, k: int) -> ShardScanner:
+        import torch
+        if k not in self._scanners:
+            d = self.devices[k]
+            with torch.cuda.device(d):
+                self._scanners[k] = ShardScanner(self.matchers[d])
+        return self._scanners[k]
+
+    def scan_array(self, data) -> np.ndarray:
+        """(n, 3) uint64 (pattern_id, start, end), sorted by (start, pattern_id, end)."""
+        import torch
+        from concurrent.futures import ThreadPoolExecutor
+        from . import _buffer
+        ptr, n, keep = _buffer(data)
+        host = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint8)), shape=(n,)) if n else \
+            np.zeros(0, np.uint8)
+        world = len(self.devices)
+        scanners = [self._scanner(k) for k in range(world)]
+        shards = build_scan_shards(n, world, scanners[0].halo(n))
+        bufs = {}
+
+        def upload(r):
+            with torch.cuda.device(self.devices[r]):
+                bufs[r] = torch.from_numpy(np.ascontiguousarray(host[shards[r].start:shards[r].scan_end])).to(
+                    scanners[r].dev)
+
+        def scan(r, cursor):
+            with torch.cuda.device(self.devices[r]):
+                return scanners[r].scan(bufs[r], shards[r], cursor)
+
+        with ThreadPoolExecutor(max_workers=max(len(shards), 1)) as ex:
+            list(ex.map(upload, range(len(shards))))
+            results = run_parallel_protocol(len(shards), scanners[0].n_regex if shards else 0, shards, scan, ex)
+        del keep
+        return _sort(np.concatenate(results)) if results else np.zeros((0, 3), np.uint64)
+
+    def scan(self, data):
+        from . import Match
+        return [Match(int(p), int(s), int(e)) for p, s, e in self.scan_array(data).tolist()]
+
+
+def run_parallel_protocol(world: int, n_regex: int, shards: list[ScanShard],
+                          scan: Callable[[int, np.ndarray], "tuple[np.ndarray, np.ndarray]"], executor) -> list[np.ndarray]:
+    """``run_local_protocol`` with the scans of each round submitted to
+    ``executor`` together (they touch disjoint shards and devices' streams)."""
+    base = [s.start for s in shards]
+    cur_in = [np.full(n_regex, b, dtype=np.uint64) for b in base]
+    res = list(executor.map(lambda r: scan(r, cur_in[r]), range(world)))
+    for _ in range(world):
+        outs = [res[r][1] for r in range(world)]
+        redo = []
+        for r in range(1, world):
+            if not n_regex:
+                break
+            want = np.maximum(outs[r - 1], np.uint64(base[r]))
+            if not np.array_equal(want, cur_in[r]):
+                cur_in[r] = want
+                redo.append(r)
+        if not redo:
+            break
+        for r, out in zip(redo, executor.map(lambda r: scan(r, cur_in[r]), redo)):
+            res[r] = out
+    return [m for m, _ in res]
