@@ -275,7 +275,11 @@ ws_status ws_scan_device64(ws_matcher* m, const uint8_t* d_data, uint64_t len,
  * stream offsets; pass base when nothing before the shard reaches into it) and
  * decides every match starting before own_end, after which d_cursor[r] holds
  * max(end of its last match, own_end): the next shard's incoming cursor.
- * Offsets in d_out are stream offsets.  Asynchronous on `stream`. */
+ * Offsets in d_out are stream offsets.  Asynchronous on `stream`.
+ * Look-behind assertions (^ \b \B \A) at d_data[0] read it as the start of
+ * the input: for a pattern set with such regexes (ws_matcher_info.
+ * regex_context), give a shard after the first one byte before its own range
+ * (base one lower) and drop the literal matches that start at that byte. */
 ws_status ws_scan_shard(ws_matcher* m, const uint8_t* d_data, uint64_t len, uint64_t base,
                         uint64_t own_end, uint64_t* d_cursor, ws_match64* d_out, uint64_t cap,
                         uint64_t* d_count, void* stream, ws_error_info* err);
@@ -379,6 +383,8 @@ typedef struct {
   uint64_t last_rewalk_bytes;    /* bytes re-walked by the fix-up (over all groups) */
   uint64_t last_guess_hits;      /* chunk boundaries whose guessed start state was the true one */
   uint64_t last_guesses;         /* chunk boundaries guessed (chunks - 1, per group) */
+  uint32_t regex_context;        /* 1 when some regex has a look-around assertion */
+  uint32_t n_context_groups;     /* DFA groups of such regexes (walked per start position) */
 } ws_matcher_info;
 ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
 

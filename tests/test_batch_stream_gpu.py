@@ -457,3 +457,32 @@ def test_hot_swap_pattern_set():
     for r in results:  # every scan saw one whole pattern set
         assert np.array_equal(r, ra) or np.array_equal(r, rb_exp)
     assert hs.swap(a) is True and np.array_equal(hs.scan_array(data), ra)
+
+
+def test_look_around_batch_stream_and_shards():
+    # item starts and ends are input starts and ends for ^ $ \A \z \b; stream
+    # pieces and shards keep the byte before a start and after a match end
+    ws = _ws()
+    from warpstate_b200 import multi_gpu as mg
+    rng = np.random.default_rng(9)
+    alpha = np.frombuffer(b"ab cx,fo\n_!y0123", dtype=np.uint8)
+    data = alpha[rng.integers(0, alpha.size, 300_000)].tobytes()
+    pats = [(1, b"^abc"), (1, b"abc$"), (1, b"\\bfoo\\b"), (1, b"\\Aab"), (1, b"ab\\z"), (1, b"x\\B"),
+            (1, b"\\b[0-9]+\\b"), (0, b"fo")]
+    m = matcher(pats, max_matches=1 << 20)
+    items, off = [], 0
+    while off < len(data):
+        n = int(rng.integers(1, 700))
+        items.append((off, min(n, len(data) - off)))
+        off += n
+    lens = np.array([n for _, n in items], dtype=np.uint64)
+    got = ws.scan_batch_packed(m, np.frombuffer(data, dtype=np.uint8), lens)
+    exp = oracle.batch_scan(pats, np.frombuffer(data, dtype=np.uint8), items)
+    assert len(exp) > 500 and np.array_equal(got, exp)
+    whole = oracle.scan_patterns(pats, data)
+    for block in (1, 777, 65536):
+        sp = ws.StreamPipeline(m).scan_array(data[:50_000] if block == 1 else data, block=block)
+        ref = whole if block != 1 else oracle.scan_patterns(pats, data[:50_000])
+        assert np.array_equal(sp.astype(np.uint32), ref), block
+    for n in (2, 3):
+        assert np.array_equal(mg.sharded_scan_local(m, data, n), whole.astype(np.uint64)), n

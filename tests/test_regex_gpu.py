@@ -59,14 +59,14 @@ def _outside_classes(pattern: str) -> str:
 
 
 def supported(pattern: str) -> bool:
-    r = oracle.Regex(pattern)
-    bare = _outside_classes(pattern)
-    return not r.nullable and not any(a in bare for a in ("^", "$", "\\b", "\\B", "\\A", "\\z"))
+    """Every regex except those that can match the empty string."""
+    return not oracle.Regex(pattern).nullable
 
 
-def test_negated_classes_are_run():
-    # [^a-z] style goldens are not look-around: they must reach the GPU
-    assert supported("[^a-z]+") and supported("x[^\\]]y") and not supported("^abc")
+def test_goldens_with_assertions_and_negated_classes_are_run(golden):
+    pats = [c["pattern"] for c in golden["regex_find_iter"]]
+    assert any("[^" in p for p in pats if supported(p))
+    assert any(a in _outside_classes(p) for p in pats if supported(p) for a in ("^", "$", "\\b"))
 
 
 def test_golden_regex_cases(golden):
@@ -170,8 +170,9 @@ def test_leftmost_first_semantics_on_gpu():
 
 
 def test_unsupported_regexes_fail_loudly():
+    # patterns that can match the empty string (the rest of the syntax runs)
     ws = _ws()
-    for pat in ["^abc", "abc$", "\\bword", "a*", "a|"]:
+    for pat in ["a*", "a|", "^", "\\b", "(?:ab)?"]:
         with pytest.raises(ws.PatternCompilationFailed):
             matcher([(1, pat.encode())])
 
@@ -260,3 +261,38 @@ def test_nucleotide_config_scaled_vs_oracle(mode):
     rx_ids = {i for i, (k, _) in enumerate(wl.patterns) if k == 1}
     assert sum(1 for p in exp[:, 0].tolist() if p in rx_ids) >= 20  # regex matches are part of the check
     assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
+# ------------------------------------------------------------ look-around
+LOOK_PATTERNS = [r"^abc", r"abc$", r"\bfoo\b", r"\Bx", r"^\w+$", r"\Aab", r"ab\z", r"a\b.", r"\b[0-9]+\b",
+                 r"(?:^|,)ab", r"ab(?:$|,)", r"x\B", r"\w+\b!", r"\Bab\B", r"^[a-z]+ [a-z]+$"]
+
+
+def _look_data(n, seed):
+    rng = np.random.default_rng(seed)
+    alpha = np.frombuffer(b"ab cx,fo\n_!y0123", dtype=np.uint8)
+    return alpha[rng.integers(0, alpha.size, n)].tobytes()
+
+
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+def test_look_around_vs_oracle(mode):
+    # ^ $ (multi-line), \b \B (ASCII), \A \z: context groups walked per start
+    data = _look_data(1 << 18, 8)
+    pats = [(1, p.encode()) for p in LOOK_PATTERNS] + [(1, b"fo[a-z]+"), (0, b"abc")]
+    m = matcher(pats, mode=mode, max_matches=1 << 20)
+    assert m.info()["regex_context"] == 1
+    got = m.scan_array(data)
+    exp = oracle.scan_patterns(pats, data)
+    assert len(exp) > 1000
+    assert np.array_equal(got, exp)
+
+
+def test_look_around_candidates_and_anchors_at_ends():
+    data = b"abc\nabc abc\n foo foo\nab"
+    pats = [(1, b"^abc"), (1, b"abc$"), (1, b"\\bfoo\\b"), (1, b"ab\\z"), (1, b"\\Aab")]
+    m = matcher(pats)
+    exp = oracle.scan_patterns(pats, data)
+    assert np.array_equal(m.scan_array(data), exp)
+    a = oracle.sort_matches(m.regex_candidates(data, PLAIN))
+    b = oracle.sort_matches(m.regex_candidates(data, SPEC))
+    assert np.array_equal(a, b)

@@ -70,7 +70,7 @@ RxLayout layout(const RegexPlan& p, uint64_t len, uint32_t chunk, uint64_t max_m
   L.chunk = chunk;
   L.n_chunks = (len + chunk - 1) / chunk;
   L.nck = chunk / kCkpt;
-  L.n_q = L.n_chunks * p.n_groups;
+  L.n_q = L.n_chunks * p.n_spec;
   const uint64_t base = std::max<uint64_t>(2 * max_matches, len / 256 + 65536);
   L.k_cap = std::min(kMaxCandidates, std::max(base, k_min));
   L.ev_cap = std::min(kMaxCandidates, std::max(base, ev_min));
@@ -108,8 +108,9 @@ struct DevTables {
   const uint32_t* rmptr;
   const uint32_t* rmlist;
   const uint4* lfinfo;   // per regex: {lf_off, lf_start row, group, classes}
+  const uint32_t* lfx;   // per regex: context DFA starts and end-step flags (8 words)
   const uint32_t* pid;
-  uint32_t n_groups, n_regex;
+  uint32_t n_groups, n_regex, n_spec;
 };
 
 struct ScanPtrs {
@@ -358,6 +359,66 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_plain_kernel(DevTables t,
       }
       if (!alive) break;
     }
+  }
+}
+
+// --------------------------------------------------------- context groups
+// Context of a byte for the assertions (byte_context in ws_regex.h).
+__device__ __forceinline__ uint32_t ctx_of(uint32_t b) {
+  if (b == '\n') return CTX_NL;
+  const bool w = (b - '0' < 10u) || ((b | 0x20u) - 'a' < 26u) || b == '_';
+  return w ? CTX_WORD : CTX_OTHER;
+}
+
+// Context groups: one thread per start position, the anchored walk of the
+// group's context DFA (build_context_all_dfa): the start row chosen by the
+// byte before the start (CTX_BEGIN at the start of the input or item), the
+// transition on the byte at e reporting the patterns whose match ends at e,
+// and after the last byte the end step (right context CTX_BEGIN) at the end
+// of the input or item.  Walks of starts whose match cannot end by then stop
+// at the buffer's end like the others; a caller decides only starts whose
+// walks die before it (streams, shards).  blockIdx.y = context group.  The
+// tables are read through L1/L2: these groups hold the patterns with
+// assertions, whose anchored walks mostly die within a few bytes.
+__global__ void __launch_bounds__(256) dfa_context_kernel(DevTables t, ScanPtrs p) {
+  __shared__ uint8_t cls_s[256];
+  const uint32_t g = t.n_spec + blockIdx.y;
+  const GroupDev gd = t.groups[g];
+  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) cls_s[k] = t.cls[g * 256 + k];
+  __syncthreads();
+  const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint32_t* mp = t.mptr + gd.mptr_off;
+  const uint32_t C = gd.n_classes;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < p.len; s += stride) {
+    const uint64_t lo = p.n_items ? item_start_of(p.item_end, p.n_items, (uint32_t)s) : 0;
+    const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, (uint32_t)s)) : p.len;
+    uint32_t st = gd.cstart[s == lo ? CTX_BEGIN : ctx_of(__ldg(p.data + s - 1))];
+    // a candidate is (regex, start); a list reported earlier on this walk
+    // adds nothing (the last four are kept)
+    uint32_t seen0 = 0xFFFFFFFFu, seen1 = 0xFFFFFFFFu, seen2 = 0xFFFFFFFFu, seen3 = 0xFFFFFFFFu;
+    auto report = [&](uint32_t slot, uint64_t e) {
+      const uint32_t a = __ldg(mp + slot), b = __ldg(mp + slot + 1);
+      if (a == b) return;
+      if (!p.full_k && (a == seen0 || a == seen1 || a == seen2 || a == seen3)) return;
+      for (uint32_t j = a; j < b; ++j) emit_k(p, __ldg(t.mlist + j), (uint32_t)s, (uint32_t)e);
+      seen3 = seen2;
+      seen2 = seen1;
+      seen1 = seen0;
+      seen0 = a;
+    };
+    bool alive = true;
+    for (uint64_t e = s; e < stop; ++e) {
+      const uint32_t b = __ldg(p.data + e);
+      const uint32_t w = __ldg(tab + st * C + cls_s[b]);
+      if (w & F_MATCH) report(st * 4 + ctx_of(b), e);
+      if (w & F_DEAD) {
+        alive = false;
+        break;
+      }
+      st = w & F_MASK;
+    }
+    if (alive) report(st * 4 + CTX_BEGIN, stop);
   }
 }
 
@@ -712,6 +773,23 @@ __device__ uint32_t lf_walk(const DevTables& t, const ScanPtrs& p, uint32_t r, u
   uint32_t st = info.y;
   int64_t last = -1;
   const uint64_t stop = p.n_items ? min(p.len, (uint64_t)item_end_of(p.item_end, p.n_items, s)) : p.len;
+  const uint32_t* x = t.lfx + 8 * (size_t)r;
+  if (__ldg(x)) {
+    // context DFA (build_context_lf_dfa): start row by the byte before s, a
+    // match flag on the byte at pos ends a match at pos, the end step after
+    // the last byte of the input or item
+    const uint64_t lo = p.n_items ? item_start_of(p.item_end, p.n_items, s) : 0;
+    st = __ldg(x + 1 + (s == lo ? CTX_BEGIN : ctx_of(__ldg(p.data + s - 1))));
+    for (uint64_t pos = s; pos < stop; ++pos) {
+      if (pos - s == cap) return kLfLong;
+      const uint32_t w = __ldg(tab + st * info.w + __ldg(cm + __ldg(p.data + pos)));
+      if (w & F_MATCH) last = (int64_t)pos;
+      if (w & F_DEAD) return last < 0 ? kLfNone : (uint32_t)last;
+      st = w & F_MASK;
+    }
+    if (__ldg(t.lf + __ldg(x + 5) + st)) last = (int64_t)stop;
+    return last < 0 ? kLfNone : (uint32_t)last;
+  }
   for (uint64_t pos = s; pos < stop; ++pos) {
     if (pos - s == cap) return kLfLong;
     uint32_t w = __ldg(tab + st * info.w + __ldg(cm + __ldg(p.data + pos)));
@@ -865,9 +943,11 @@ DevTables dev_tables(const RegexPlan& P) {
   t.rmptr = P.d_rmptr.as<uint32_t>();
   t.rmlist = P.d_rmlist.as<uint32_t>();
   t.lfinfo = P.d_lfinfo.as<uint4>();
+  t.lfx = P.d_lfx.as<uint32_t>();
   t.pid = P.d_pid.as<uint32_t>();
   t.n_groups = P.n_groups;
   t.n_regex = P.n_regex;
+  t.n_spec = P.n_spec;
   return t;
 }
 
@@ -888,26 +968,48 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
                           int sm_count, cudaEvent_t* ev) {
   uint32_t launches = 0;
   auto mark = [&](int k) { if (ev) check_cuda(cudaEventRecord(ev[k], st), "event"); };
-  if (mode == WS_REGEX_PLAIN) {
-    size_t smem = hot_smem_bytes(max_rows(P, true));
-    set_smem(dfa_plain_kernel, smem, "smem(plain)");
-    uint64_t per_group = std::max<uint64_t>(1, (uint64_t)sm_count / P.n_groups);
-    uint64_t want = (p.len + kWalkThreads - 1) / kWalkThreads;
-    dim3 grid((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, per_group * 2)), P.n_groups);
-    mark(1);
-    dfa_plain_kernel<<<grid, kWalkThreads, smem, st>>>(t, p);
-    check_cuda(cudaGetLastError(), "dfa_plain_kernel");
+  // context groups: one anchored walk per start in either mode
+  auto context_groups = [&]() {
+    const uint32_t nc = P.n_groups - P.n_spec;
+    if (!nc) return;
+    const uint64_t want = (p.len + 255) / 256;
+    const uint64_t per_group = std::max<uint64_t>(1, (uint64_t)sm_count * 8 / nc);
+    dim3 grid((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, per_group)), nc);
+    dfa_context_kernel<<<grid, 256, 0, st>>>(t, p);
+    check_cuda(cudaGetLastError(), "dfa_context_kernel");
     launches++;
+  };
+  if (mode == WS_REGEX_PLAIN) {
+    mark(1);
+    if (P.n_spec) {
+      size_t smem = hot_smem_bytes(max_rows(P, true));
+      set_smem(dfa_plain_kernel, smem, "smem(plain)");
+      uint64_t per_group = std::max<uint64_t>(1, (uint64_t)sm_count / P.n_spec);
+      uint64_t want = (p.len + kWalkThreads - 1) / kWalkThreads;
+      dim3 grid((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, per_group * 2)), P.n_spec);
+      dfa_plain_kernel<<<grid, kWalkThreads, smem, st>>>(t, p);
+      check_cuda(cudaGetLastError(), "dfa_plain_kernel");
+      launches++;
+    }
+    context_groups();
     mark(2);
     mark(3);
     mark(4);
     return launches;
   }
-  dim3 cgrid(P.n_groups, (unsigned)((p.n_chunks + kWalkThreads - 1) / kWalkThreads));
+  if (!P.n_spec) {
+    mark(1);
+    context_groups();
+    mark(2);
+    mark(3);
+    mark(4);
+    return launches;
+  }
+  dim3 cgrid(P.n_spec, (unsigned)((p.n_chunks + kWalkThreads - 1) / kWalkThreads));
   if (P.proposer && P.use_proposer) {
     launches += proposer_predict(*P.proposer, p.data, p.len, p.chunk, p.n_chunks, p.guess, st);
   } else {
-    fill_guess_kernel<<<dim3(std::min<unsigned>((unsigned)((p.n_chunks + 255) / 256), 1024), P.n_groups), 256, 0, st>>>(t, p);
+    fill_guess_kernel<<<dim3(std::min<unsigned>((unsigned)((p.n_chunks + 255) / 256), 1024), P.n_spec), 256, 0, st>>>(t, p);
     check_cuda(cudaGetLastError(), "fill_guess_kernel");
     launches++;
   }
@@ -926,19 +1028,20 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
   check_cuda(cudaGetLastError(), "dfa_walk_kernel");
   launches++;
   mark(2);
-  dim3 fgrid((unsigned)((p.n_chunks + 255) / 256), P.n_groups);
+  dim3 fgrid((unsigned)((p.n_chunks + 255) / 256), P.n_spec);
   for (int r = 0; r < kFixRounds; ++r) {
     dfa_fixup_kernel<<<fgrid, 256, 0, st>>>(t, p, r);
     check_cuda(cudaGetLastError(), "dfa_fixup_kernel");
     launches++;
   }
-  dfa_fixup_serial_kernel<<<P.n_groups, 1, 0, st>>>(t, p);
+  dfa_fixup_serial_kernel<<<P.n_spec, 1, 0, st>>>(t, p);
   check_cuda(cudaGetLastError(), "dfa_fixup_serial_kernel");
   launches++;
   mark(3);
   dfa_reverse_kernel<<<sm_count * 8, 256, 0, st>>>(t, p);
   check_cuda(cudaGetLastError(), "dfa_reverse_kernel");
   launches++;
+  context_groups();
   mark(4);
   return launches;
 }
@@ -956,6 +1059,7 @@ struct GroupBuild {
   Dfa fwd, rev;
   std::vector<Dfa> lf;
   uint32_t n_hot_u = 0, n_hot_a = 0;
+  bool context = false;  // a context group (patterns with look-around assertions)
 };
 
 // Byte distribution assumed when ranking states: text-like input (printable
@@ -1056,6 +1160,33 @@ bool try_group(const std::vector<ReTree>& trees, const std::vector<uint32_t>& me
   return true;
 }
 
+// A group of patterns with look-around assertions: the context DFA of the
+// group and a context leftmost-first DFA per pattern; no unanchored walk, no
+// reverse DFA, no hot rows.
+bool try_context_group(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
+                       GroupBuild& out) {
+  std::vector<const ReTree*> tp;
+  for (uint32_t r : members) tp.push_back(&trees[r]);
+  Nfa fn = build_nfa(tp, false);
+  ByteClasses bc = compute_classes({&fn});
+  Dfa fwd = build_context_all_dfa(fn, bc, max_states);
+  if (fwd.too_big) return false;
+  out.regexes = members;
+  out.cls = bc;
+  out.fwd = std::move(fwd);
+  out.rev = Dfa();
+  out.context = true;
+  out.n_hot_u = out.n_hot_a = 0;
+  out.lf.clear();
+  for (uint32_t r : members) {
+    Nfa one = build_nfa({&trees[r]}, false);
+    Dfa lf = build_context_lf_dfa(one, bc, 1 << 20);
+    if (lf.too_big) throw CompileError("leftmost-first DFA too large for regex " + std::to_string(r));
+    out.lf.push_back(std::move(lf));
+  }
+  return true;
+}
+
 uint32_t append_trans(const Dfa& d, std::vector<uint32_t>& dst) {
   size_t base = dst.size();
   dst.insert(dst.end(), d.trans.begin(), d.trans.end());
@@ -1099,18 +1230,22 @@ void layout_forward(RegexPlan& P) {
         }
       return off;
     };
-    gd.hot_rows = fits ? P.nhot_u[g] : 0;
+    const bool spec = g < P.n_spec;
+    gd.hot_rows = fits && spec ? P.nhot_u[g] : 0;
     gd.hot_off = image(0, gd.hot_rows);
     gd.ahot_base = P.nhot_u[g];
-    gd.ahot_rows = fits ? P.nhot_a[g] : 0;
+    gd.ahot_rows = fits && spec ? P.nhot_a[g] : 0;
     gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows);
     gd.mptr_off = (uint32_t)P.mptr.size();
-    for (int s = 0; s < d.n_states; ++s) {
+    // one list per state, or per (state, right context) in a context group
+    const size_t n_lists = d.match_ptr.size() - 1;
+    for (size_t s = 0; s < n_lists; ++s) {
       P.mptr.push_back((uint32_t)P.mlist.size());
-      for (uint32_t j = d.match_ptr[(size_t)s]; j < d.match_ptr[(size_t)s + 1]; ++j)
-        P.mlist.push_back(P.gregex[g][d.match_list[j]]);
+      for (uint32_t j = d.match_ptr[s]; j < d.match_ptr[s + 1]; ++j) P.mlist.push_back(P.gregex[g][d.match_list[j]]);
     }
     P.mptr.push_back((uint32_t)P.mlist.size());
+    gd.context = g >= P.n_spec ? 1u : 0u;
+    for (int k = 0; k < 4; ++k) gd.cstart[k] = d.ctx_start[k];
     P.total_states += gd.n_states;
     P.max_classes = std::max(P.max_classes, C);
   }
@@ -1123,9 +1258,9 @@ void layout_forward(RegexPlan& P) {
 }
 
 void build_groups(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
-                  std::vector<GroupBuild>& out) {
+                  std::vector<GroupBuild>& out, bool context) {
   GroupBuild gb;
-  if (try_group(trees, members, max_states, gb)) {
+  if (context ? try_context_group(trees, members, max_states, gb) : try_group(trees, members, max_states, gb)) {
     out.push_back(std::move(gb));
     return;
   }
@@ -1133,8 +1268,8 @@ void build_groups(const std::vector<ReTree>& trees, const std::vector<uint32_t>&
     raise(WS_ERR_COMPILE, "regex " + std::to_string(members[0]) + " needs more than " +
                               std::to_string(max_states) + " DFA states (raise dfa_max_states)");
   size_t h = members.size() / 2;
-  build_groups(trees, std::vector<uint32_t>(members.begin(), members.begin() + h), max_states, out);
-  build_groups(trees, std::vector<uint32_t>(members.begin() + h, members.end()), max_states, out);
+  build_groups(trees, std::vector<uint32_t>(members.begin(), members.begin() + h), max_states, out, context);
+  build_groups(trees, std::vector<uint32_t>(members.begin() + h, members.end()), max_states, out, context);
 }
 
 }  // namespace
@@ -1153,15 +1288,14 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
       raise(WS_ERR_COMPILE, "invalid regex at index " + std::to_string(t.regex_pattern_ids[r]) + ": " + e.what(),
             t.regex_pattern_ids[r]);
     }
-    if (tree_has_look(trees[r]))
-      raise(WS_ERR_COMPILE, "regex " + std::to_string(t.regex_pattern_ids[r]) +
-                                " uses a look-around assertion (^ $ \\b \\B \\A \\z), which the GPU DFA path does not support",
-            t.regex_pattern_ids[r]);
     if (tree_nullable(trees[r]))
       raise(WS_ERR_COMPILE, "regex " + std::to_string(t.regex_pattern_ids[r]) +
                                 " can match the empty string, which the GPU DFA path does not support",
             t.regex_pattern_ids[r]);
+    // a look-ahead assertion reads the byte after the match: one more byte
+    // of reach for the stream and shard bookkeeping
     int64_t ml = tree_max_len(trees[r]);
+    if (ml >= 0 && tree_has_look(trees[r])) ml += 1;
     if (ml < 0 || P.max_len < 0) P.max_len = -1;
     else P.max_len = std::max(P.max_len, ml);
   }
@@ -1170,25 +1304,34 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
   // Greedy packing by the size of each regex's own unanchored DFA, then exact
   // verification of every group (halved while it exceeds the budget).
   std::vector<int> est(t.n_regex);
+  std::vector<uint8_t> ctx(t.n_regex, 0);
   for (uint32_t r = 0; r < t.n_regex; ++r) {
+    ctx[r] = tree_has_look(trees[r]) ? 1 : 0;
     Nfa n = build_nfa({&trees[r]}, false);
     ByteClasses bc = compute_classes({&n});
-    Dfa d = build_all_dfa(n, bc, true, max_states);
+    Dfa d = ctx[r] ? build_context_all_dfa(n, bc, max_states) : build_all_dfa(n, bc, true, max_states);
     if (d.too_big)
       raise(WS_ERR_COMPILE, "regex " + std::to_string(t.regex_pattern_ids[r]) + " needs more than " +
                                 std::to_string(max_states) + " DFA states (raise dfa_max_states)",
             t.regex_pattern_ids[r]);
     est[r] = d.n_states;
   }
-  std::vector<std::vector<uint32_t>> packs(1);
-  int sum = 0;
-  for (uint32_t r = 0; r < t.n_regex; ++r) {
-    if (!packs.back().empty() && 4 * (sum + est[r]) > 3 * max_states) { packs.emplace_back(); sum = 0; }
-    packs.back().push_back(r);
-    sum += est[r];
-  }
+  // speculative groups first, then the context groups
   std::vector<GroupBuild> gbs;
-  for (auto& pk : packs) build_groups(trees, pk, max_states, gbs);
+  for (int want_ctx = 0; want_ctx < 2; ++want_ctx) {
+    std::vector<std::vector<uint32_t>> packs(1);
+    int sum = 0;
+    for (uint32_t r = 0; r < t.n_regex; ++r) {
+      if (ctx[r] != want_ctx) continue;
+      if (!packs.back().empty() && 4 * (sum + est[r]) > 3 * max_states) { packs.emplace_back(); sum = 0; }
+      packs.back().push_back(r);
+      sum += est[r];
+    }
+    for (auto& pk : packs)
+      if (!pk.empty()) build_groups(trees, pk, max_states, gbs, want_ctx != 0);
+    if (!want_ctx) P.n_spec = (uint32_t)gbs.size();
+  }
+  P.has_context = P.n_spec < gbs.size();
 
   // device layout: reverse and leftmost-first tables, then the forward layout
   P.n_groups = (uint32_t)gbs.size();
@@ -1197,6 +1340,7 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
   P.rev.clear(); P.lf.clear(); P.rmptr.clear(); P.rmlist.clear(); P.cls.clear();
   P.fdfa.clear(); P.fcls.clear(); P.gregex.clear(); P.nhot_u.clear(); P.nhot_a.clear();
   P.lfinfo.assign(4 * (size_t)t.n_regex, 0);
+  P.lfx.assign(8 * (size_t)t.n_regex, 0);
   P.pid.assign(t.regex_pattern_ids, t.regex_pattern_ids + t.n_regex);
   P.regex_group.assign(t.n_regex, 0);
   for (uint32_t g = 0; g < P.n_groups; ++g) {
@@ -1223,6 +1367,12 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
       P.lfinfo[4 * r + 2] = g;
       P.lfinfo[4 * r + 3] = C;
       P.regex_group[r] = g;
+      if (gb.context) {  // start rows per left context, end-step flags after the table
+        P.lfx[8 * r + 0] = 1;
+        for (int k = 0; k < 4; ++k) P.lfx[8 * r + 1 + k] = lf.ctx_start[k];
+        P.lfx[8 * r + 5] = (uint32_t)P.lf.size();
+        for (int s = 0; s < lf.n_states; ++s) P.lf.push_back(lf.is_match[(size_t)s]);
+      }
     }
     P.fdfa.push_back(std::move(gb.fwd));
     P.fcls.push_back(gb.cls);
@@ -1237,6 +1387,7 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
   P.d_rmptr.upload(P.rmptr.data(), P.rmptr.size() * 4);
   P.d_rmlist.upload(P.rmlist.data(), std::max<size_t>(P.rmlist.size(), 1) * 4);
   P.d_lfinfo.upload(P.lfinfo.data(), P.lfinfo.size() * 4);
+  P.d_lfx.upload(P.lfx.data(), P.lfx.size() * 4);
   P.d_pid.upload(P.pid.data(), P.pid.size() * 4);
   P.use_proposer = cfg.proposer == WS_PROPOSER_MLP;
 }
@@ -1270,7 +1421,7 @@ __global__ void visit_hist_kernel(const uint32_t* tab, uint32_t C, uint32_t star
 void regex_rerank_from_corpus(RegexPlan& P, const uint8_t* d_corpus, uint64_t len) {
   if (!P.n_regex) return;
   const uint64_t use = std::min<uint64_t>(len, 64ull << 20);
-  for (uint32_t g = 0; g < P.n_groups; ++g) {
+  for (uint32_t g = 0; g < P.n_spec; ++g) {
     Dfa& d = P.fdfa[g];
     const uint32_t n = (uint32_t)d.n_states, C = (uint32_t)d.n_classes;
     if (n > (1u << 14)) continue;  // L2-only group: nothing to place
@@ -1324,6 +1475,8 @@ void regex_rerank_from_corpus(RegexPlan& P, const uint8_t* d_corpus, uint64_t le
 
 void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
   info.n_groups = P.n_groups;
+  info.regex_context = P.has_context ? 1 : 0;
+  info.n_context_groups = P.n_groups - P.n_spec;
   info.total_states = P.total_states;
   info.max_classes = P.max_classes;
   info.proposer_top1 = P.top1;
@@ -1381,8 +1534,8 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   if (ev) {
     // profiled scans also count the boundary guesses that held and read the
     // counters back for ws_matcher_get_info
-    if (l.mode != WS_REGEX_PLAIN && L.n_chunks > 1) {
-      dim3 hg2((unsigned)std::min<uint64_t>((L.n_chunks + 255) / 256, 1024), P.n_groups);
+    if (l.mode != WS_REGEX_PLAIN && L.n_chunks > 1 && P.n_spec) {
+      dim3 hg2((unsigned)std::min<uint64_t>((L.n_chunks + 255) / 256, 1024), P.n_spec);
       guess_hits_kernel<<<hg2, 256, 0, st>>>(t, p);
       check_cuda(cudaGetLastError(), "guess_hits_kernel");
       launches += 1;

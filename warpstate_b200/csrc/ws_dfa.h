@@ -41,7 +41,11 @@ struct GroupDev {
   uint32_t mptr_off, rmptr_off, cls_off;
   uint32_t hot_off, hot_rows;                 // unanchored hot rows [0, hot_rows), byte-indexed
   uint32_t ahot_off, ahot_base, ahot_rows;    // anchored hot rows [ahot_base, +ahot_rows)
-  uint32_t pad;
+  // Context groups (patterns with look-around assertions): the forward table
+  // is a context DFA (build_context_all_dfa) with a start row per left
+  // context, and match lists per (row, right context) at mptr[4 * row + k].
+  uint32_t context;
+  uint32_t cstart[4];
 };
 
 struct Proposer;
@@ -53,6 +57,11 @@ struct ProposerDeleter {
 struct RegexPlan {
   uint32_t n_regex = 0;
   uint32_t n_groups = 0;
+  // Groups [0, n_spec) take the speculative walk (or the plain kernel);
+  // groups [n_spec, n_groups) are context groups, walked one anchored walk
+  // per start position in both modes.
+  uint32_t n_spec = 0;
+  bool has_context = false;              // some regex has a look-around assertion
   uint32_t total_states = 0;
   uint32_t max_classes = 0;
   int64_t max_len = 0;                   // longest match (-1 unbounded)
@@ -60,9 +69,14 @@ struct RegexPlan {
   std::vector<GroupDev> groups;
   std::vector<uint32_t> regex_group;     // regex index -> group
   // device tables
-  DeviceBuffer d_groups, d_fwd, d_hot, d_rev, d_lf, d_cls, d_mptr, d_mlist, d_rmptr, d_rmlist, d_lfinfo, d_pid;
+  DeviceBuffer d_groups, d_fwd, d_hot, d_rev, d_lf, d_cls, d_mptr, d_mlist, d_rmptr, d_rmlist, d_lfinfo, d_pid,
+      d_lfx;
   // host copies
   std::vector<uint32_t> fwd, rev, lf, mptr, mlist, rmptr, rmlist, lfinfo, pid;
+  // per regex, 8 words: {context, start row per left context (4), offset in
+  // `lf` of the end-step flags, 0, 0}; context 0 for regexes without
+  // assertions
+  std::vector<uint32_t> lfx;
   std::vector<uint32_t> hot;   // shared-memory images, one per (group, part)
   std::vector<uint8_t> cls;
   // host forward DFAs per group (their numbering defines the layout above)

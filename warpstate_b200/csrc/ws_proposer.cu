@@ -485,9 +485,9 @@ unsigned blocks(uint64_t n, unsigned t = 256) { return (unsigned)((n + t - 1) / 
 void proposer_train(RegexPlan& P, const uint8_t* d_corpus, uint64_t len, uint64_t seed, int sm_count,
                     ProposerStats* stats) {
   (void)sm_count;
-  if (!P.n_regex || P.n_groups == 0) return;
+  if (!P.n_regex || P.n_spec == 0) return;  // context groups take no boundary guesses
   if (len < 65536) raise(WS_ERR_INVALID_ARGUMENT, "proposer training corpus must hold at least 64 KiB");
-  const uint32_t G = P.n_groups;
+  const uint32_t G = P.n_spec;
   auto* pr = new Proposer();
   std::unique_ptr<Proposer> guard(pr);
   pr->G = G;

@@ -10,6 +10,10 @@ namespace ws {
 namespace {
 
 enum Look { LK_LINE_START = 1, LK_LINE_END, LK_TEXT_START, LK_TEXT_END, LK_WORD, LK_NOT_WORD };
+static_assert((int)LK_LINE_START == (int)LOOK_LINE_START && (int)LK_LINE_END == (int)LOOK_LINE_END &&
+                  (int)LK_TEXT_START == (int)LOOK_TEXT_START && (int)LK_TEXT_END == (int)LOOK_TEXT_END &&
+                  (int)LK_WORD == (int)LOOK_WORD && (int)LK_NOT_WORD == (int)LOOK_NOT_WORD,
+              "parser and NFA look-around kinds agree");
 
 struct Mode {
   bool ci = false;       // (?i)
@@ -477,7 +481,19 @@ struct NfaBuilder {
         return add(s);
       }
       case ReNode::EMPTY: return next;
-      case ReNode::LOOK: throw CompileError("look-around assertions are not supported on the GPU path");
+      case ReNode::LOOK: {
+        // a reversed pattern sees every look-behind as a look-ahead and back
+        int look = n.look;
+        if (reverse) {
+          look = look == LOOK_LINE_START ? LOOK_LINE_END
+                 : look == LOOK_LINE_END ? LOOK_LINE_START
+                 : look == LOOK_TEXT_START ? LOOK_TEXT_END
+                 : look == LOOK_TEXT_END ? LOOK_TEXT_START
+                                         : look;
+        }
+        NfaState s; s.kind = NfaState::ASSERT; s.a = next; s.look = look;
+        return add(s);
+      }
       case ReNode::CAPTURE: return compile(n.kids[0], next);
       case ReNode::CAT: {
         int entry = next;
@@ -566,14 +582,39 @@ Nfa build_nfa(const std::vector<const ReTree*>& trees, bool reverse) {
   return nfa;
 }
 
+bool look_holds(int look, int left, int right) {
+  switch (look) {
+    case LOOK_LINE_START: return left == CTX_BEGIN || left == CTX_NL;
+    case LOOK_LINE_END: return right == CTX_BEGIN || right == CTX_NL;
+    case LOOK_TEXT_START: return left == CTX_BEGIN;
+    case LOOK_TEXT_END: return right == CTX_BEGIN;
+    case LOOK_WORD: return (left == CTX_WORD) != (right == CTX_WORD);
+    case LOOK_NOT_WORD: return (left == CTX_WORD) == (right == CTX_WORD);
+  }
+  return false;
+}
+
 ByteClasses compute_classes(const std::vector<const Nfa*>& nfas) {
   // Refine the single class {0..255} by every set: two bytes stay together only
-  // if every set contains both or neither.
+  // if every set contains both or neither.  With assertions, the byte contexts
+  // (line feed, word bytes, others) are sets too.
   std::vector<uint64_t> sig(256, 0);
   std::vector<uint32_t> cls(256, 0);
   uint32_t n_cls = 1;
-  for (const Nfa* nfa : nfas) {
-    for (const ByteSet& s : nfa->sets) {
+  std::vector<ByteSet> context_sets;
+  for (const Nfa* nfa : nfas)
+    for (const NfaState& q : nfa->states)
+      if (q.kind == NfaState::ASSERT && context_sets.empty()) {
+        ByteSet nl, word;
+        nl.set('\n');
+        for (int b = 0; b < 256; ++b) if (byte_context((uint8_t)b) == CTX_WORD) word.set((size_t)b);
+        context_sets = {nl, word};
+      }
+  std::vector<const std::vector<ByteSet>*> all;
+  for (const Nfa* nfa : nfas) all.push_back(&nfa->sets);
+  all.push_back(&context_sets);
+  for (const std::vector<ByteSet>* sets : all) {
+    for (const ByteSet& s : *sets) {
       std::unordered_map<uint64_t, uint32_t> remap;
       std::vector<uint32_t> next(256);
       uint32_t k = 0;
@@ -616,6 +657,7 @@ void closure_all(const Nfa& nfa, int start, std::vector<uint32_t>& mark, uint32_
       case NfaState::CONSUME: case NfaState::MATCH: out.push_back((uint32_t)q); break;
       case NfaState::SPLIT: stack.push_back(s.b); stack.push_back(s.a); break;
       case NfaState::EPS: stack.push_back(s.a); break;
+      case NfaState::ASSERT: throw CompileError("assertion in a DFA without contexts");
     }
   }
 }
@@ -729,6 +771,7 @@ Dfa build_leftmost_first_dfa(const Nfa& nfa, const ByteClasses& cls, int max_sta
         case NfaState::MATCH: matched = true; break;
         case NfaState::SPLIT: st.push_back(s.b); st.push_back(s.a); break;
         case NfaState::EPS: st.push_back(s.a); break;
+        case NfaState::ASSERT: throw CompileError("assertion in a DFA without contexts");
       }
     }
   };
@@ -782,6 +825,181 @@ Dfa build_leftmost_first_dfa(const Nfa& nfa, const ByteClasses& cls, int max_sta
     uint32_t t = w;
     w = t | (d.is_match[t] ? DFA_FLAG_MATCH : 0u) | (t == 0 ? DFA_FLAG_DEAD : 0u);
   }
+  return d;
+}
+
+namespace {
+
+// Context of a byte class (the classes of a context DFA separate contexts).
+int class_context(const ByteClasses& cls, int c) { return byte_context(cls.representative[(size_t)c]); }
+
+// Epsilon closure under the contexts (left, right), depth-first in priority
+// order: SPLIT, EPS and holding ASSERT edges are followed, CONSUME and MATCH
+// states collected in the order reached.  With `first_match`, stops at the
+// first MATCH (the leftmost-first cut) and reports it in `matched`.
+void closure_ctx(const Nfa& nfa, int start, int left, int right, std::vector<uint32_t>& mark, uint32_t stamp,
+                 std::vector<uint32_t>& out, bool first_match, bool& matched) {
+  std::vector<int> st{start};
+  while (!st.empty() && !(first_match && matched)) {
+    const int q = st.back();
+    st.pop_back();
+    if (mark[(size_t)q] == stamp) continue;
+    mark[(size_t)q] = stamp;
+    const NfaState& s = nfa.states[(size_t)q];
+    switch (s.kind) {
+      case NfaState::CONSUME: out.push_back((uint32_t)q); break;
+      case NfaState::MATCH:
+        if (first_match) matched = true;
+        else out.push_back((uint32_t)q);
+        break;
+      case NfaState::SPLIT: st.push_back(s.b); st.push_back(s.a); break;
+      case NfaState::EPS: st.push_back(s.a); break;
+      case NfaState::ASSERT:
+        if (look_holds(s.look, left, right)) st.push_back(s.a);
+        break;
+    }
+  }
+}
+
+// The subset construction shared by both context DFAs.  A state's key is its
+// ordered seed list (NFA states whose closure is pending) and left context.
+// `step(seeds, left, right_class, next_seeds, match)` computes a transition.
+struct ContextBuilder {
+  const Nfa& nfa;
+  const ByteClasses& cls;
+  std::unordered_map<std::vector<uint32_t>, uint32_t, VecHash> index;
+  std::vector<std::vector<uint32_t>> seeds;
+  std::vector<int> left;
+  ContextBuilder(const Nfa& n, const ByteClasses& c) : nfa(n), cls(c) {
+    intern({}, CTX_BEGIN);  // 0: dead (no seeds)
+  }
+  uint32_t intern(std::vector<uint32_t>&& key, int ctx) {
+    if (key.empty() && !seeds.empty()) return 0;
+    std::vector<uint32_t> k = key;
+    k.push_back((uint32_t)ctx);
+    auto it = index.find(k);
+    if (it != index.end()) return it->second;
+    const uint32_t id = (uint32_t)seeds.size();
+    index.emplace(std::move(k), id);
+    seeds.push_back(std::move(key));
+    left.push_back(ctx);
+    return id;
+  }
+};
+
+}  // namespace
+
+Dfa build_context_all_dfa(const Nfa& nfa, const ByteClasses& cls, int max_states) {
+  Dfa d;
+  d.n_classes = cls.count;
+  ContextBuilder B(nfa, cls);
+  std::vector<uint32_t> starts;
+  for (int s : nfa.starts) starts.push_back((uint32_t)s);
+  for (int k = 0; k < 4; ++k) d.ctx_start[k] = B.intern(std::vector<uint32_t>(starts), k);
+  d.start_anchored = d.ctx_start[CTX_BEGIN];
+  std::vector<uint32_t> mark(nfa.states.size(), 0);
+  uint32_t stamp = 0;
+  const int C = cls.count;
+  // patterns matching at a state's position, per right context
+  std::vector<std::vector<uint32_t>> lists;
+  auto closure = [&](uint32_t cur, int right, std::vector<uint32_t>& out) {
+    ++stamp;
+    out.clear();
+    bool unused = false;
+    for (uint32_t q : B.seeds[cur]) closure_ctx(nfa, (int)q, B.left[cur], right, mark, stamp, out, false, unused);
+  };
+  std::vector<uint32_t> cl, nxt;
+  for (size_t cur = 0; cur < B.seeds.size(); ++cur) {
+    if ((int)B.seeds.size() > max_states) { d.too_big = true; return d; }
+    d.trans.resize((cur + 1) * (size_t)C, 0);
+    lists.resize((cur + 1) * 4);
+    for (int k = 0; k < 4; ++k) {
+      closure((uint32_t)cur, k, cl);
+      std::vector<uint32_t> pats;
+      for (uint32_t q : cl)
+        if (nfa.states[q].kind == NfaState::MATCH) pats.push_back((uint32_t)nfa.states[q].pattern);
+      std::sort(pats.begin(), pats.end());
+      pats.erase(std::unique(pats.begin(), pats.end()), pats.end());
+      lists[cur * 4 + (size_t)k] = std::move(pats);
+    }
+    if (cur == 0) continue;
+    for (int c = 0; c < C; ++c) {
+      const int right = class_context(cls, c);
+      const uint8_t b = cls.representative[(size_t)c];
+      closure((uint32_t)cur, right, cl);
+      nxt.clear();
+      for (uint32_t q : cl) {
+        const NfaState& s = nfa.states[q];
+        if (s.kind == NfaState::CONSUME && nfa.sets[(size_t)s.set].test(b)) nxt.push_back((uint32_t)s.a);
+      }
+      std::sort(nxt.begin(), nxt.end());
+      nxt.erase(std::unique(nxt.begin(), nxt.end()), nxt.end());
+      const uint32_t id = B.intern(std::vector<uint32_t>(nxt), right);
+      d.trans[cur * (size_t)C + (size_t)c] =
+          id | (lists[cur * 4 + (size_t)right].empty() ? 0u : DFA_FLAG_MATCH) | (id == 0 ? DFA_FLAG_DEAD : 0u);
+    }
+  }
+  d.n_states = (int)B.seeds.size();
+  d.is_match.assign((size_t)d.n_states, 0);
+  d.match_ptr.assign(4 * (size_t)d.n_states + 1, 0);
+  for (size_t j = 0; j < 4 * (size_t)d.n_states; ++j) {
+    d.match_ptr[j] = (uint32_t)d.match_list.size();
+    d.match_list.insert(d.match_list.end(), lists[j].begin(), lists[j].end());
+    if (!lists[j].empty()) d.is_match[j / 4] = 1;
+  }
+  d.match_ptr[4 * (size_t)d.n_states] = (uint32_t)d.match_list.size();
+  return d;
+}
+
+Dfa build_context_lf_dfa(const Nfa& nfa, const ByteClasses& cls, int max_states) {
+  Dfa d;
+  d.n_classes = cls.count;
+  ContextBuilder B(nfa, cls);
+  std::vector<uint32_t> starts;
+  for (int s : nfa.starts) starts.push_back((uint32_t)s);
+  for (int k = 0; k < 4; ++k) d.ctx_start[k] = B.intern(std::vector<uint32_t>(starts), k);
+  d.start_anchored = d.ctx_start[CTX_BEGIN];
+  std::vector<uint32_t> mark(nfa.states.size(), 0);
+  uint32_t stamp = 0;
+  const int C = cls.count;
+  // ordered closure of a state's seeds under a right context: the threads in
+  // priority order up to the first match (which cuts the rest)
+  auto closure = [&](uint32_t cur, int right, std::vector<uint32_t>& out, bool& matched) {
+    ++stamp;
+    out.clear();
+    matched = false;
+    for (uint32_t q : B.seeds[cur]) {
+      closure_ctx(nfa, (int)q, B.left[cur], right, mark, stamp, out, true, matched);
+      if (matched) break;
+    }
+  };
+  std::vector<uint32_t> cl, nxt;
+  std::vector<uint8_t> end_match;
+  for (size_t cur = 0; cur < B.seeds.size(); ++cur) {
+    if ((int)B.seeds.size() > max_states) { d.too_big = true; return d; }
+    d.trans.resize((cur + 1) * (size_t)C, 0);
+    bool m_end = false;
+    closure((uint32_t)cur, CTX_BEGIN, cl, m_end);
+    end_match.push_back(m_end ? 1 : 0);
+    if (cur == 0) continue;
+    for (int c = 0; c < C; ++c) {
+      const int right = class_context(cls, c);
+      const uint8_t b = cls.representative[(size_t)c];
+      bool m = false;
+      closure((uint32_t)cur, right, cl, m);
+      nxt.clear();
+      for (uint32_t q : cl) {  // successors in priority order, first occurrence kept
+        const NfaState& s = nfa.states[q];
+        if (!nfa.sets[(size_t)s.set].test(b)) continue;
+        if (std::find(nxt.begin(), nxt.end(), (uint32_t)s.a) == nxt.end()) nxt.push_back((uint32_t)s.a);
+      }
+      const uint32_t id = B.intern(std::vector<uint32_t>(nxt), right);
+      d.trans[cur * (size_t)C + (size_t)c] = id | (m ? DFA_FLAG_MATCH : 0u) | (id == 0 ? DFA_FLAG_DEAD : 0u);
+    }
+  }
+  d.n_states = (int)B.seeds.size();
+  d.is_match.assign(end_match.begin(), end_match.end());
+  d.match_ptr.assign((size_t)d.n_states + 1, 0);
   return d;
 }
 

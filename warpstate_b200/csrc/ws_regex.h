@@ -4,9 +4,10 @@
 // Syntax and flags follow what the reference compiles its regexes with:
 // regex-syntax with unicode(false), utf8(false) and multi_line(true)
 // (core/src/pattern/compiler.rs:167-174, core/src/regex_engine.rs:7-17,
-// core/src/dfa/builder.rs:36-54).  Look-around assertions (^ $ \b \B \A \z) and
-// patterns that can match the empty string are rejected for the GPU path with
-// PatternCompilationFailed; everything else in that syntax is supported.
+// core/src/dfa/builder.rs:36-54).  Patterns that can match the empty string
+// are rejected for the GPU path with PatternCompilationFailed; everything
+// else in that syntax is supported, look-around assertions (^ $ \b \B \A \z)
+// through the context DFAs below.
 #pragma once
 #include <bitset>
 #include <cstdint>
@@ -48,11 +49,28 @@ int64_t tree_max_len(const ReTree& t);  // -1 when unbounded
 
 // ------------------------------------------------------------------------- NFA
 struct NfaState {
-  enum Kind : uint8_t { CONSUME, SPLIT, EPS, MATCH } kind;
+  enum Kind : uint8_t { CONSUME, SPLIT, EPS, MATCH, ASSERT } kind;
   int a = -1, b = -1;  // successors (SPLIT: a has priority over b)
   int set = -1;        // CONSUME: index into Nfa::sets
   int pattern = -1;    // MATCH: local pattern index
+  int look = 0;        // ASSERT: look-around kind (LOOK_* below); passes to a when it holds
 };
+
+// Look-around kinds (multi_line(true), ASCII word characters).
+enum { LOOK_LINE_START = 1, LOOK_LINE_END, LOOK_TEXT_START, LOOK_TEXT_END, LOOK_WORD, LOOK_NOT_WORD };
+
+// Context of a position for the assertions: the byte before it (CTX_BEGIN at
+// the start of the input or batch item) and the byte at it (CTX_BEGIN standing
+// for the end of the input or item): a line feed, an ASCII word byte
+// [0-9A-Za-z_], or any other byte.
+enum { CTX_BEGIN = 0, CTX_NL = 1, CTX_WORD = 2, CTX_OTHER = 3 };
+inline int byte_context(uint8_t c) {
+  if (c == '\n') return CTX_NL;
+  const bool w = (c >= '0' && c <= '9') || (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z') || c == '_';
+  return w ? CTX_WORD : CTX_OTHER;
+}
+// Whether an assertion holds between a position's left and right contexts.
+bool look_holds(int look, int left, int right);
 
 struct Nfa {
   std::vector<NfaState> states;
@@ -90,6 +108,7 @@ struct Dfa {
   uint32_t start_anchored = 0;
   uint32_t start_unanchored = 0;        // forward DFAs only
   bool too_big = false;
+  uint32_t ctx_start[4] = {0, 0, 0, 0};  // context DFAs: start state per left context
 };
 
 // MatchKind::All DFA over a group of patterns.  With `with_unanchored`, the
@@ -102,6 +121,24 @@ Dfa build_all_dfa(const Nfa& nfa, const ByteClasses& cls, bool with_unanchored, 
 // first match corresponds to.  Walking it from s and remembering the last match
 // position gives the end find_iter reports for a match starting at s.
 Dfa build_leftmost_first_dfa(const Nfa& nfa, const ByteClasses& cls, int max_states);
+
+// Context DFAs of patterns with look-around assertions.  A state is the set of
+// NFA threads before their epsilon closure plus the left context of the
+// current position; the closure is taken on the next byte, whose context
+// decides the look-ahead half of every assertion.  So the transition on the
+// byte at position p reports the matches that END AT p (one byte late), and
+// the end of the input or item needs the end step: the closure under the
+// right context CTX_BEGIN.  Anchored only; ctx_start[k] is the start state for
+// left context k.  The byte classes must separate the contexts
+// (compute_classes does when the NFA has assertions).
+//   build_context_all_dfa: MatchKind::All over a group of patterns.  The
+//     patterns matching at p are listed per (state, right context):
+//     match_ptr has 4 * n_states + 1 entries, list (s, k) at 4 * s + k; the
+//     match flag of a transition says its list is not empty.
+//   build_context_lf_dfa: leftmost-first over one pattern (a match drops
+//     every lower-priority thread); is_match[s] says the end step matches.
+Dfa build_context_all_dfa(const Nfa& nfa, const ByteClasses& cls, int max_states);
+Dfa build_context_lf_dfa(const Nfa& nfa, const ByteClasses& cls, int max_states);
 
 // Reorders states so that `order` (old ids, dead state first) becomes 0..n-1.
 void renumber_dfa(Dfa& d, const std::vector<uint32_t>& order);

@@ -135,6 +135,8 @@ StepPlan plan_step(const ws_matcher* m, uint64_t win_base, uint64_t old_seen, ui
   if (m->lit.n_literals && m->max_literal_len > 1)
     keep = std::min(keep, old_seen - std::min<uint64_t>(old_seen, m->max_literal_len - 1));
   if (m->rx.n_regex) keep = std::min(keep, frontier);
+  // look-behind assertions read the byte before a start: keep it too
+  if (m->rx.has_context && keep > 0 && keep == frontier) keep -= 1;
   p.keep = std::max(keep, win_base);
   const int64_t mx = regex_max_len(m);
   if (last) {

@@ -124,6 +124,13 @@ def resolve_chains(rank: int, world: int, shard: ScanShard | None, n_regex: int,
     return matches
 
 
+def shard_lead(shard: ScanShard, context: bool) -> int:
+    """Bytes before a shard's own range that its buffer holds: one when the
+    pattern set has look-behind assertions (^ \\b \\B \\A read the byte before a
+    start) and the shard is not the first, else none."""
+    return 1 if context and shard.start > 0 else 0
+
+
 class ShardScanner:
     """``ws_scan_shard`` on this process's GPU for one matcher."""
 
@@ -132,6 +139,7 @@ class ShardScanner:
         self.m = matcher
         self.torch = torch
         info = matcher.info()
+        self.context = bool(info["regex_context"])
         self.n_regex = int(info["n_regex"])
         self.max_literal_len = int(info["max_literal_len"])
         self.max_regex_len = int(info["max_regex_len"])
@@ -145,14 +153,23 @@ class ShardScanner:
     def halo(self, input_len: int) -> int:
         return shard_halo(self.max_literal_len, self.max_regex_len, input_len)
 
+    def lead(self, shard: ScanShard) -> int:
+        return shard_lead(shard, self.context)
+
+    def buffer(self, host: np.ndarray, shard: ScanShard):
+        """The device copy of a shard's bytes, its lead byte included."""
+        a = shard.start - self.lead(shard)
+        return self.torch.from_numpy(np.ascontiguousarray(host[a:shard.scan_end])).to(self.dev)
+
     def scan(self, d_buf, shard: ScanShard, cursor_in: np.ndarray):
-        """d_buf: device tensor holding bytes [shard.start, shard.scan_end)."""
+        """d_buf: device tensor holding bytes [shard.start - lead, shard.scan_end)."""
         torch = self.torch
         from . import _call
         if self.n_regex:
             self.d_cursor[: self.n_regex].copy_(torch.from_numpy(cursor_in.astype(np.int64)))
         s = torch.cuda.current_stream()
-        _call(N.lib().ws_scan_shard, self.m._h, d_buf.data_ptr(), shard.scan_end - shard.start, shard.start,
+        base = shard.start - self.lead(shard)
+        _call(N.lib().ws_scan_shard, self.m._h, d_buf.data_ptr(), shard.scan_end - base, base,
               shard.nominal_end, self.d_cursor.data_ptr(), self.d_out.data_ptr(), self.cap, self.d_cnt.data_ptr(),
               s.cuda_stream)
         n = int(self.d_cnt.item())
@@ -161,6 +178,8 @@ class ShardScanner:
             raise MatchBufferOverflow(n, self.cap)
         a = self.d_out[: 3 * n].view(n, 3).cpu().numpy().view(np.uint64)
         out = np.stack([a[:, 0] & np.uint64(0xFFFFFFFF), a[:, 1], a[:, 2]], axis=1)
+        if base < shard.start:  # literal matches at the lead byte belong to the previous shard
+            out = out[out[:, 1] >= np.uint64(shard.start)]
         cur = self.d_cursor[: self.n_regex].cpu().numpy().view(np.uint64).copy()
         return out, cur
 
@@ -189,7 +208,7 @@ def sharded_scan(matcher, data, group=None, gather: bool = True) -> np.ndarray:
     shard = shards[rank] if rank < len(shards) else None
     d_buf = None
     if shard is not None:
-        d_buf = torch.from_numpy(np.ascontiguousarray(host[shard.start:shard.scan_end])).to(sc.dev)
+        d_buf = sc.buffer(host, shard)
     backend = dist.get_backend(group)
     tdev = sc.dev if backend == "nccl" else torch.device("cpu")
 
@@ -218,7 +237,7 @@ def sharded_scan_local(matcher, data, n_shards: int) -> np.ndarray:
         np.zeros(0, np.uint8)
     sc = ShardScanner(matcher)
     shards = build_scan_shards(n, n_shards, sc.halo(n))
-    bufs = [torch.from_numpy(np.ascontiguousarray(host[s.start:s.scan_end])).to(sc.dev) for s in shards]
+    bufs = [sc.buffer(host, s) for s in shards]
     results = run_local_protocol(len(shards), sc.n_regex, shards,
                                  lambda r, c: sc.scan(bufs[r], shards[r], c))
     del keep
@@ -302,8 +321,7 @@ class MultiGpuMatcher:
 
         def upload(r):
             with torch.cuda.device(self.devices[r]):
-                bufs[r] = torch.from_numpy(np.ascontiguousarray(host[shards[r].start:shards[r].scan_end])).to(
-                    scanners[r].dev)
+                bufs[r] = scanners[r].buffer(host, shards[r])
 
         def scan(r, cursor):
             with torch.cuda.device(self.devices[r]):
