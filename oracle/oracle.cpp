@@ -11,6 +11,7 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include <unordered_map>
 
 namespace {
 
@@ -442,6 +443,10 @@ struct Program {
   std::vector<uint64_t> pair_ok;  // 65536 bits: (b0,b1) may begin a match
   std::bitset<256> first;         // b0 may begin a match
   std::bitset<256> one_byte;      // b0 alone is a complete match
+  // every match is at least prefix_len (8) bytes long and begins with
+  // one of these (little-endian), when there are few enough to list
+  int prefix_len = 0;
+  std::vector<uint64_t> prefixes;
 };
 
 struct Compiler {
@@ -581,6 +586,57 @@ void analyze_prefixes(Program& P) {
       if (!ok) for (int q : s1) if (P.sets[P.code[q].x][b1]) { ok = true; break; }
       if (ok) { size_t key = (size_t)b0 << 8 | b1; P.pair_ok[key >> 6] |= 1ull << (key & 63); }
     }
+  }
+}
+
+// The first K bytes of every match (K = 8 here), listed when the regex
+// matches nothing shorter than K bytes and the prefixes number at most
+// kMaxPrefixes (assertions pass here: an over-approximation, as for the pair
+// index).  Used only to skip start positions where no match can begin.
+constexpr size_t kMaxPrefixes = 4096;
+bool list_prefixes(const Program& P, int K, std::vector<uint64_t>& out) {
+  const size_t n = P.code.size();
+  struct Prefix { uint64_t bytes; std::vector<int> pcs; };
+  std::vector<Prefix> cur;
+  {
+    std::vector<char> seen(n, 0);
+    std::vector<int> s0;
+    bool m0 = false;
+    closure(P, 0, seen, s0, m0);
+    if (m0) return false;
+    cur.push_back({0ull, s0});
+  }
+  for (int depth = 0; depth < K; ++depth) {
+    std::vector<Prefix> nxt;
+    for (const Prefix& pf : cur) {
+      std::bitset<256> can;
+      for (int q : pf.pcs) can |= P.sets[P.code[q].x];
+      for (int b = 0; b < 256; ++b) {
+        if (!can[b]) continue;
+        std::vector<char> seen(n, 0);
+        std::vector<int> s1;
+        bool m1 = false, any = false;
+        for (int q : pf.pcs)
+          if (P.sets[P.code[q].x][b]) { any = true; closure(P, q + 1, seen, s1, m1); }
+        if (!any) continue;
+        if (m1 && depth < K - 1) return false;  // a match shorter than K bytes
+        nxt.push_back({pf.bytes | ((uint64_t)b << (8 * depth)), s1});
+        if (nxt.size() > kMaxPrefixes) return false;
+      }
+    }
+    cur.swap(nxt);
+  }
+  for (const Prefix& pf : cur) out.push_back(pf.bytes);
+  std::sort(out.begin(), out.end());
+  return true;
+}
+
+void analyze_long_prefixes(Program& P) {
+  if (P.nullable || P.has_assert) return;
+  std::vector<uint64_t> v;
+  if (list_prefixes(P, 8, v)) {
+    P.prefix_len = 8;
+    P.prefixes.swap(v);
   }
 }
 
@@ -781,6 +837,7 @@ or_regex* or_regex_new(const char* pattern, char* err, size_t err_cap) {
     r->prog.maxlen = (int)std::min<long long>(mx, 1 << 30);
     r->prog.nullable = (mn == 0);
     analyze_prefixes(r->prog);
+    analyze_long_prefixes(r->prog);
     return r;
   } catch (const std::exception& e) {
     if (err && err_cap) { std::strncpy(err, e.what(), err_cap - 1); err[err_cap - 1] = 0; }
@@ -870,13 +927,16 @@ uint64_t or_regex_set_scan(or_regex* const* rs, const uint32_t* pattern_ids, uin
   std::vector<std::vector<or_match>> res(T);
   std::atomic<uint32_t> next{0};
   std::vector<std::thread> th;
+  // at most 32 regexes per block, and a whole number of blocks per thread
+  const uint32_t nblocks = ((n + 31) / 32 + (uint32_t)T - 1) / (uint32_t)T * (uint32_t)T;
+  const uint32_t BLOCK = std::max<uint32_t>(1, (n + nblocks - 1) / nblocks);
   for (int t = 0; t < T; ++t) {
     th.emplace_back([&, t] {
       // Threads take blocks of regexes; within a block, non-nullable regexes
       // without assertions share one pass over the input driven by an inverted
-      // index of their possible first byte pairs (each regex keeps its own
-      // find_iter cursor, so results equal per-regex find_iter).
-      const uint32_t BLOCK = 32;
+      // index of their possible first four bytes (or first byte pairs, for
+      // regexes whose 4-byte prefixes are not listed); each regex keeps its
+      // own find_iter cursor, so results equal per-regex find_iter.
       std::vector<std::pair<uint32_t, uint32_t>> tmp;
       while (true) {
         uint32_t b0 = next.fetch_add(BLOCK);
@@ -896,8 +956,36 @@ uint64_t or_regex_set_scan(or_regex* const* rs, const uint32_t* pattern_ids, uin
         if (simple.empty()) continue;
         std::vector<std::vector<uint16_t>> index(65536);
         std::vector<std::vector<uint16_t>> last_byte(256);
+        // regexes with listed 8-byte prefixes: a 2^20-bit filter of the prefix
+        // hashes, then the exact lists
+        std::unordered_map<uint64_t, std::vector<uint16_t>> pre_index;
+        std::vector<uint64_t> pre_bits((1u << 20) / 64, 0);
+        std::vector<uint64_t> pre_pairs(65536 / 64, 0);  // their first two bytes
+        auto pre_hash = [](uint64_t x) { return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 44); };
+        // a listed prefix replaces the pair index only for a regex whose pairs
+        // start a search at more than one position in 64 of (a sample of) the
+        // input
+        const uint64_t sample = std::min<uint64_t>(len, 1u << 20);
+        auto pairs_busy = [&](const Program& P) {
+          uint64_t hits = 0;
+          for (uint64_t q = 0; q + 1 < sample; ++q) {
+            const size_t key = (size_t)data[q] << 8 | data[q + 1];
+            hits += (P.pair_ok[key >> 6] >> (key & 63)) & 1;
+          }
+          return hits * 64 > sample;
+        };
         for (uint16_t j = 0; j < simple.size(); ++j) {
           const Program& P = rs[simple[j]]->prog;
+          if (P.prefix_len && pairs_busy(P)) {
+            for (uint64_t x : P.prefixes) {
+              pre_index[x].push_back(j);
+              const uint32_t h = pre_hash(x);
+              pre_bits[h >> 6] |= 1ull << (h & 63);
+              const size_t key = (size_t)(x & 0xFF) << 8 | ((x >> 8) & 0xFF);
+              pre_pairs[key >> 6] |= 1ull << (key & 63);
+            }
+            continue;
+          }
           for (size_t key = 0; key < 65536; ++key)
             if ((P.pair_ok[key >> 6] >> (key & 63)) & 1) index[key].push_back(j);
           for (int c = 0; c < 256; ++c) if (P.one_byte[c]) last_byte[c].push_back(j);
@@ -905,18 +993,38 @@ uint64_t or_regex_set_scan(or_regex* const* rs, const uint32_t* pattern_ids, uin
         std::vector<std::unique_ptr<Backtracker>> bts;
         for (uint32_t k : simple) bts.emplace_back(new Backtracker(rs[k]->prog));
         std::vector<uint64_t> cursor(simple.size(), 0);
-        for (uint64_t q = 0; q < len; ++q) {
-          const std::vector<uint16_t>* lst;
-          if (q + 1 < len) lst = &index[(size_t)data[q] << 8 | data[q + 1]];
-          else lst = &last_byte[data[q]];
-          for (uint16_t j : *lst) {
-            if (q < cursor[j]) continue;
-            int64_t e = bts[j]->run(data, len, q);
-            if (e >= 0) {
-              res[t].push_back({pattern_ids[simple[j]], (uint32_t)q, (uint32_t)e});
-              cursor[j] = (uint64_t)e;
-            }
+        auto attempt = [&](uint16_t j, uint64_t q) {
+          if (q < cursor[j]) return;
+          int64_t e = bts[j]->run(data, len, q);
+          if (e >= 0) {
+            res[t].push_back({pattern_ids[simple[j]], (uint32_t)q, (uint32_t)e});
+            cursor[j] = (uint64_t)e;
           }
+        };
+        if (pre_index.empty()) {
+          for (uint64_t q = 0; q < len; ++q) {
+            const std::vector<uint16_t>* lst;
+            if (q + 1 < len) lst = &index[(size_t)data[q] << 8 | data[q + 1]];
+            else lst = &last_byte[data[q]];
+            for (uint16_t j : *lst) attempt(j, q);
+          }
+          continue;
+        }
+        for (uint64_t q = 0; q < len; ++q) {
+          if (q + 1 >= len) {
+            for (uint16_t j : last_byte[data[q]]) attempt(j, q);
+            continue;
+          }
+          const size_t key = (size_t)data[q] << 8 | data[q + 1];
+          for (uint16_t j : index[key]) attempt(j, q);
+          if (q + 8 > len || !((pre_pairs[key >> 6] >> (key & 63)) & 1)) continue;
+          uint64_t x;
+          std::memcpy(&x, data + q, 8);
+          const uint32_t h = pre_hash(x);
+          if (!((pre_bits[h >> 6] >> (h & 63)) & 1)) continue;
+          auto it = pre_index.find(x);
+          if (it != pre_index.end())
+            for (uint16_t j : it->second) attempt(j, q);
         }
       }
     });
