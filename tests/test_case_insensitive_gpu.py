@@ -84,7 +84,7 @@ def test_batch_and_stream_vs_oracle():
     lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
     got = ws.scan_batch_packed(m, data, lens)
     exp = oracle.batch_scan(wl.patterns, data, wl.items, case_insensitive=True)
-    assert len(exp) > 100 and np.array_equal(got, exp)
+    assert len(exp) > 50 and np.array_equal(got, exp)
     total = int(lens.sum())
     whole = oracle.scan_patterns(wl.patterns, data[:total], case_insensitive=True)
     sp = ws.StreamPipeline(m).scan_array(data[:total], block=(1 << 16) + 7)

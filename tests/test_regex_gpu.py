@@ -255,11 +255,20 @@ def test_nucleotide_config_scaled_vs_oracle(mode):
     # the nucleotide configuration (k-mer literals plus IUPAC-degenerate
     # regexes over ACGT with N runs) at 64 MiB, both regex paths
     wl = w.dna(size=64 << 20)
+    # more IUPAC regex samples than the configuration's one plant per MiB
+    rng = np.random.default_rng(17)
+    r = w.Rng(77)
+    rx = w.gen_iupac(200, 5 * 1000 + 2)
+    for k in range(600):
+        src, pos = rx[k % len(rx)]
+        s = bytes(r.choice(w.IUPAC.get(c, c)).encode()[0] for c in pos)
+        at = int(rng.integers(0, wl.data.size - 64))
+        wl.data[at:at + len(s)] = np.frombuffer(s, dtype=np.uint8)
     m = matcher(wl.patterns, mode=mode, max_matches=1 << 20)
     got = m.scan_array(wl.data)
     exp = oracle.scan_patterns(wl.patterns, wl.data)
     rx_ids = {i for i, (k, _) in enumerate(wl.patterns) if k == 1}
-    assert sum(1 for p in exp[:, 0].tolist() if p in rx_ids) >= 20  # regex matches are part of the check
+    assert sum(1 for p in exp[:, 0].tolist() if p in rx_ids) >= 100  # regex matches are part of the check
     assert got.shape == exp.shape and np.array_equal(got, exp)
 
 

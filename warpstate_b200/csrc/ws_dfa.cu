@@ -437,30 +437,28 @@ __device__ __forceinline__ uint4 load_stream16(const uint8_t* p) {
 // 16-bit image of a group's unanchored hot rows (kImg16Slots halfwords per
 // input byte value, 224 KiB): entry (row r, byte b) at halfword
 // b * kImg16Slots + slot(r), where the first row takes the even slots 0..62
-// (one copy per lane, lane l at slot 2l), rows 1..32 the odd slots 1..63 and
-// rows 33..415 the slots 64..446; slot 447 is the trap column of cold states.
-// kImg16Slots / 2 is a multiple of 32, so a slot sits in bank (slot / 2) mod
-// 32 for every byte: lane l's copy of the first row in bank l, as in the
-// 32-bit image.  A walk state is the byte offset 2 * slot (lane * 4 for the
-// first row); an entry is the next row's state, or -1 for every transition
-// that is not into a hot row (match, cold, dead), which the walk takes from
-// the class-indexed table.
+// (one copy per lane, lane l at slot 2l) and rows 1..383 the slots 64..446;
+// slot 447 is the trap column of cold states.  kImg16Slots / 2 is a multiple
+// of 32, so a slot sits in bank (slot / 2) mod 32 for every byte: lane l's
+// copy of the first row in bank l, as in the 32-bit image.  A walk state is
+// the byte offset 2 * slot (lane * 4 for the first row); an entry is the next
+// row's state (0 for the first row, made lane-specific by max(entry,
+// lane * 4): every other row's state is at least 128, above every lane's),
+// or -1 for every transition that is not into a hot row (match, cold, dead),
+// which the walk takes from the class-indexed table.
 constexpr uint32_t kImg16Slots = 448;
 constexpr uint32_t kImg16Entries = 256 * kImg16Slots;
 constexpr uint32_t kTrap16 = 2 * 447;
 static_assert(kImg16Entries * 2 <= kImgWords * 4, "the 16-bit image fits the shared-memory budget");
-static_assert(kHotRows16 == 1 + 32 + 383, "row slots");
-__host__ __device__ __forceinline__ uint32_t slot16_of_row(uint32_t r) {
-  return r <= 32 ? 2 * r - 1 : 64 + (r - 33);
-}
+static_assert(kHotRows16 == 1 + (447 - 64), "row slots");
+__host__ __device__ __forceinline__ uint32_t slot16_of_row(uint32_t r) { return 63 + r; }
 __host__ __device__ __forceinline__ uint32_t state16_of_row(uint32_t r, uint32_t lane4) {
   return r == 0 ? lane4 : 2 * slot16_of_row(r);
 }
 __device__ __forceinline__ uint32_t row16_of_state(uint32_t st, uint32_t cold_row) {
   if (st == kTrap16) return cold_row;
   const uint32_t slot = st >> 1;
-  if (slot < 64) return (slot & 1) ? (slot + 1) >> 1 : 0;
-  return slot - 31;
+  return slot < 64 ? 0 : slot - 63;
 }
 
 #define WS_STEP16(img, st, b) \
@@ -1601,10 +1599,14 @@ void layout_forward(RegexPlan& P) {
   if (P.fwd.size() > DFA_MASK_STATE) raise(WS_ERR_COMPILE, "regex tables exceed 2^30 words");
   P.d_groups.upload(P.groups.data(), P.groups.size() * sizeof(GroupDev));
   P.d_fwd.upload(P.fwd.data(), P.fwd.size() * 4);
-  P.d_hot.upload(P.hot.data(), std::max<size_t>(P.hot.size(), 4) * 4);
-  P.d_hot16.upload(P.hot16.data(), std::max<size_t>(P.hot16.size(), 8) * 2);
+  // sets whose groups all carry context have no hot image: the buffers still exist
+  if (P.hot.size() < 4) P.hot.resize(4, 0);
+  if (P.hot16.size() < 8) P.hot16.resize(8, 0);
+  if (P.mlist.empty()) P.mlist.push_back(0);
+  P.d_hot.upload(P.hot.data(), P.hot.size() * 4);
+  P.d_hot16.upload(P.hot16.data(), P.hot16.size() * 2);
   P.d_mptr.upload(P.mptr.data(), P.mptr.size() * 4);
-  P.d_mlist.upload(P.mlist.data(), std::max<size_t>(P.mlist.size(), 1) * 4);
+  P.d_mlist.upload(P.mlist.data(), P.mlist.size() * 4);
 }
 
 void build_groups(const std::vector<ReTree>& trees, const std::vector<uint32_t>& members, int max_states,
@@ -1735,7 +1737,8 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
   P.d_lf.upload(P.lf.data(), P.lf.size() * 4);
   P.d_cls.upload(P.cls.data(), P.cls.size());
   P.d_rmptr.upload(P.rmptr.data(), P.rmptr.size() * 4);
-  P.d_rmlist.upload(P.rmlist.data(), std::max<size_t>(P.rmlist.size(), 1) * 4);
+  if (P.rmlist.empty()) P.rmlist.push_back(0);
+  P.d_rmlist.upload(P.rmlist.data(), P.rmlist.size() * 4);
   P.d_lfinfo.upload(P.lfinfo.data(), P.lfinfo.size() * 4);
   P.d_lfx.upload(P.lfx.data(), P.lfx.size() * 4);
   P.d_pid.upload(P.pid.data(), P.pid.size() * 4);

@@ -33,8 +33,8 @@ namespace ws {
 // replicated per lane, 191 more rows column-interleaved; see ws_dfa.cu).
 constexpr uint32_t kHotRows = 192;
 // Hot rows of the 16-bit unanchored image (see ws_dfa.cu): the first row
-// replicated per lane, 415 more.
-constexpr uint32_t kHotRows16 = 416;
+// replicated per lane, 383 more.
+constexpr uint32_t kHotRows16 = 384;
 
 struct GroupDev {
   uint32_t fwd_off;          // class-indexed forward table (u32 words)

@@ -19,6 +19,7 @@ void raise(ws_status s, const std::string& msg, uint64_t index, uint64_t count, 
 
 void check_cuda(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return;
+  cudaGetLastError();  // a failed call's error is not left behind for the caller's next check
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
     raise(WS_ERR_NO_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
   raise(WS_ERR_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
@@ -90,7 +91,8 @@ void DeviceBuffer::alloc(size_t n) {
 void DeviceBuffer::upload(const void* src, size_t n) {
   alloc(n + 16);  // 16 spare bytes: vector loads of the tail stay inside the allocation
   check_cuda(cudaMemset(ptr, 0, n + 16), "cudaMemset");
-  if (n) check_cuda(cudaMemcpy(ptr, src, n, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  // a null source (an empty table given a minimum size) leaves zeros
+  if (n && src) check_cuda(cudaMemcpy(ptr, src, n, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
 }
 
 void plan_literals(const ws_pattern_tables& given, LiteralPlan& plan) {
