@@ -100,7 +100,6 @@ struct DevTables {
   const GroupDev* groups;
   const uint32_t* fwd;
   const uint32_t* hot;
-  const uint16_t* hot16;
   const uint32_t* rev;
   const uint32_t* lf;
   const uint8_t* cls;
@@ -424,171 +423,10 @@ __global__ void __launch_bounds__(256) dfa_context_kernel(DevTables t, ScanPtrs 
 }
 
 // ------------------------------------------------------- speculative walk
-// 16 input bytes of a chunk (global loads that do not allocate in L1, which
-// keeps L1 for the class-indexed rows of cold states).
-__device__ __forceinline__ uint4 load_stream16(const uint8_t* p) {
-  uint4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(p));
-  return v;
-}
-
-// 16-bit image of a group's unanchored hot rows (kImg16Slots halfwords per
-// input byte value, 224 KiB): entry (row r, byte b) at halfword
-// b * kImg16Slots + slot(r), where the first row takes the even slots 0..62
-// (one copy per lane, lane l at slot 2l) and rows 1..383 the slots 64..446;
-// slot 447 is the trap column of cold states.  kImg16Slots / 2 is a multiple
-// of 32, so a slot sits in bank (slot / 2) mod 32 for every byte: lane l's
-// copy of the first row in bank l, as in the 32-bit image.  A walk state is
-// the byte offset 2 * slot (lane * 4 for the first row); an entry is the next
-// row's state (0 for the first row, made lane-specific by max(entry,
-// lane * 4): every other row's state is at least 128, above every lane's),
-// or -1 for every transition that is not into a hot row (match, cold, dead),
-// which the walk takes from the class-indexed table.
-constexpr uint32_t kImg16Slots = 448;
-constexpr uint32_t kImg16Entries = 256 * kImg16Slots;
-constexpr uint32_t kTrap16 = 2 * 447;
-static_assert(kImg16Entries * 2 <= kImgWords * 4, "the 16-bit image fits the shared-memory budget");
-static_assert(kHotRows16 == 1 + (447 - 64), "row slots");
-__host__ __device__ __forceinline__ uint32_t slot16_of_row(uint32_t r) { return 63 + r; }
-__host__ __device__ __forceinline__ uint32_t state16_of_row(uint32_t r, uint32_t lane4) {
-  return r == 0 ? lane4 : 2 * slot16_of_row(r);
-}
-__device__ __forceinline__ uint32_t row16_of_state(uint32_t st, uint32_t cold_row) {
-  if (st == kTrap16) return cold_row;
-  const uint32_t slot = st >> 1;
-  return slot < 64 ? 0 : slot - 63;
-}
-
-#define WS_STEP16(img, st, b) \
-  ((int32_t)(*reinterpret_cast<const int16_t*>(reinterpret_cast<const char*>(img) + (st) + (b) * (2 * kImg16Slots))))
-
-// A transition of the 16-bit walk that is not into a hot row, from the
-// class-indexed table: updates the state (the trap column for a cold row)
-// and returns the row of a match state (0xFFFFFFFF when none).
-__device__ __forceinline__ uint32_t slow16(uint32_t b, uint32_t& st, uint32_t& cold_row, uint32_t H, uint32_t lane4,
-                                          const uint8_t* cls_s, const uint32_t* tab, uint32_t C) {
-  const uint32_t row = row16_of_state(st, cold_row);
-  const uint32_t t = __ldg(tab + row * C + cls_s[b]);
-  const uint32_t n = t & F_MASK;
-  if (n < H && !(t & F_DEAD)) st = state16_of_row(n, lane4);
-  else { st = kTrap16; cold_row = n; }
-  return (t & F_MATCH) ? n : 0xFFFFFFFFu;
-}
-
-// The speculative walk over the 16-bit image (see dfa_walk_kernel): the same
-// steps with twice the hot rows in the same shared memory.
-template <int V>
-__global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk16_kernel(DevTables t, ScanPtrs p) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  const uint32_t g = blockIdx.x;
-  const GroupDev gd = t.groups[g];
-  uint16_t* img = reinterpret_cast<uint16_t*>(smem);
-  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(1);
-  {
-    uint64_t* bar = reinterpret_cast<uint64_t*>(cls_s + 256);
-    if (threadIdx.x == 0) {
-      mbar_init(bar, 1);
-      mbar_init_fence();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      mbar_expect_tx(bar, kImg16Entries * 2 + 256);
-      bulk_copy_g2s(img, t.hot16 + gd.hot16_off, kImg16Entries * 2, bar);
-      bulk_copy_g2s(cls_s, t.cls + g * 256, 256, bar);
-    }
-    bool ok = false;
-    for (uint32_t it = 0; it < (1u << 22) && !ok; ++it) ok = mbar_try(bar, 0);
-    if (!__syncthreads_and(ok)) {
-      if (threadIdx.x == 0) atomicOr(&p.ctr[C_ERR], kErrTimeout);
-      ok = false;
-      for (uint32_t it = 0; it < (1u << 22) && !ok; ++it) ok = mbar_try(bar, 0);
-      __syncthreads();
-      return;
-    }
-  }
-  const uint64_t i = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
-  if (i >= p.n_chunks) return;
-  const uint32_t* tab = t.fwd + gd.fwd_off;
-  const uint32_t C = gd.n_classes, H = gd.hot16_rows;
-  const int32_t lane4 = (int32_t)((threadIdx.x & 31) * 4);
-  const uint64_t q = (uint64_t)g * p.n_chunks + i;
-  const uint64_t c0 = i * p.chunk;
-  const uint64_t c1 = min(p.len, c0 + p.chunk);
-  uint32_t start = (i == 0) ? gd.start_unanchored : p.guess[q];
-  if (start >= gd.n_states) start = gd.start_unanchored;
-  p.used[q] = start;
-  p.conv[q] = (uint32_t)c0;
-  p.round[q] = 0;
-  uint32_t* ck = p.ckpt + q * p.nck;
-  uint32_t cold_row = 0;
-  uint32_t st = start < H ? state16_of_row(start, (uint32_t)lane4) : kTrap16;
-  if (start >= H) cold_row = start;
-  const uint64_t nfull = (c1 - c0) / 16;
-  auto load16 = [&](uint64_t k) -> uint4 {
-    if (k >= nfull) return make_uint4(0, 0, 0, 0);
-    const uint8_t* a = p.data + c0 + k * 16;
-    if (V & 2) return load_stream16(a);
-    return __ldg(reinterpret_cast<const uint4*>(a));
-  };
-  constexpr int kAhead = 4;
-  uint4 ring[kAhead];
-#pragma unroll
-  for (int a = 0; a < kAhead; ++a) ring[a] = load16(a);
-  for (uint64_t k16 = 0; k16 < nfull; ++k16) {
-    const uint4 cur = ring[0];
-    const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
-#pragma unroll
-    for (int a = 0; a < kAhead - 1; ++a) ring[a] = ring[a + 1];
-    ring[kAhead - 1] = load16(k16 + kAhead);
-    const uint32_t st0 = st, cold0 = cold_row;
-    int32_t acc = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
-      const int32_t w = WS_STEP16(img, st, b);
-      acc |= w;
-      st = (uint32_t)max(w, lane4);
-    }
-    if (acc < 0) {
-      st = st0;
-      cold_row = cold0;
-      for (int k = 0; k < 16; ++k) {
-        const uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-        const int32_t w = WS_STEP16(img, st, b);
-        if (w >= 0) {
-          st = (uint32_t)max(w, lane4);
-        } else {
-          const uint32_t m_row = slow16(b, st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
-          if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(c0 + k16 * 16 + k + 1), m_row, (uint32_t)q, 0);
-        }
-      }
-    }
-    const uint64_t done = (k16 + 1) * 16;
-    if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = row16_of_state(st, cold_row);
-  }
-  for (uint64_t pos = c0 + nfull * 16; pos < c1; ++pos) {
-    const uint32_t b = __ldg(p.data + pos);
-    const int32_t w = WS_STEP16(img, st, b);
-    if (w >= 0) {
-      st = (uint32_t)max(w, lane4);
-    } else {
-      const uint32_t m_row = slow16(b, st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
-      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
-    }
-  }
-  const uint32_t end_row = row16_of_state(st, cold_row);
-  p.end[q] = end_row;
-  p.spec[q] = end_row;
-}
-
 // Thread per (group, chunk): unanchored walk from the proposed start state,
 // recording the state every kCkpt bytes, the end state and every match event.
-// blockIdx.y = group; the group's hottest rows sit in shared memory.
-// V bit 0: slow words handled at the byte (else a careful re-walk of the
-// 16-byte block); V bit 1: input loads bypass L1.
-template <int V>
+// blockIdx.x = group; the group's hottest rows sit in shared memory.  The
+// input is read in 16-byte vectors, four ahead of the walk.
 __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, ScanPtrs p) {
   extern __shared__ __align__(16) uint32_t smem[];
   // blockIdx.x = group (fastest), so the groups' blocks over the same chunks
@@ -614,119 +452,55 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
   uint32_t* ck = p.ckpt + q * p.nck;
   uint32_t cold_row = 0;
   uint32_t st = state_of(start, 0, H, (uint32_t)lane4, &cold_row);
-  const uint64_t nfull = (c1 - c0) / 16;
-  auto load16 = [&](uint64_t k) -> uint4 {
-    const uint8_t* a = p.data + c0 + k * 16;
-    if (V & 2) return load_stream16(a);
-    return __ldg(reinterpret_cast<const uint4*>(a));
-  };
-  // four 16-byte vectors in flight ahead of the walk
-  constexpr int kAhead = 4;
-  uint4 ring[kAhead];
+  // One 16-byte block: an optimistic pass over fast entries only (a slow word
+  // is negative: it sends the walk to the first row, in bounds, and marks the
+  // block), then, for a marked block, a careful pass for match events and
+  // cold rows.
+  auto block16 = [&](const uint32_t* words, uint64_t at) {
+    const uint32_t st0 = st, cold0 = cold_row;
+    uint32_t acc = 0;
 #pragma unroll
-  for (int a = 0; a < kAhead; ++a) ring[a] = (uint64_t)a < nfull ? load16(a) : make_uint4(0, 0, 0, 0);
-  for (uint64_t k16 = 0; k16 < nfull; ++k16) {
-    const uint4 cur = ring[0];
-    const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
-#pragma unroll
-    for (int a = 0; a < kAhead - 1; ++a) ring[a] = ring[a + 1];
-    ring[kAhead - 1] = (k16 + kAhead < nfull) ? load16(k16 + kAhead) : make_uint4(0, 0, 0, 0);
-    if (V & 1) {
-      // every byte: a fast entry (the next row's column) or, rarely, the slow
-      // path for a match, cold or dead transition
-#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
+      uint32_t w = WS_STEP_FAST(img, st, b);
+      acc |= w;
+      st = (uint32_t)max((int32_t)w, lane4);
+    }
+    if ((int32_t)acc < 0) {
+      st = st0;
+      cold_row = cold0;
       for (int k = 0; k < 16; ++k) {
-        uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
+        uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
         uint32_t w = WS_STEP_FAST(img, st, b);
         if ((int32_t)w >= 0) {
           st = (uint32_t)max((int32_t)w, lane4);
         } else {
           uint32_t m_row;
           slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
-          if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(c0 + k16 * 16 + k + 1), m_row, (uint32_t)q, 0);
+          if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + k + 1), m_row, (uint32_t)q, 0);
         }
       }
-    } else {
-      // optimistic pass: fast entries only; a slow word (negative) sends the
-      // walk to the first row (in bounds) and marks the block for the careful
-      // pass
-      const uint32_t st0 = st, cold0 = cold_row;
-      uint32_t acc = 0;
+    }
+  };
+  const uint64_t nvec = (c1 - c0) / 16;
+  auto load16 = [&](uint64_t k) -> uint4 {
+    return k < nvec ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + k * 16)) : make_uint4(0, 0, 0, 0);
+  };
+  constexpr int kAhead = 4;
+  uint4 ring[kAhead];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
-        uint32_t w = WS_STEP_FAST(img, st, b);
-        acc |= w;
-        st = (uint32_t)max((int32_t)w, lane4);
-      }
-      if ((int32_t)acc < 0) {
-        // careful pass over the same 16 bytes: match events, cold rows
-        st = st0;
-        cold_row = cold0;
-        for (int k = 0; k < 16; ++k) {
-          uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-          uint32_t w = WS_STEP_FAST(img, st, b);
-          if ((int32_t)w >= 0) {
-            st = (uint32_t)max((int32_t)w, lane4);
-          } else {
-            uint32_t m_row;
-            slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
-            if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(c0 + k16 * 16 + k + 1), m_row, (uint32_t)q, 0);
-          }
-        }
-      }
-    }
-    const uint64_t done = (k16 + 1) * 16;
-    if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = row_of(st, cold_row, 0);
-  }
-  for (uint64_t pos = c0 + nfull * 16; pos < c1; ++pos) {
-    uint32_t b = __ldg(p.data + pos);
-    uint32_t w = WS_STEP_FAST(img, st, b);
-    if ((int32_t)w >= 0) {
-      st = (uint32_t)max((int32_t)w, lane4);
-    } else {
-      uint32_t m_row;
-      slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
-      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
-    }
-  }
-  const uint32_t end_row = row_of(st, cold_row, 0);
-  p.end[q] = end_row;
-  p.spec[q] = end_row;
-}
-
-// The careful walk of one 16-byte block of a chunk (match events, cold rows).
-__device__ __forceinline__ void careful_block(const ScanPtrs& p, const uint32_t* img, const uint8_t* cls_s,
-                                              const uint32_t* tab, uint32_t C, uint32_t H, int32_t lane4,
-                                              const uint32_t (&words)[4], uint64_t at, uint64_t q, uint32_t& st,
-                                              uint32_t& cold_row) {
-  for (int k = 0; k < 16; ++k) {
-    uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-    uint32_t w = WS_STEP_FAST(img, st, b);
-    if ((int32_t)w >= 0) {
-      st = (uint32_t)max((int32_t)w, lane4);
-    } else {
-      uint32_t m_row;
-      slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
-      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + k + 1), m_row, (uint32_t)q, 0);
-    }
-  }
-}
-
-// The remaining blocks and tail bytes of one chunk, then its end state.
-__device__ __forceinline__ void walk_rest(const ScanPtrs& p, const uint32_t* img, const uint8_t* cls_s,
-                                          const uint32_t* tab, uint32_t C, uint32_t H, int32_t lane4, uint64_t q,
-                                          uint64_t c0, uint64_t c1, uint64_t from, uint32_t st, uint32_t cold_row) {
-  uint32_t* ck = p.ckpt + q * p.nck;
-  const uint64_t nfull = (c1 - c0) / 16;
-  for (uint64_t k = from; k < nfull; ++k) {
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + c0 + k * 16));
-    const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
-    careful_block(p, img, cls_s, tab, C, H, lane4, w4, c0 + k * 16, q, st, cold_row);
+  for (int a = 0; a < kAhead; ++a) ring[a] = load16((uint64_t)a);
+  for (uint64_t k = 0; k < nvec; ++k) {
+    const uint4 cur = ring[0];
+    const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+    for (int a = 0; a < kAhead - 1; ++a) ring[a] = ring[a + 1];
+    ring[kAhead - 1] = load16(k + kAhead);
+    block16(words, c0 + k * 16);
     const uint64_t done = (k + 1) * 16;
     if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = row_of(st, cold_row, 0);
   }
-  for (uint64_t pos = c0 + nfull * 16; pos < c1; ++pos) {
+  for (uint64_t pos = c0 + nvec * 16; pos < c1; ++pos) {
     uint32_t b = __ldg(p.data + pos);
     uint32_t w = WS_STEP_FAST(img, st, b);
     if ((int32_t)w >= 0) {
@@ -740,108 +514,6 @@ __device__ __forceinline__ void walk_rest(const ScanPtrs& p, const uint32_t* img
   const uint32_t end_row = row_of(st, cold_row, 0);
   p.end[q] = end_row;
   p.spec[q] = end_row;
-}
-
-// Two chunks per thread (2t and 2t + 1), their walks interleaved byte by
-// byte so that each thread keeps two independent lookup chains in flight;
-// otherwise the walk of dfa_walk_kernel (careful re-walk of a 16-byte block
-// with a slow word).  V bit 1: input loads bypass L1.
-template <int V>
-__global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk2_kernel(DevTables t, ScanPtrs p) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  const uint32_t g = blockIdx.x;
-  const GroupDev gd = t.groups[g];
-  uint32_t* img = smem;
-  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.hot_rows);
-  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR])) return;
-  const uint64_t tid = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
-  const uint32_t* tab = t.fwd + gd.fwd_off;
-  const uint32_t C = gd.n_classes, H = gd.hot_rows;
-  const int32_t lane4 = (int32_t)((threadIdx.x & 31) * 4);
-  const uint64_t ia = 2 * tid, ib = ia + 1;
-  if (ia >= p.n_chunks) return;
-  const bool hb = ib < p.n_chunks;
-  const uint64_t qa = (uint64_t)g * p.n_chunks + ia, qb = qa + 1;
-  const uint64_t c0a = ia * p.chunk, c1a = min(p.len, c0a + p.chunk);
-  const uint64_t c0b = ib * p.chunk, c1b = hb ? min(p.len, c0b + p.chunk) : c0b;
-  uint32_t cola = 0, colb = 0;
-  uint32_t sta, stb = 0;
-  {
-    uint32_t s = (ia == 0) ? gd.start_unanchored : p.guess[qa];
-    if (s >= gd.n_states) s = gd.start_unanchored;
-    p.used[qa] = s;
-    p.conv[qa] = (uint32_t)c0a;
-    p.round[qa] = 0;
-    sta = state_of(s, 0, H, (uint32_t)lane4, &cola);
-  }
-  if (hb) {
-    uint32_t s = p.guess[qb];
-    if (s >= gd.n_states) s = gd.start_unanchored;
-    p.used[qb] = s;
-    p.conv[qb] = (uint32_t)c0b;
-    p.round[qb] = 0;
-    stb = state_of(s, 0, H, (uint32_t)lane4, &colb);
-  }
-  const uint64_t nfa = (c1a - c0a) / 16, nfb = (c1b - c0b) / 16;
-  auto load16 = [&](uint64_t c0, uint64_t nf, uint64_t k) -> uint4 {
-    if (k >= nf) return make_uint4(0, 0, 0, 0);
-    const uint8_t* a = p.data + c0 + k * 16;
-    if (V & 2) return load_stream16(a);
-    return __ldg(reinterpret_cast<const uint4*>(a));
-  };
-  uint32_t* cka = p.ckpt + qa * p.nck;
-  uint32_t* ckb = p.ckpt + qb * p.nck;
-  constexpr int kAhead = 2;
-  uint4 ra[kAhead], rb[kAhead];
-#pragma unroll
-  for (int a = 0; a < kAhead; ++a) {
-    ra[a] = load16(c0a, nfa, a);
-    rb[a] = load16(c0b, nfb, a);
-  }
-  const uint64_t both = min(nfa, nfb);
-  uint64_t k16 = 0;
-  for (; k16 < both; ++k16) {
-    const uint4 ca = ra[0], cb = rb[0];
-    const uint32_t wa[4] = {ca.x, ca.y, ca.z, ca.w}, wb[4] = {cb.x, cb.y, cb.z, cb.w};
-#pragma unroll
-    for (int a = 0; a < kAhead - 1; ++a) {
-      ra[a] = ra[a + 1];
-      rb[a] = rb[a + 1];
-    }
-    ra[kAhead - 1] = load16(c0a, nfa, k16 + kAhead);
-    rb[kAhead - 1] = load16(c0b, nfb, k16 + kAhead);
-    const uint32_t sa0 = sta, ca0 = cola, sb0 = stb, cb0 = colb;
-    uint32_t acca = 0, accb = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const uint32_t ba = __byte_perm(wa[k >> 2], 0, 0x4440 + (k & 3));
-      const uint32_t bb = __byte_perm(wb[k >> 2], 0, 0x4440 + (k & 3));
-      const uint32_t xa = WS_STEP_FAST(img, sta, ba);
-      const uint32_t xb = WS_STEP_FAST(img, stb, bb);
-      acca |= xa;
-      accb |= xb;
-      sta = (uint32_t)max((int32_t)xa, lane4);
-      stb = (uint32_t)max((int32_t)xb, lane4);
-    }
-    if ((int32_t)acca < 0) {
-      sta = sa0;
-      cola = ca0;
-      careful_block(p, img, cls_s, tab, C, H, lane4, wa, c0a + k16 * 16, qa, sta, cola);
-    }
-    if ((int32_t)accb < 0) {
-      stb = sb0;
-      colb = cb0;
-      careful_block(p, img, cls_s, tab, C, H, lane4, wb, c0b + k16 * 16, qb, stb, colb);
-    }
-    const uint64_t done = (k16 + 1) * 16;
-    if ((done % kCkpt) == 0) {
-      cka[done / kCkpt - 1] = row_of(sta, cola, 0);
-      ckb[done / kCkpt - 1] = row_of(stb, colb, 0);
-    }
-  }
-  // the rest of each chunk on its own (only the input's last chunks differ)
-  walk_rest(p, img, cls_s, tab, C, H, lane4, qa, c0a, c1a, k16, sta, cola);
-  if (hb) walk_rest(p, img, cls_s, tab, C, H, lane4, qb, c0b, c1b, k16, stb, colb);
 }
 
 // One chunk of a fix-up round: re-walk from the predecessor's end state until
@@ -888,12 +560,87 @@ __device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uin
   }
 }
 
-__global__ void __launch_bounds__(256) dfa_fixup_kernel(DevTables t, ScanPtrs p, int round) {
+// fix_chunk over the group's hot-row image in shared memory (the walk's own
+// steps: a shared-memory lookup per byte, the class-indexed table in L2 only
+// for cold rows), so that a re-walk is not a chain of L2 round trips.  The
+// input is 16-byte aligned and chunks start at multiples of kCkpt.
+__device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const GroupDev& gd, const uint32_t* img,
+                              const uint8_t* cls_s, uint32_t g, uint64_t i, uint32_t tag,
+                              unsigned long long* changed, uint32_t lane4) {
+  const uint64_t q = (uint64_t)g * p.n_chunks + i;
+  volatile uint32_t* endv = p.end;
+  const uint32_t S = endv[q - 1];
+  if (S == p.used[q]) return;
+  const uint32_t* tab = t.fwd + gd.fwd_off;
+  const uint32_t C = gd.n_classes, H = gd.hot_rows;
+  const uint64_t c0 = i * p.chunk;
+  const uint64_t c1 = min(p.len, c0 + p.chunk);
+  const uint32_t* ck = p.ckpt + q * p.nck;
+  uint32_t cold_row = 0;
+  uint32_t st = state_of(S, 0, H, lane4, &cold_row);
+  auto step = [&](uint32_t b, uint64_t at) {
+    const uint32_t w = WS_STEP_FAST(img, st, b);
+    if ((int32_t)w >= 0) {
+      st = (uint32_t)max((int32_t)w, (int32_t)lane4);
+    } else {
+      uint32_t m_row;
+      slow_step(w, b, st, cold_row, 0, H, lane4, cls_s, tab, C, m_row);
+      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + 1), m_row, (uint32_t)q, tag);
+    }
+  };
+  uint64_t pos = c0;
+  bool converged = false;
+  uint64_t conv = c1;
+  for (uint64_t k = 0; pos < c1; ++k) {
+    const uint64_t stop = min(c1, c0 + (k + 1) * kCkpt);
+    for (; pos + 16 <= stop; pos += 16) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + pos));
+      const uint32_t wd[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int j = 0; j < 16; ++j) step((wd[j >> 2] >> (8 * (j & 3))) & 0xFFu, pos + j);
+    }
+    for (; pos < stop; ++pos) step(__ldg(p.data + pos), pos);
+    if (stop == c0 + (k + 1) * kCkpt && k < p.nck && row_of(st, cold_row, 0) == ck[k]) {
+      converged = true;
+      conv = stop;
+      break;
+    }
+  }
+  p.used[q] = S;
+  p.round[q] = tag;
+  p.conv[q] = (uint32_t)conv;
+  atomicAdd(&p.ctr[C_FIX], 1ull);
+  atomicAdd(&p.ctr[C_REWALK], (unsigned long long)(conv - c0));
+  const uint32_t new_end = converged ? p.spec[q] : row_of(st, cold_row, 0);
+  if (new_end != endv[q]) {
+    endv[q] = new_end;
+    atomicOr(changed, 1ull);
+  }
+}
+
+// One parallel fix-up round: blocks per group (blockIdx.x = group, as in the
+// walk), each over a strided share of the group's chunks.  A block stages the
+// hot-row image only when one of its chunks was walked from a start that
+// differs from its predecessor's end.
+__global__ void __launch_bounds__(kWalkThreads, 1) dfa_fixup_kernel(DevTables t, ScanPtrs p, int round) {
   if (round > 0 && p.ctr[C_ROUND + round - 1] == 0) return;  // nothing changed last round
-  const uint32_t g = blockIdx.y;
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i >= p.n_chunks) return;
-  fix_chunk(t, p, g, i, (uint32_t)round + 1, &p.ctr[C_ROUND + round]);
+  extern __shared__ __align__(16) uint32_t smem[];
+  const uint32_t g = blockIdx.x;
+  const uint64_t first = 1 + (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.y * blockDim.x;
+  bool need = false;
+  for (uint64_t i = first; i < p.n_chunks && !need; i += stride) {
+    const uint64_t q = (uint64_t)g * p.n_chunks + i;
+    need = p.end[q - 1] != p.used[q];
+  }
+  if (!__syncthreads_or(need)) return;
+  const GroupDev gd = t.groups[g];
+  uint32_t* img = smem;
+  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.hot_rows);
+  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR])) return;
+  const uint32_t lane4 = (threadIdx.x & 31) * 4;
+  for (uint64_t i = first; i < p.n_chunks; i += stride)
+    fix_chunk_img(t, p, gd, img, cls_s, g, i, (uint32_t)round + 1, &p.ctr[C_ROUND + round], lane4);
 }
 
 // Final sweep, one thread per group, in chunk order: exact whatever happened
@@ -1234,7 +981,6 @@ DevTables dev_tables(const RegexPlan& P) {
   t.groups = P.d_groups.as<GroupDev>();
   t.fwd = P.d_fwd.as<uint32_t>();
   t.hot = P.d_hot.as<uint32_t>();
-  t.hot16 = P.d_hot16.as<uint16_t>();
   t.rev = P.d_rev.as<uint32_t>();
   t.lf = P.d_lf.as<uint32_t>();
   t.cls = P.d_cls.as<uint8_t>();
@@ -1315,51 +1061,18 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
   }
   mark(1);
   size_t smem = hot_smem_bytes(max_rows(P, false));
-  static const int variant = getenv("WS_WALK_VARIANT") ? atoi(getenv("WS_WALK_VARIANT")) : 0;
-  switch (variant) {
-#define WS_WALK_CASE(v)                                                    \
-    case v:                                                                \
-      set_smem(dfa_walk_kernel<v>, smem, "smem(walk)");                    \
-      dfa_walk_kernel<v><<<cgrid, kWalkThreads, smem, st>>>(t, p);         \
-      break;
-    WS_WALK_CASE(1) WS_WALK_CASE(2) WS_WALK_CASE(3)
-    case 8: case 10: {
-      bool any16 = false;
-      for (uint32_t g = 0; g < P.n_spec; ++g) any16 |= P.groups[g].hot16_rows != 0;
-      if (any16) {
-        const size_t smem16 = hot_smem_bytes(1);
-        if (variant == 8) {
-          set_smem(dfa_walk16_kernel<0>, smem16, "smem(walk16)");
-          dfa_walk16_kernel<0><<<cgrid, kWalkThreads, smem16, st>>>(t, p);
-        } else {
-          set_smem(dfa_walk16_kernel<2>, smem16, "smem(walk16)");
-          dfa_walk16_kernel<2><<<cgrid, kWalkThreads, smem16, st>>>(t, p);
-        }
-        break;
-      }
-      set_smem(dfa_walk_kernel<0>, smem, "smem(walk)");
-      dfa_walk_kernel<0><<<cgrid, kWalkThreads, smem, st>>>(t, p);
-      break;
-    }
-    case 4: case 6: {
-      dim3 g2(P.n_spec, (unsigned)(((p.n_chunks + 1) / 2 + kWalkThreads - 1) / kWalkThreads));
-      if (variant == 4) {
-        set_smem(dfa_walk2_kernel<0>, smem, "smem(walk2)");
-        dfa_walk2_kernel<0><<<g2, kWalkThreads, smem, st>>>(t, p);
-      } else {
-        set_smem(dfa_walk2_kernel<2>, smem, "smem(walk2)");
-        dfa_walk2_kernel<2><<<g2, kWalkThreads, smem, st>>>(t, p);
-      }
-      break;
-    }
-    default: WS_WALK_CASE(0)
-  }
+  set_smem(dfa_walk_kernel, smem, "smem(walk)");
+  dfa_walk_kernel<<<cgrid, kWalkThreads, smem, st>>>(t, p);
   check_cuda(cudaGetLastError(), "dfa_walk_kernel");
   launches++;
   mark(2);
-  dim3 fgrid((unsigned)((p.n_chunks + 255) / 256), P.n_spec);
+  // one wave of fix-up blocks (one per SM, the walk's shared memory)
+  const uint64_t fper = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count / P.n_spec,
+                                                                  (p.n_chunks + kWalkThreads - 1) / kWalkThreads));
+  dim3 fgrid(P.n_spec, (unsigned)fper);
+  set_smem(dfa_fixup_kernel, smem, "smem(fixup)");
   for (int r = 0; r < kFixRounds; ++r) {
-    dfa_fixup_kernel<<<fgrid, 256, 0, st>>>(t, p, r);
+    dfa_fixup_kernel<<<fgrid, kWalkThreads, smem, st>>>(t, p, r);
     check_cuda(cudaGetLastError(), "dfa_fixup_kernel");
     launches++;
   }
@@ -1452,7 +1165,7 @@ void rank_states(GroupBuild& gb) {
   for (int s = 1; s < n; ++s) (in_u[(size_t)s] ? us : as).push_back((uint32_t)s);
   std::stable_sort(us.begin(), us.end(), [&](uint32_t a, uint32_t b) { return pu[a] > pu[b]; });
   std::stable_sort(as.begin(), as.end(), [&](uint32_t a, uint32_t b) { return pa[a] > pa[b]; });
-  gb.n_hot_u = (uint32_t)std::min<size_t>(us.size(), kHotRows16);
+  gb.n_hot_u = (uint32_t)std::min<size_t>(us.size(), kHotRows);
   gb.n_hot_a = (uint32_t)std::min<size_t>(as.size(), kHotRows);
   std::vector<uint32_t> order;
   order.insert(order.end(), us.begin(), us.begin() + gb.n_hot_u);
@@ -1525,7 +1238,7 @@ uint32_t append_trans(const Dfa& d, std::vector<uint32_t>& dst) {
 // Builds the forward tables of every group from P.fdfa (class-indexed words,
 // 16-bit byte-indexed hot rows, match lists) and uploads them.
 void layout_forward(RegexPlan& P) {
-  P.fwd.clear(); P.hot.clear(); P.hot16.clear(); P.mptr.clear(); P.mlist.clear();
+  P.fwd.clear(); P.hot.clear(); P.mptr.clear(); P.mlist.clear();
   P.total_states = 0;
   P.max_classes = 0;
   for (uint32_t g = 0; g < P.n_groups; ++g) {
@@ -1560,26 +1273,8 @@ void layout_forward(RegexPlan& P) {
       return off;
     };
     const bool spec = g < P.n_spec;
-    gd.hot_rows = fits && spec ? std::min(P.nhot_u[g], kHotRows) : 0;
+    gd.hot_rows = fits && spec ? P.nhot_u[g] : 0;
     gd.hot_off = image(0, gd.hot_rows);
-    // the 16-bit image of the unanchored hot rows (dfa_walk16_kernel)
-    gd.hot16_rows = fits && spec ? P.nhot_u[g] : 0;
-    gd.hot16_off = (uint32_t)P.hot16.size();
-    if (gd.hot16_rows) {
-      P.hot16.resize(P.hot16.size() + kImg16Entries, (uint16_t)0xFFFF);
-      uint16_t* img = P.hot16.data() + gd.hot16_off;
-      for (uint32_t r = 0; r < gd.hot16_rows; ++r)
-        for (int b = 0; b < 256; ++b) {
-          const uint32_t w = d.trans[(size_t)r * C + bc.map[b]];
-          const uint32_t n = w & DFA_MASK_STATE;
-          const bool fast = !(w & (DFA_FLAG_MATCH | DFA_FLAG_DEAD)) && n < gd.hot16_rows;
-          const uint16_t e = fast ? (uint16_t)state16_of_row(n, 0) : (uint16_t)0xFFFF;
-          if (r == 0)
-            for (uint32_t l = 0; l < 32; ++l) img[(size_t)b * kImg16Slots + 2 * l] = e;
-          else
-            img[(size_t)b * kImg16Slots + slot16_of_row(r)] = e;
-        }
-    }
     gd.ahot_base = P.nhot_u[g];
     gd.ahot_rows = fits && spec ? P.nhot_a[g] : 0;
     gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows);
@@ -1601,10 +1296,8 @@ void layout_forward(RegexPlan& P) {
   P.d_fwd.upload(P.fwd.data(), P.fwd.size() * 4);
   // sets whose groups all carry context have no hot image: the buffers still exist
   if (P.hot.size() < 4) P.hot.resize(4, 0);
-  if (P.hot16.size() < 8) P.hot16.resize(8, 0);
   if (P.mlist.empty()) P.mlist.push_back(0);
   P.d_hot.upload(P.hot.data(), P.hot.size() * 4);
-  P.d_hot16.upload(P.hot16.data(), P.hot16.size() * 2);
   P.d_mptr.upload(P.mptr.data(), P.mptr.size() * 4);
   P.d_mlist.upload(P.mlist.data(), P.mlist.size() * 4);
 }
@@ -1814,7 +1507,7 @@ void regex_rerank_from_corpus(RegexPlan& P, const uint8_t* d_corpus, uint64_t le
     std::stable_sort(us.begin(), us.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
     (void)hu;
     std::vector<uint32_t> order;
-    uint32_t nu = (uint32_t)std::min<size_t>(us.size(), kHotRows16);
+    uint32_t nu = (uint32_t)std::min<size_t>(us.size(), kHotRows);
     order.insert(order.end(), us.begin(), us.begin() + nu);
     order.insert(order.end(), as.begin(), as.begin() + std::min<size_t>(as.size(), ha));
     order.insert(order.end(), us.begin() + nu, us.end());

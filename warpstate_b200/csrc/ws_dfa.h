@@ -32,9 +32,6 @@ namespace ws {
 // Hot rows staged per group in shared memory (a 224 KiB image: the first row
 // replicated per lane, 191 more rows column-interleaved; see ws_dfa.cu).
 constexpr uint32_t kHotRows = 192;
-// Hot rows of the 16-bit unanchored image (see ws_dfa.cu): the first row
-// replicated per lane, 383 more.
-constexpr uint32_t kHotRows16 = 384;
 
 struct GroupDev {
   uint32_t fwd_off;          // class-indexed forward table (u32 words)
@@ -49,8 +46,6 @@ struct GroupDev {
   // context, and match lists per (row, right context) at mptr[4 * row + k].
   uint32_t context;
   uint32_t cstart[4];
-  uint32_t hot16_off, hot16_rows;             // 16-bit unanchored image: rows [0, hot16_rows)
-  uint32_t pad[2];
 };
 
 struct Proposer;
@@ -83,8 +78,6 @@ struct RegexPlan {
   // assertions
   std::vector<uint32_t> lfx;
   std::vector<uint32_t> hot;   // shared-memory images, one per (group, part)
-  std::vector<uint16_t> hot16; // 16-bit unanchored images, one per group
-  DeviceBuffer d_hot16;
   std::vector<uint8_t> cls;
   // host forward DFAs per group (their numbering defines the layout above)
   std::vector<Dfa> fdfa;

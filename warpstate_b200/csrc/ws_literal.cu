@@ -28,7 +28,6 @@
 // The output is contract L: every overlapping occurrence of every literal.
 #include <cuda_runtime.h>
 
-#include <cstdlib>
 
 #include "ws_internal.h"
 
@@ -592,46 +591,16 @@ struct LeanGrams {
   uint32_t n[4], bw[4];
 };
 
-// L2 eviction policies: the input streams through L2 once (evict first), the
-// stage-1b table should stay (evict last).
-__device__ __forceinline__ uint64_t l2_evict_first() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ uint64_t l2_evict_last() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-// 16 input bytes, not kept in L1, evict-first in L2.
-__device__ __forceinline__ uint4 ld_stream16(const void* ptr, uint64_t pol) {
-  uint4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(ptr), "l"(pol));
-  return v;
-}
-// One byte of a table that should stay in L2.
-__device__ __forceinline__ uint32_t ld_keep8(const uint8_t* ptr, uint64_t pol) {
-  unsigned short v;
-  asm volatile("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(ptr), "l"(pol));
-  return v;
-}
-
 // Stage 1 of a lane's four aligned grams from the byte table in shared memory
 // (top kFilter8Bits bits of the hash); the stage-1b loads from the byte table
 // in L2 (top kBigBits bits) are issued for the grams that pass.
-template <bool kHint>
-__device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g,
-                                           uint64_t keep) {
+__device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint32_t hf = w[q] * 0x9E3779B1u;
     g.n[q] = filt[hf >> (32 - kFilter8Bits)];
-    const uint8_t* at = big + (hf >> (32 - kBigBits));
-    g.bw[q] = g.n[q] ? (kHint ? ld_keep8(at, keep) : (uint32_t)__ldg(at)) : 0u;
+    g.bw[q] = g.n[q] ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
   }
 }
 
@@ -702,7 +671,6 @@ __device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, cons
   }
 }
 
-template <bool kHint>
 __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a) {
   constexpr uint32_t W = kLeanThreads / 32, V = kLeanVecs;
   extern __shared__ __align__(16) uint8_t smem8[];
@@ -722,12 +690,10 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
   const uint32_t nw = gridDim.x * W;
   const uint8_t* big = a.big;
   const uint4 zero = make_uint4(0, 0, 0, 0);
-  const uint64_t stream_pol = kHint ? l2_evict_first() : 0, keep_pol = kHint ? l2_evict_last() : 0;
   // half h of warp step blk: the 512 coalesced bytes at (blk * V + h) * 512
   auto load = [&](uint32_t blk, uint32_t h) -> uint4 {
     const uint32_t v = (blk * V + h) * 32 + lane;
-    const uint4 x = v < full_vecs ? (kHint ? ld_stream16(reinterpret_cast<const uint4*>(a.data) + v, stream_pol)
-                                           : __ldg(reinterpret_cast<const uint4*>(a.data) + v))
+    const uint4 x = v < full_vecs ? __ldg(reinterpret_cast<const uint4*>(a.data) + v)
                     : v < nvec ? load_vec(a.data, a.len, v) : zero;
     return a.fold ? fold16(x) : x;
   };
@@ -740,7 +706,7 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
 #pragma unroll
   for (uint32_t h = 0; h < V; ++h) {
     vn[h] = b + nw < nblk ? load(b + nw, h) : zero;
-    if (b < nblk) lean_issue<kHint>(filt, big, load(b, h), gc[h], keep_pol);
+    if (b < nblk) lean_issue(filt, big, load(b, h), gc[h]);
   }
   for (; b < nblk; b += nw) {
     const uint32_t b1 = b + nw, b2 = b1 + nw;
@@ -750,7 +716,7 @@ __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a
 #pragma unroll
     for (uint32_t h = 0; h < V; ++h) {
       vn2[h] = b2 < nblk ? load(b2, h) : zero;
-      if (b1 < nblk) lean_issue<kHint>(filt, big, vn[h], gn[h], keep_pol);
+      if (b1 < nblk) lean_issue(filt, big, vn[h], gn[h]);
       base[h] = (b * V + h) * 512 + lane * 16;
       mask[h] = lean_finish(gc[h], base[h], len);
     }
@@ -860,11 +826,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   if (lg && !sh && a.big && a.filter8 && plan.period == 4 && plan.gram_len == 4) {
     a.verify_bloom = 1;
     const size_t lsmem = (size_t)1 << kFilter8Bits;
-    static const int variant = getenv("WS_LIT_VARIANT") ? atoi(getenv("WS_LIT_VARIANT")) : 0;
-    auto lean = variant & 1 ? literal_lean_kernel<true> : literal_lean_kernel<false>;
-    check_cuda(cudaFuncSetAttribute(lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
+    check_cuda(cudaFuncSetAttribute(literal_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
                "cudaFuncSetAttribute(literal lean)");
-    lean<<<sm_count, kLeanThreads, lsmem, st>>>(a);
+    literal_lean_kernel<<<sm_count, kLeanThreads, lsmem, st>>>(a);
     check_cuda(cudaGetLastError(), "literal_lean_kernel launch");
   } else if (lg && sh && a.big && plan.period == 4 && plan.gram_len == 4) {
     run_big(literal_filter_big_kernel<4, true>);
