@@ -1,5 +1,7 @@
 // Regex DFA path for sm_100a (see ws_dfa.h for the pipeline).
 #include <cooperative_groups.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -135,6 +137,7 @@ struct ScanPtrs {
   uint32_t* lfend;
   unsigned long long* rmark;    // visited reverse-walk triples, or null (state numbers too large, or full K)
   uint32_t full_k;              // report every (start, end) of K, not only distinct starts (diagnostics)
+  uint32_t count_guesses;       // profiled speculative scans: the speculative groups whose guesses are counted
   uint64_t n_chunks, chunk, nck;
   ws_match* out;
   uint64_t out_cap;
@@ -169,6 +172,7 @@ ScanPtrs make_ptrs(const RxLayout& L, void* base, const RegexLaunch& l) {
   p.lfend = reinterpret_cast<uint32_t*>(b + L.off_lfend);
   p.rmark = reinterpret_cast<unsigned long long*>(b + L.off_rmark);
   p.full_k = 0;
+  p.count_guesses = 0;
   p.n_chunks = L.n_chunks;
   p.chunk = L.chunk;
   p.nck = L.nck;
@@ -229,6 +233,20 @@ __host__ __device__ constexpr size_t hot_smem_bytes(uint32_t rows) {
 }
 __host__ __device__ constexpr size_t cls_offset(uint32_t rows) { return rows ? (size_t)kImgWords * 4 : 0; }
 
+// The speculative walk and the fix-up stage the first kWalkImgBlocks blocks
+// of the unanchored image (its hot rows are at most kHotRowsWalk, all in those
+// blocks); the walk block's shared memory is
+//   [image, 192 KiB][input stages: per warp 2 x 512 B][classes, 256 B]
+//   [image mbarrier, 16 B][stage mbarriers: per warp 2 x 8 B].
+constexpr uint32_t kWalkImgBlocks = 6;
+constexpr uint32_t kWalkImgBytes = kWalkImgBlocks * kImgBlock * 4;
+constexpr uint32_t kWalkWarps = kWalkThreads / 32;
+constexpr uint32_t kWalkStage = 512;  // one warp's 16 bytes per lane (a 16 x 32 box of the chunk rows)
+constexpr uint32_t kWalkStageBytes = kWalkWarps * 2 * kWalkStage;
+constexpr size_t kWalkSmem = kWalkImgBytes + kWalkStageBytes + 256 + 16 + kWalkWarps * 2 * 8;
+constexpr size_t kFixSmem = kWalkImgBytes + 256 + 16;
+static_assert(kWalkSmem <= 232448, "walk block shared memory");
+
 __host__ __device__ __forceinline__ uint32_t slot_word(uint32_t r) { return (1 + (r >> 5)) * kImgBlock + (r & 31); }
 
 __device__ __forceinline__ uint32_t slot_byte(uint32_t r, uint32_t lane4) { return r == 0 ? lane4 : slot_word(r) * 4; }
@@ -256,7 +274,8 @@ __device__ __forceinline__ uint32_t state_of(uint32_t row, uint32_t first, uint3
 // `err`, waits once more (again bounded) for the copies it issued, and the
 // caller returns without walking (false); the scan then reports the timeout.
 __device__ __forceinline__ bool stage_hot(const DevTables& t, uint32_t g, uint32_t off, uint32_t rows,
-                                          uint32_t* img, uint8_t* cls_s, unsigned long long* err) {
+                                          uint32_t* img, uint8_t* cls_s, unsigned long long* err,
+                                          uint32_t img_bytes = kImgWords * 4) {
   uint64_t* bar = reinterpret_cast<uint64_t*>(cls_s + 256);
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
@@ -264,8 +283,8 @@ __device__ __forceinline__ bool stage_hot(const DevTables& t, uint32_t g, uint32
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_expect_tx(bar, (rows ? kImgWords * 4 : 0) + 256);
-    if (rows) bulk_copy_g2s(img, t.hot + off, kImgWords * 4, bar);
+    mbar_expect_tx(bar, (rows ? img_bytes : 0) + 256);
+    if (rows) bulk_copy_g2s(img, t.hot + off, img_bytes, bar);
     bulk_copy_g2s(cls_s, t.cls + g * 256, 256, bar);
   }
   bool ok = false;
@@ -425,30 +444,63 @@ __global__ void __launch_bounds__(256) dfa_context_kernel(DevTables t, ScanPtrs 
 // ------------------------------------------------------- speculative walk
 // Thread per (group, chunk): unanchored walk from the proposed start state,
 // recording the state every kCkpt bytes, the end state and every match event.
-// blockIdx.x = group; the group's hottest rows sit in shared memory.  The
-// input is read in 16-byte vectors, four ahead of the walk.
-__global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, ScanPtrs p) {
-  extern __shared__ __align__(16) uint32_t smem[];
+// blockIdx.x = group; the group's hottest rows sit in shared memory.
+//
+// Input staging: the 32 lanes of a warp walk 32 adjacent chunks, so a warp's
+// next 16 bytes per lane are a 16 x 32 box of the input seen as a 2-D tensor
+// of full chunks (rows of `chunk` bytes).  Lane 0 brings each box into one of
+// the warp's two shared-memory stages with a tensor copy (TMA) on the stage's
+// mbarrier, two steps ahead, and every lane reads its 16 bytes from there.
+// The input never passes through the load/store pipe, whose wavefronts the
+// hot-row lookups need; one 16-byte load per lane and step from 32 different
+// chunks would each take a wavefront and an L2 sector.  A lane whose chunk
+// is not a full one (the last, partial chunk) loads its bytes itself.
+__global__ void __launch_bounds__(kWalkThreads, 1)
+    dfa_walk_kernel(DevTables t, ScanPtrs p, const __grid_constant__ CUtensorMap rows, uint64_t n_full) {
+  extern __shared__ __align__(128) uint32_t smem[];
   // blockIdx.x = group (fastest), so the groups' blocks over the same chunks
   // run together and the input is read from HBM once, then from L2
   const uint32_t g = blockIdx.x;
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
-  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.hot_rows);
-  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR])) return;
-  const uint64_t i = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x;
-  if (i >= p.n_chunks) return;
+  uint8_t* stages = reinterpret_cast<uint8_t*>(smem) + kWalkImgBytes;
+  uint8_t* cls_s = stages + kWalkStageBytes;
+  uint64_t* sbar = reinterpret_cast<uint64_t*>(cls_s + 256 + 16);
+  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR], kWalkImgBytes)) return;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t wfirst = (uint64_t)blockIdx.y * blockDim.x + warp * 32;  // lane 0's chunk
+  if (wfirst >= p.n_chunks) return;  // the whole warp
+  const bool wtma = wfirst < n_full;  // the warp's boxes come by TMA
+  uint64_t* bar = sbar + warp * 2;
+  uint8_t* stg = stages + warp * 2 * kWalkStage;
+  const uint64_t K = p.chunk / 16;  // 16-byte steps of a full chunk
+  if (wtma && lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+    for (uint32_t s = 0; s < 2 && s < K; ++s) {
+      mbar_expect_tx(&bar[s], kWalkStage);
+      tma_load_2d(stg + s * kWalkStage, &rows, (int32_t)(s * 16), (int32_t)wfirst, &bar[s]);
+    }
+  }
+  __syncwarp();
+  const uint64_t i = wfirst + lane;
+  const bool active = i < p.n_chunks;
+  const bool own = i >= n_full;  // loads its own bytes (partial chunk) or, out of range, none
   const uint32_t* tab = t.fwd + gd.fwd_off;
   const uint32_t C = gd.n_classes, H = gd.hot_rows;
-  const int32_t lane4 = (int32_t)((threadIdx.x & 31) * 4);
+  const int32_t lane4 = (int32_t)(lane * 4);
   const uint64_t q = (uint64_t)g * p.n_chunks + i;
   const uint64_t c0 = i * p.chunk;
-  const uint64_t c1 = min(p.len, c0 + p.chunk);
-  uint32_t start = (i == 0) ? gd.start_unanchored : p.guess[q];
-  if (start >= gd.n_states) start = gd.start_unanchored;  // a guess never written
-  p.used[q] = start;
-  p.conv[q] = (uint32_t)c0;
-  p.round[q] = 0;
+  const uint64_t c1 = active ? min(p.len, c0 + p.chunk) : c0;
+  uint32_t start = gd.start_unanchored;
+  if (active) {
+    if (i != 0) start = p.guess[q];
+    if (start >= gd.n_states) start = gd.start_unanchored;  // a guess never written
+    p.used[q] = start;
+    p.conv[q] = (uint32_t)c0;
+    p.round[q] = 0;
+  }
   uint32_t* ck = p.ckpt + q * p.nck;
   uint32_t cold_row = 0;
   uint32_t st = state_of(start, 0, H, (uint32_t)lane4, &cold_row);
@@ -483,23 +535,42 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_walk_kernel(DevTables t, 
     }
   };
   const uint64_t nvec = (c1 - c0) / 16;
-  auto load16 = [&](uint64_t k) -> uint4 {
-    return k < nvec ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + k * 16)) : make_uint4(0, 0, 0, 0);
-  };
-  constexpr int kAhead = 4;
-  uint4 ring[kAhead];
-#pragma unroll
-  for (int a = 0; a < kAhead; ++a) ring[a] = load16((uint64_t)a);
-  for (uint64_t k = 0; k < nvec; ++k) {
-    const uint4 cur = ring[0];
+  // K steps for every lane of the warp (the stage protocol is warp-wide); a
+  // lane walks its own steps [0, nvec)
+  for (uint64_t k = 0; k < K; ++k) {
+    uint4 cur = make_uint4(0, 0, 0, 0);
+    if (wtma) {
+      const uint32_t s = (uint32_t)(k & 1);
+      bool ok = false;
+      for (uint32_t it = 0; it < (1u << 22) && !ok; ++it) ok = mbar_try(&bar[s], (uint32_t)(k >> 1) & 1u);
+      if (!__all_sync(0xFFFFFFFFu, ok)) {
+        // (should not happen) record the time-out, let the copies this warp
+        // issued land, and stop
+        if (lane == 0) {
+          atomicOr(&p.ctr[C_ERR], kErrTimeout);
+          for (uint64_t j = k; j < K && j < k + 2; ++j)
+            for (uint32_t it = 0; it < (1u << 22) && !mbar_try(&bar[j & 1], (uint32_t)(j >> 1) & 1u); ++it) {
+            }
+        }
+        __syncwarp();
+        return;
+      }
+      if (!own) cur = *reinterpret_cast<const uint4*>(stg + s * kWalkStage + lane * 16);
+      __syncwarp();  // every lane has read stage s
+      if (lane == 0 && k + 2 < K) {
+        fence_proxy_async_smem();
+        mbar_expect_tx(&bar[s], kWalkStage);
+        tma_load_2d(stg + s * kWalkStage, &rows, (int32_t)((k + 2) * 16), (int32_t)wfirst, &bar[s]);
+      }
+    }
+    if (k >= nvec) continue;
+    if (own) cur = __ldg(reinterpret_cast<const uint4*>(p.data + c0 + k * 16));
     const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
-#pragma unroll
-    for (int a = 0; a < kAhead - 1; ++a) ring[a] = ring[a + 1];
-    ring[kAhead - 1] = load16(k + kAhead);
     block16(words, c0 + k * 16);
     const uint64_t done = (k + 1) * 16;
     if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = row_of(st, cold_row, 0);
   }
+  if (!active) return;
   for (uint64_t pos = c0 + nvec * 16; pos < c1; ++pos) {
     uint32_t b = __ldg(p.data + pos);
     uint32_t w = WS_STEP_FAST(img, st, b);
@@ -588,24 +659,33 @@ __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const Group
       if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + 1), m_row, (uint32_t)q, tag);
     }
   };
-  uint64_t pos = c0;
+  // 16-byte vectors, four in flight ahead of the walk; the state is compared
+  // with the speculative walk's at every checkpoint
+  const uint64_t nvec = (c1 - c0) / 16;
+  auto load16 = [&](uint64_t k) -> uint4 {
+    return k < nvec ? __ldg(reinterpret_cast<const uint4*>(p.data + c0 + k * 16)) : make_uint4(0, 0, 0, 0);
+  };
+  uint4 ring[4] = {load16(0), load16(1), load16(2), load16(3)};
   bool converged = false;
   uint64_t conv = c1;
-  for (uint64_t k = 0; pos < c1; ++k) {
-    const uint64_t stop = min(c1, c0 + (k + 1) * kCkpt);
-    for (; pos + 16 <= stop; pos += 16) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + pos));
-      const uint32_t wd[4] = {v.x, v.y, v.z, v.w};
+  uint64_t k = 0;
+  for (; k < nvec; ++k) {
+    const uint32_t wd[4] = {ring[0].x, ring[0].y, ring[0].z, ring[0].w};
+    ring[0] = ring[1];
+    ring[1] = ring[2];
+    ring[2] = ring[3];
+    ring[3] = load16(k + 4);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) step((wd[j >> 2] >> (8 * (j & 3))) & 0xFFu, pos + j);
-    }
-    for (; pos < stop; ++pos) step(__ldg(p.data + pos), pos);
-    if (stop == c0 + (k + 1) * kCkpt && k < p.nck && row_of(st, cold_row, 0) == ck[k]) {
+    for (int j = 0; j < 16; ++j) step((wd[j >> 2] >> (8 * (j & 3))) & 0xFFu, c0 + k * 16 + j);
+    const uint64_t done = (k + 1) * 16;
+    if (done % kCkpt == 0 && done / kCkpt <= p.nck && row_of(st, cold_row, 0) == ck[done / kCkpt - 1]) {
       converged = true;
-      conv = stop;
+      conv = c0 + done;
       break;
     }
   }
+  if (!converged)
+    for (uint64_t pos = c0 + nvec * 16; pos < c1; ++pos) step(__ldg(p.data + pos), pos);
   p.used[q] = S;
   p.round[q] = tag;
   p.conv[q] = (uint32_t)conv;
@@ -636,8 +716,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_fixup_kernel(DevTables t,
   if (!__syncthreads_or(need)) return;
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
-  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + cls_offset(gd.hot_rows);
-  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR])) return;
+  uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + kWalkImgBytes;
+  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR], kWalkImgBytes)) return;
   const uint32_t lane4 = (threadIdx.x & 31) * 4;
   for (uint64_t i = first; i < p.n_chunks; i += stride)
     fix_chunk_img(t, p, gd, img, cls_s, g, i, (uint32_t)round + 1, &p.ctr[C_ROUND + round], lane4);
@@ -652,8 +732,34 @@ __global__ void dfa_fixup_serial_kernel(DevTables t, ScanPtrs p) {
     fix_chunk(t, p, g, i, (uint32_t)kFixRounds + 1, &p.ctr[C_ROUND + kFixRounds]);
 }
 
-// Valid match events -> reverse walk -> K candidates.
+// Profiled scans: how many chunk boundaries the guess the walk started from
+// was the predecessor's true end state (the fix-up has run).
+__device__ void count_guess_hits(const DevTables& t, const ScanPtrs& p) {
+  const uint64_t per = p.n_chunks - 1, total = (uint64_t)p.count_guesses * per;
+  unsigned long long hits = 0, seen = 0;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = (uint32_t)(x / per);
+    const uint64_t q = (uint64_t)g * p.n_chunks + x % per + 1;
+    uint32_t guess = p.guess[q];
+    if (guess >= t.groups[g].n_states) guess = t.groups[g].start_unanchored;
+    hits += guess == p.end[q - 1];
+    seen += 1;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    hits += __shfl_down_sync(0xFFFFFFFFu, hits, o);
+    seen += __shfl_down_sync(0xFFFFFFFFu, seen, o);
+  }
+  if ((threadIdx.x & 31) == 0 && seen) {
+    atomicAdd(&p.ctr[C_HITS], hits);
+    atomicAdd(&p.ctr[C_GUESSES], seen);
+  }
+}
+
+// Valid match events -> reverse walk -> K candidates (and, in profiled
+// speculative scans, the guess count).
 __global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs p) {
+  if (p.count_guesses && p.n_chunks > 1) count_guess_hits(t, p);
   unsigned long long n = p.ctr[C_EV];
   if (n > p.ev_cap) n = p.ev_cap;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -947,28 +1053,6 @@ __global__ void finalize_kernel(ScanPtrs p, unsigned long long* need) {
 
 // Counts the chunk boundaries whose guess (the proposer's, or the unanchored
 // start) was the true state: the predecessor's end state after the fix-up.
-__global__ void guess_hits_kernel(DevTables t, ScanPtrs p) {
-  const uint32_t g = blockIdx.y;
-  const GroupDev gd = t.groups[g];
-  unsigned long long hits = 0, total = 0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < p.n_chunks;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t q = (uint64_t)g * p.n_chunks + i;
-    uint32_t guess = p.guess[q];
-    if (guess >= gd.n_states) guess = gd.start_unanchored;
-    hits += guess == p.end[q - 1];
-    total += 1;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    hits += __shfl_down_sync(0xFFFFFFFFu, hits, o);
-    total += __shfl_down_sync(0xFFFFFFFFu, total, o);
-  }
-  if ((threadIdx.x & 31) == 0 && total) {
-    atomicAdd(&p.ctr[C_HITS], hits);
-    atomicAdd(&p.ctr[C_GUESSES], total);
-  }
-}
-
 __global__ void fill_guess_kernel(DevTables t, ScanPtrs p) {
   const uint32_t g = blockIdx.y;
   const uint32_t st = t.groups[g].start_unanchored;
@@ -1007,6 +1091,35 @@ uint32_t max_rows(const RegexPlan& P, bool anchored) {
 template <class K>
 void set_smem(K kernel, size_t bytes, const char* what) {
   check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), what);
+}
+
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link
+// dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// The walk's view of the input: n_full rows of `chunk` bytes (16-byte
+// aligned base, chunk a multiple of 256), boxes of 16 bytes x 32 rows.
+void encode_chunk_rows(CUtensorMap* map, const uint8_t* data, uint64_t chunk, uint64_t n_full) {
+  auto fn = tensor_map_encoder();
+  if (!fn) raise(WS_ERR_DEVICE, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[2] = {chunk, n_full};
+  const cuuint64_t strides[1] = {chunk};
+  const cuuint32_t box[2] = {16, 32};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(data), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) raise(WS_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the walk's input view");
 }
 
 // Runs the candidate phase (plain or speculative) and leaves K in scratch.
@@ -1060,9 +1173,13 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
     launches++;
   }
   mark(1);
-  size_t smem = hot_smem_bytes(max_rows(P, false));
-  set_smem(dfa_walk_kernel, smem, "smem(walk)");
-  dfa_walk_kernel<<<cgrid, kWalkThreads, smem, st>>>(t, p);
+  // the input as a 2-D tensor of its full chunks (rows of p.chunk bytes)
+  const uint64_t n_full = p.len / p.chunk;
+  CUtensorMap rows;
+  std::memset(&rows, 0, sizeof(rows));
+  if (n_full) encode_chunk_rows(&rows, p.data, p.chunk, n_full);
+  set_smem(dfa_walk_kernel, kWalkSmem, "smem(walk)");
+  dfa_walk_kernel<<<cgrid, kWalkThreads, kWalkSmem, st>>>(t, p, rows, n_full);
   check_cuda(cudaGetLastError(), "dfa_walk_kernel");
   launches++;
   mark(2);
@@ -1070,9 +1187,9 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
   const uint64_t fper = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count / P.n_spec,
                                                                   (p.n_chunks + kWalkThreads - 1) / kWalkThreads));
   dim3 fgrid(P.n_spec, (unsigned)fper);
-  set_smem(dfa_fixup_kernel, smem, "smem(fixup)");
+  set_smem(dfa_fixup_kernel, kFixSmem, "smem(fixup)");
   for (int r = 0; r < kFixRounds; ++r) {
-    dfa_fixup_kernel<<<fgrid, kWalkThreads, smem, st>>>(t, p, r);
+    dfa_fixup_kernel<<<fgrid, kWalkThreads, kFixSmem, st>>>(t, p, r);
     check_cuda(cudaGetLastError(), "dfa_fixup_kernel");
     launches++;
   }
@@ -1273,7 +1390,7 @@ void layout_forward(RegexPlan& P) {
       return off;
     };
     const bool spec = g < P.n_spec;
-    gd.hot_rows = fits && spec ? P.nhot_u[g] : 0;
+    gd.hot_rows = fits && spec ? std::min(P.nhot_u[g], kHotRowsWalk) : 0;
     gd.hot_off = image(0, gd.hot_rows);
     gd.ahot_base = P.nhot_u[g];
     gd.ahot_rows = fits && spec ? P.nhot_a[g] : 0;
@@ -1558,6 +1675,8 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   RxLayout L = layout(P, l.len, P.walk_chunk, l.cap, l.k_min, l.ev_min);
   ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
+  // profiled speculative scans count the boundary guesses that held
+  if (ev && l.mode != WS_REGEX_PLAIN) p.count_guesses = P.n_spec;
   DevTables t = dev_tables(P);
   uint32_t launches = 0;
   clear_marks(P, p, st);
@@ -1578,14 +1697,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   check_cuda(cudaGetLastError(), "finalize_kernel");
   launches += 1;
   if (ev) {
-    // profiled scans also count the boundary guesses that held and read the
-    // counters back for ws_matcher_get_info
-    if (l.mode != WS_REGEX_PLAIN && L.n_chunks > 1 && P.n_spec) {
-      dim3 hg2((unsigned)std::min<uint64_t>((L.n_chunks + 255) / 256, 1024), P.n_spec);
-      guess_hits_kernel<<<hg2, 256, 0, st>>>(t, p);
-      check_cuda(cudaGetLastError(), "guess_hits_kernel");
-      launches += 1;
-    }
+    // profiled scans read the counters back for ws_matcher_get_info
     if (!P.prof_ctr) {
       unsigned long long* h = nullptr;
       check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&h), 16 * 8, cudaHostAllocDefault), "cudaHostAlloc");

@@ -32,6 +32,10 @@ namespace ws {
 // Hot rows staged per group in shared memory (a 224 KiB image: the first row
 // replicated per lane, 191 more rows column-interleaved; see ws_dfa.cu).
 constexpr uint32_t kHotRows = 192;
+// Unanchored hot rows of the speculative walk and the fix-up, which stage six
+// of the image's seven 32 KiB blocks (the first row and rows 1..159) and keep
+// the rest of their shared memory for input stages.
+constexpr uint32_t kHotRowsWalk = 160;
 
 struct GroupDev {
   uint32_t fwd_off;          // class-indexed forward table (u32 words)

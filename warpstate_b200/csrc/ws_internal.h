@@ -125,12 +125,13 @@ struct LiteralPlan {
   // sparse enough; the host copy is released once uploaded (has_big).
   std::vector<uint8_t> big;
   bool has_big = false;
-  // With the stage-1b table: stage 1 of the lean kernel as bytes, indexed by
-  // the top kFilter8Bits bits of the same hashes (the OR of the 2^7 stage-1b
-  // bytes below each entry), so a lookup needs no nibble extract.
-  std::vector<uint8_t> filter8;
+  // With the stage-1b table: stage 1 of the lean kernel, a bitmap indexed by
+  // the top kLeanBits bits of the same hashes (a bit is set when any of the
+  // 2^(kBigBits - kLeanBits) stage-1b bytes below it is non-zero), so that
+  // only about 3% of the grams of text-like input go on to a stage-1b load.
+  std::vector<uint8_t> lean_bits;
   DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2, d_big,
-      d_filter8;
+      d_lean_bits;
   uint32_t n_buckets = 0;
   // ASCII case-insensitive: the tables hold folded literals and the kernels
   // fold the input (A-Z to a-z) before hashing and comparing.
@@ -152,7 +153,7 @@ __host__ __device__ inline uint32_t ascii_fold4(uint32_t w) {
 
 constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
 constexpr uint32_t kBigBits = 25;     // stage-1b table: 2^25 bytes, 32 MiB, read through L2
-constexpr uint32_t kFilter8Bits = 17; // byte-wide stage 1 of the lean kernel: 128 KiB of shared memory
+constexpr uint32_t kLeanBits = 20;    // stage 1 of the lean kernel: a 2^20-bit bitmap, 128 KiB of shared memory
 
 // Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).
 inline uint32_t gram_hash(uint32_t gram, uint32_t bits) { return (gram * 0x9E3779B1u) >> (32 - bits); }

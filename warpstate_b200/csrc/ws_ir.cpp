@@ -251,9 +251,13 @@ void plan_literals(const ws_pattern_tables& given, LiteralPlan& plan) {
         }
       }
       plan.d_big.upload(plan.big.data(), plan.big.size());
-      plan.filter8.assign((size_t)1 << kFilter8Bits, 0);
-      for (size_t h = 0; h < plan.big.size(); ++h) plan.filter8[h >> (kBigBits - kFilter8Bits)] |= plan.big[h];
-      plan.d_filter8.upload(plan.filter8.data(), plan.filter8.size());
+      plan.lean_bits.assign((size_t)1 << (kLeanBits - 3), 0);
+      for (size_t h = 0; h < plan.big.size(); ++h)
+        if (plan.big[h]) {
+          const size_t b = h >> (kBigBits - kLeanBits);
+          plan.lean_bits[b >> 3] |= (uint8_t)(1u << (b & 7));
+        }
+      plan.d_lean_bits.upload(plan.lean_bits.data(), plan.lean_bits.size());
       plan.has_big = true;
       std::vector<uint8_t>().swap(plan.big);
     }

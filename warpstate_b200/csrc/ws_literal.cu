@@ -72,7 +72,7 @@ struct LitArgs {
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
   const uint8_t* big;        // stage-1b gram table (2^kBigBits bytes, L2), or null
-  const uint8_t* filter8;    // byte-wide stage 1 of the lean kernel (2^kFilter8Bits), or null
+  const uint32_t* lean_bits; // stage-1 bitmap of the lean kernel (2^kLeanBits bits), or null
   uint32_t verify_bloom;     // the verify kernel runs stage 1.5 first
   uint32_t fold;             // ASCII case-insensitive: input bytes A-Z read as a-z
 };
@@ -588,19 +588,20 @@ constexpr int kLeanThreads = 1024;
 constexpr int kLeanVecs = 2;  // 16-byte vectors per lane per warp step (a step covers kLeanVecs x 512 bytes)
 
 struct LeanGrams {
-  uint32_t n[4], bw[4];
+  uint32_t bw[4];  // the stage-1b phase bits of the four grams (0: rejected by stage 1)
 };
 
-// Stage 1 of a lane's four aligned grams from the byte table in shared memory
-// (top kFilter8Bits bits of the hash); the stage-1b loads from the byte table
-// in L2 (top kBigBits bits) are issued for the grams that pass.
-__device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g) {
+// Stage 1 of a lane's four aligned grams from the bitmap in shared memory
+// (top kLeanBits bits of the hash); the stage-1b loads from the byte table in
+// L2 (top kBigBits bits, the P phase bits) are issued for the grams that pass.
+__device__ __forceinline__ void lean_issue(const uint32_t* filt, const uint8_t* big, const uint4& v, LeanGrams& g) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint32_t hf = w[q] * 0x9E3779B1u;
-    g.n[q] = filt[hf >> (32 - kFilter8Bits)];
-    g.bw[q] = g.n[q] ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
+    const uint32_t b = hf >> (32 - kLeanBits);
+    const bool pass = (filt[b >> 5] >> (b & 31)) & 1u;
+    g.bw[q] = pass ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
   }
 }
 
@@ -608,7 +609,7 @@ __device__ __forceinline__ void lean_issue(const uint8_t* filt, const uint8_t* b
 __device__ __forceinline__ uint32_t lean_finish(const LeanGrams& g, uint32_t base, uint32_t len) {
   uint32_t mask = 0;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) mask |= (g.n[q] & g.bw[q]) << (4 * q);
+  for (int q = 0; q < 4; ++q) mask |= g.bw[q] << (4 * q);
   if (base == 0) mask &= ~7u;  // positions -3 .. -1
   if (base + 13 > len) {
     const uint32_t valid = len + 3 > base ? len + 3 - base : 0;
@@ -673,12 +674,11 @@ __device__ __forceinline__ void lean_append(const LitArgs& a, LeanSlots& r, cons
 
 __global__ void __launch_bounds__(kLeanThreads, 1) literal_lean_kernel(LitArgs a) {
   constexpr uint32_t W = kLeanThreads / 32, V = kLeanVecs;
-  extern __shared__ __align__(16) uint8_t smem8[];
-  uint8_t* filt = smem8;
+  extern __shared__ __align__(16) uint32_t filt[];
   {
-    const uint4* src = reinterpret_cast<const uint4*>(a.filter8);
+    const uint4* src = reinterpret_cast<const uint4*>(a.lean_bits);
     uint4* dst = reinterpret_cast<uint4*>(filt);
-    for (uint32_t k = threadIdx.x; k < (1u << (kFilter8Bits - 4)); k += kLeanThreads) dst[k] = __ldg(src + k);
+    for (uint32_t k = threadIdx.x; k < (1u << (kLeanBits - 7)); k += kLeanThreads) dst[k] = __ldg(src + k);
   }
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31;
@@ -796,7 +796,7 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   a.parts16 = plan.parts16;
   a.bloom2 = plan.gram_len > 4 ? plan.d_bloom2.as<uint32_t>() : nullptr;
   a.big = plan.has_big ? plan.d_big.as<uint8_t>() : nullptr;
-  a.filter8 = plan.has_big ? plan.d_filter8.as<uint8_t>() : nullptr;
+  a.lean_bits = plan.has_big ? plan.d_lean_bits.as<uint32_t>() : nullptr;
   a.verify_bloom = 0;
   a.fold = plan.fold ? 1 : 0;
   check_cuda(cudaMemsetAsync(a.survivor_count, 0, 8, st), "memset survivors");
@@ -823,9 +823,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   // large sets with 4-byte grams: the lean kernel, or with literals shorter
   // than 4 bytes the pipelined compacting kernel; long grams, whose hashing
   // dominates, keep 32 warps per SM
-  if (lg && !sh && a.big && a.filter8 && plan.period == 4 && plan.gram_len == 4) {
+  if (lg && !sh && a.big && a.lean_bits && plan.period == 4 && plan.gram_len == 4) {
     a.verify_bloom = 1;
-    const size_t lsmem = (size_t)1 << kFilter8Bits;
+    const size_t lsmem = (size_t)1 << (kLeanBits - 3);
     check_cuda(cudaFuncSetAttribute(literal_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
                "cudaFuncSetAttribute(literal lean)");
     literal_lean_kernel<<<sm_count, kLeanThreads, lsmem, st>>>(a);

@@ -43,8 +43,10 @@ constexpr uint32_t kSlotBytes = 256 * 64 * 2;          // 32 KiB: one K slice of
 constexpr uint32_t kSlots = 2;                         // weight slots: one copy in flight ahead of the MMAs
 constexpr uint32_t kBarBytes = 64;                     // mbarriers, TMEM address, abort flag
 // per-CTA constants staged once: b1, b2 (FP32), the joint-class map and the
-// embedding table (at most 64 classes x 16 BF16)
-constexpr uint32_t kConstBytes = 2 * 256 * 4 + 256 + 64 * kPropEmb * 2;
+// embedding table (at most 64 classes x 16 BF16); then the head biases and
+// guessed states of the head GEMM in flight (256 columns each), staged per
+// head GEMM
+constexpr uint32_t kConstBytes = 2 * 256 * 4 + 256 + 64 * kPropEmb * 2 + 2 * 256 * 4;
 constexpr uint32_t kTcSmem = kABytes + kSlots * kSlotBytes + kBarBytes + kConstBytes;
 constexpr uint32_t kWaitSpins = 1u << 24;
 
@@ -190,6 +192,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) proposer_tc_kernel(TcArgs a) {
   float* const b2s = b1s + 256;
   uint8_t* const jmap_s = reinterpret_cast<uint8_t*>(b2s + 256);
   uint8_t* const emb_s = jmap_s + 256;
+  float* const b3s = reinterpret_cast<float*>(emb_s + 64 * kPropEmb * 2);
+  uint32_t* const vocab_s = reinterpret_cast<uint32_t*>(b3s + 256);
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (a.a_test == nullptr) {
     for (uint32_t k = tid; k < 256; k += kTcThreads) {
@@ -237,6 +241,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) proposer_tc_kernel(TcArgs a) {
   if (tid == 0)
     for (; issued < kSlots - 1 && issued < total_jobs; ++issued) issue_load(issued);
 
+  // the 8 context bytes of this thread's (row, half) of tile t: loaded one
+  // tile ahead, so that the load overlaps the previous tile's GEMMs
+  auto load_ctx = [&](uint32_t t) -> uint2 {
+    const uint64_t i = (uint64_t)(blockIdx.x + t * gridDim.x) * kTcRows + 1 + (tid & (kTcRows - 1));
+    if (testing || t >= my_tiles || i >= a.n_chunks) return make_uint2(0, 0);
+    return *reinterpret_cast<const uint2*>(a.data + i * a.chunk - kPropCtx + (tid >> 8) * 8);
+  };
+  uint2 ctx_next = load_ctx(0);
   for (uint32_t t = 0; t < my_tiles && !*abort; ++t) {
     const uint64_t i0 = (uint64_t)(blockIdx.x + t * gridDim.x) * kTcRows + 1;  // first boundary of the tile
     // 1. A = embeddings of the context bytes (or the test operand): thread t
@@ -251,8 +263,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) proposer_tc_kernel(TcArgs a) {
         }
       } else {
         const uint64_t i = i0 + r;
-        uint2 ctx = make_uint2(0, 0);  // class 0 pads the rows past the last boundary
-        if (i < a.n_chunks) ctx = *reinterpret_cast<const uint2*>(a.data + i * a.chunk - kPropCtx + kh * 8);
+        const uint2 ctx = ctx_next;  // class 0 pads the rows past the last boundary
+        ctx_next = load_ctx(t + 1);
 #pragma unroll
         for (uint32_t k = 0; k < 8; ++k) {
           const uint32_t byte = ((k < 4 ? ctx.x : ctx.y) >> (8 * (k & 3))) & 0xFFu;
@@ -299,6 +311,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) proposer_tc_kernel(TcArgs a) {
           }
         }
         if (!*abort) mma_commit(layer_bar);
+      }
+      if (g >= 2 && !testing) {
+        // the head biases and guessed states of this GEMM's (up to) four groups
+        const uint32_t c = tid & 255, grp = (g - 2) * 4 + c / kPropVocab;
+        if (c < N && grp < a.G) {
+          if (tid < 256) b3s[c] = __ldg(a.b3 + grp * kPropVocab + c % kPropVocab);
+          else vocab_s[c] = __ldg(a.vocab + grp * kPropVocab + c % kPropVocab);
+        }
+        __syncthreads();
       }
       // 3. epilogue, all threads
       // warp-uniform: the tcgen05.ld below are warp-collective
@@ -350,15 +371,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) proposer_tc_kernel(TcArgs a) {
             if (c_start + 64 > N || grp >= a.G) continue;
             float best = -3.0e38f;
             uint32_t bi = 0;
+            const float* bias = b3s + c_start;
             for (uint32_t c0 = 0; c0 < 64; c0 += 32) {
               float v[32];
               tmem_ld32(tcol + h2 * 64 + c0, v);
+#pragma unroll
               for (int k = 0; k < 32; ++k) {
-                const float x = v[k] + __ldg(a.b3 + grp * kPropVocab + c0 + k);
+                const float x = v[k] + bias[c0 + k];
                 if (x > best) { best = x; bi = c0 + k; }  // first maximum: lowest index on ties
               }
             }
-            if (i < a.n_chunks) a.guess[(uint64_t)grp * a.n_chunks + i] = a.vocab[grp * kPropVocab + bi];
+            if (i < a.n_chunks) a.guess[(uint64_t)grp * a.n_chunks + i] = vocab_s[c_start + bi];
           }
         }
       }
