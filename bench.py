@@ -141,35 +141,49 @@ class ClockSampler:
 # ----------------------------------------------------------- CPU baseline
 def cpu_baseline(wl, seconds: float = 12.0):
     """Oracle port of the reference's CPU algorithm on a bounded sample of the
-    same workload, all host threads."""
+    same workload, all host threads.  Each call compiles the pattern set (a
+    fixed cost of a few tenths of a second); the sample is sized from the rate
+    between two probes, which cancels that cost, so that the timed scan runs
+    about `seconds` and the compile is a small part of it."""
     import oracle
     threads = oracle.hw_threads()
+
+    def size_for(run, p1, p2, total):
+        t = time.perf_counter()
+        run(p1)
+        d1 = time.perf_counter() - t
+        t = time.perf_counter()
+        run(p2)
+        d2 = time.perf_counter() - t
+        rate = (p2 - p1) / max(d2 - d1, 1e-3) if p2 > p1 else p1 / max(d1, 1e-6)
+        return int(min(total, max(p2, rate * seconds)))
+
     if wl.items is not None:
         items = wl.items
-        probe = 2000
+
+        def run_items(k, th=threads):
+            oracle.batch_scan(wl.patterns, wl.data, items[:k], threads=th)
+
+        k = size_for(run_items, min(len(items), 2000), min(len(items), 8000), len(items))
         t = time.perf_counter()
-        oracle.batch_scan(wl.patterns, wl.data, items[:probe], threads=threads)
-        dt = max(time.perf_counter() - t, 1e-6)
-        k = int(min(len(items), max(probe, probe * seconds / dt)))
-        t = time.perf_counter()
-        oracle.batch_scan(wl.patterns, wl.data, items[:k], threads=threads)
+        run_items(k)
         dt = time.perf_counter() - t
         nbytes = sum(ln for _, ln in items[:k])
         return {"value": round(nbytes / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                 "sample": f"first {k} of {len(items)} items ({nbytes} bytes) scanned per item in {dt:.1f} s"}
     data = wl.data
-    probe = min(len(data), 1 << 20)
+
+    def run_bytes(n, th=threads):
+        oracle.scan_patterns(wl.patterns, data[:n], th)
+
+    n = size_for(run_bytes, min(len(data), 1 << 20), min(len(data), 16 << 20), min(len(data), 0xFFFFFFFF))
     t = time.perf_counter()
-    oracle.scan_patterns(wl.patterns, data[:probe], threads)
-    dt = max(time.perf_counter() - t, 1e-6)
-    n = int(min(len(data), max(probe, probe * seconds / dt), 0xFFFFFFFF))
-    t = time.perf_counter()
-    oracle.scan_patterns(wl.patterns, data[:n], threads)
+    run_bytes(n)
     dt = time.perf_counter() - t
     # one thread on a tenth of that sample
-    n1 = max(probe, n // 10)
+    n1 = max(min(len(data), 1 << 20), n // 10)
     t = time.perf_counter()
-    oracle.scan_patterns(wl.patterns, data[:n1], 1)
+    run_bytes(n1, 1)
     dt1 = time.perf_counter() - t
     return {"value": round(n / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"first {n} bytes of the same input ({n / dt / 1e6:.1f} MB/s over {dt:.1f} s)",
