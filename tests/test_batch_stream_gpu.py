@@ -310,6 +310,49 @@ def test_scan_batch_device_equals_oracle():
     assert len(exp) > 100 and np.array_equal(got, exp)
 
 
+@pytest.mark.parametrize("profile", [False, True])
+def test_scan_batch_device_graph_replay(profile):
+    # repeated device batch scans with the same arguments replay a captured
+    # CUDA graph from the third call on (the first runs eagerly, the second is
+    # captured); every call, and a call with other arguments in between, must
+    # equal the oracle, and a profiled replay still times its phases
+    torch = _torch()
+    wl = _batch_workload(n_items=800, seed=47)
+    m = matcher(wl.patterns, profile=profile)
+    lens = np.array([ln for _, ln in wl.items], dtype=np.uint64)
+    ends = np.cumsum(lens).astype(np.uint32)
+    ids = np.arange(len(lens), dtype=np.int64) + 7
+    d_in = torch.from_numpy(wl.data[: int(lens.sum())]).cuda()
+    d_ends = torch.from_numpy(ends.view(np.int32)).cuda()
+    d_ids = torch.from_numpy(ids).cuda()
+    cap = 1 << 16
+    d_out = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream()
+
+    def run(n_items):
+        d_out.fill_(-1)
+        d_cnt.zero_()
+        m.scan_batch_device(d_in.data_ptr(), int(ends[n_items - 1]), d_ends.data_ptr(), d_ids.data_ptr(), n_items,
+                            d_out.data_ptr(), cap, d_cnt.data_ptr(), s.cuda_stream)
+        torch.cuda.synchronize()
+        n = int(d_cnt.item())
+        a = d_out[: 3 * n].view(n, 3).cpu().numpy().view(np.uint64)
+        got = np.stack([a[:, 0], a[:, 1] & 0xFFFFFFFF, a[:, 1] >> 32, a[:, 2] & 0xFFFFFFFF], axis=1)
+        return got[np.lexsort((got[:, 3], got[:, 1], got[:, 2], got[:, 0]))]
+
+    full = oracle.batch_scan(wl.patterns, wl.data, wl.items, ids.astype(np.uint64))
+    half = oracle.batch_scan(wl.patterns, wl.data, wl.items[:400], ids[:400].astype(np.uint64))
+    assert len(full) > 100 and len(half) > 20
+    launches = []
+    for n_items, exp in [(800, full)] * 4 + [(400, half)] * 3 + [(800, full)] * 3:
+        assert np.array_equal(run(n_items), exp), n_items
+        launches.append(m.info()["last_launches"])
+    assert launches[0] == launches[1] == launches[2] == launches[3] > 1
+    if profile:
+        assert m.info()["last_kernel_ms"][7] > 0
+
+
 def test_large_pinned_scan_overlaps_copy_and_stays_exact():
     # a pinned host input of >= 256 MiB is copied in 128 MiB windows on a
     # second stream and each window scanned as soon as it arrives; the result

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 
 #include "ws_matcher.h"
@@ -129,16 +130,75 @@ extern "C" ws_status ws_scan_batch_device(ws_matcher* m, const uint8_t* d_data, 
     }
     const uint64_t dcap = std::max<uint64_t>(cap, 1);
     ensure(s->out, dcap * sizeof(ws_match));
-    ScanExtras x;
-    x.item_end = d_item_end;
-    x.n_items = (uint32_t)n_items;
-    const uint32_t launches = enqueue_scan(m, *s, st, d_data, len, s->out.as<ws_match>(), dcap, d_counter, x);
-    tag_kernel<<<m->ctx->sm_count * 4, 256, 0, st>>>(s->out.as<ws_match>(), d_counter, std::min(dcap, cap), d_item_end,
-                                                      d_ids, (uint32_t)n_items, d_out);
-    check_cuda(cudaGetLastError(), "tag_kernel");
+    auto body = [&]() -> uint32_t {
+      ScanExtras x;
+      x.item_end = d_item_end;
+      x.n_items = (uint32_t)n_items;
+      const uint32_t n = enqueue_scan(m, *s, st, d_data, len, s->out.as<ws_match>(), dcap, d_counter, x);
+      tag_kernel<<<m->ctx->sm_count * 4, 256, 0, st>>>(s->out.as<ws_match>(), d_counter, std::min(dcap, cap),
+                                                        d_item_end, d_ids, (uint32_t)n_items, d_out);
+      check_cuda(cudaGetLastError(), "tag_kernel");
+      return n + 1;
+    };
+    // The launch sequence of a call is replayed from a CUDA graph when the
+    // previous calls on this scratch had the same arguments and plan: the
+    // first runs eagerly (it sizes every buffer), the second is captured.
+    BatchGraphKey key;
+    key.data = d_data;
+    key.len = len;
+    key.item_end = d_item_end;
+    key.ids = d_ids;
+    key.n_items = n_items;
+    key.out = d_out;
+    key.cap = cap;
+    key.count = d_count;
+    key.stream = stream;
+    key.plan_gen = m->plan_gen.load();
+    if (m->need_host) {
+      key.need[0] = m->need_host[0];
+      key.need[1] = m->need_host[1];
+    }
+    key.profile = m->profile ? 1 : 0;
+    BatchGraph& bg = s->batch_graph;
+    if (std::memcmp(&bg.key, &key, sizeof(key)) != 0) {
+      bg.reset();
+      bg.key = key;
+    }
+    uint32_t launches = 0;
+    if (bg.exec) {
+      check_cuda(cudaGraphLaunch(bg.exec, st), "cudaGraphLaunch(batch)");
+      launches = bg.launches;
+    } else if (bg.seen >= 1 && !bg.broken) {
+      cudaGraph_t graph = nullptr;
+      check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+      try {
+        launches = body();
+      } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        bg.broken = true;
+        throw;
+      }
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      const cudaError_t ie = ce == cudaSuccess ? cudaGraphInstantiate(&bg.exec, graph, 0) : ce;
+      if (graph) cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {  // no graph: run this call eagerly and stay eager for this key
+        cudaGetLastError();
+        bg.exec = nullptr;
+        bg.broken = true;
+        launches = body();
+      } else {
+        bg.launches = launches;
+        check_cuda(cudaGraphLaunch(bg.exec, st), "cudaGraphLaunch(batch)");
+      }
+    } else {
+      launches = body();
+      bg.seen++;
+    }
     check_cuda(cudaEventRecord(s->busy, st), "event");
     std::lock_guard<std::mutex> g(m->info_mu);
-    m->info.last_launches = launches + 1;
+    m->info.last_launches = launches;
   });
 }
 

@@ -326,6 +326,29 @@ __device__ __forceinline__ bool slow_step(uint32_t w, uint32_t b, uint32_t& st, 
 
 #define WS_STEP_FAST(img, st, b) (*reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(img) + (st) + ((b) << 7)))
 
+// One transition of the unanchored (trap) image: an entry other than the trap
+// column's offset is the next hot row's column; the trap offset sends the
+// transition to the class-indexed table, from the hot row or the cold row the
+// walk is in.  Returns the row of a match state (0xFFFFFFFF when none).
+__device__ __forceinline__ uint32_t trap_step(const uint32_t* img, uint32_t b, uint32_t& st, uint32_t& cold_row,
+                                              uint32_t H, uint32_t lane4, const uint8_t* cls_s, const uint32_t* tab,
+                                              uint32_t C) {
+  const uint32_t w = WS_STEP_FAST(img, st, b);
+  if (w != kTrapByte) {
+    st = max(w, lane4);
+    return 0xFFFFFFFFu;
+  }
+  const uint32_t t = __ldg(tab + row_of(st, cold_row, 0) * C + cls_s[b]);
+  const uint32_t n = t & F_MASK;
+  if (n < H && !(t & F_DEAD)) {
+    st = slot_byte(n, lane4);
+  } else {
+    st = kTrapByte;
+    cold_row = n;
+  }
+  return (t & F_MATCH) ? n : 0xFFFFFFFFu;
+}
+
 // One transition through L2 only (fix-up walks, which are short and rare).
 __device__ __forceinline__ uint32_t step_l2(uint32_t st, uint32_t b, const uint8_t* cls_g, const uint32_t* tab,
                                             uint32_t C) {
@@ -508,29 +531,23 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
   // is negative: it sends the walk to the first row, in bounds, and marks the
   // block), then, for a marked block, a careful pass for match events and
   // cold rows.
+  // One 16-byte block: an optimistic pass over the image alone (a transition
+  // that is not a plain hot one lands in the absorbing trap column, so the
+  // block ends there), then, for a block that ended in the trap, a careful
+  // pass from its start for match events and cold rows.
   auto block16 = [&](const uint32_t* words, uint64_t at) {
-    const uint32_t st0 = st, cold0 = cold_row;
-    uint32_t acc = 0;
+    const uint32_t st0 = st;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
-      uint32_t w = WS_STEP_FAST(img, st, b);
-      acc |= w;
-      st = (uint32_t)max((int32_t)w, lane4);
+      st = max(WS_STEP_FAST(img, st, b), (uint32_t)lane4);
     }
-    if ((int32_t)acc < 0) {
+    if (st == kTrapByte) {
       st = st0;
-      cold_row = cold0;
       for (int k = 0; k < 16; ++k) {
-        uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-        uint32_t w = WS_STEP_FAST(img, st, b);
-        if ((int32_t)w >= 0) {
-          st = (uint32_t)max((int32_t)w, lane4);
-        } else {
-          uint32_t m_row;
-          slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
-          if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + k + 1), m_row, (uint32_t)q, 0);
-        }
+        const uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+        const uint32_t m_row = trap_step(img, b, st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
+        if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + k + 1), m_row, (uint32_t)q, 0);
       }
     }
   };
@@ -572,15 +589,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
   }
   if (!active) return;
   for (uint64_t pos = c0 + nvec * 16; pos < c1; ++pos) {
-    uint32_t b = __ldg(p.data + pos);
-    uint32_t w = WS_STEP_FAST(img, st, b);
-    if ((int32_t)w >= 0) {
-      st = (uint32_t)max((int32_t)w, lane4);
-    } else {
-      uint32_t m_row;
-      slow_step(w, b, st, cold_row, 0, H, (uint32_t)lane4, cls_s, tab, C, m_row);
-      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
-    }
+    const uint32_t m_row = trap_step(img, __ldg(p.data + pos), st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
+    if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
   }
   const uint32_t end_row = row_of(st, cold_row, 0);
   p.end[q] = end_row;
@@ -650,14 +660,8 @@ __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const Group
   uint32_t cold_row = 0;
   uint32_t st = state_of(S, 0, H, lane4, &cold_row);
   auto step = [&](uint32_t b, uint64_t at) {
-    const uint32_t w = WS_STEP_FAST(img, st, b);
-    if ((int32_t)w >= 0) {
-      st = (uint32_t)max((int32_t)w, (int32_t)lane4);
-    } else {
-      uint32_t m_row;
-      slow_step(w, b, st, cold_row, 0, H, lane4, cls_s, tab, C, m_row);
-      if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + 1), m_row, (uint32_t)q, tag);
-    }
+    const uint32_t m_row = trap_step(img, b, st, cold_row, H, lane4, cls_s, tab, C);
+    if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + 1), m_row, (uint32_t)q, tag);
   };
   // 16-byte vectors, four in flight ahead of the walk; the state is compared
   // with the speculative walk's at every checkpoint
@@ -1126,7 +1130,7 @@ void encode_chunk_rows(CUtensorMap* map, const uint8_t* data, uint64_t chunk, ui
 uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, uint32_t mode, cudaStream_t st,
                           int sm_count, cudaEvent_t* ev) {
   uint32_t launches = 0;
-  auto mark = [&](int k) { if (ev) check_cuda(cudaEventRecord(ev[k], st), "event"); };
+  auto mark = [&](int k) { if (ev) check_cuda(record_phase(ev[k], st), "event"); };
   // context groups: one anchored walk per start in either mode
   auto context_groups = [&]() {
     const uint32_t nc = P.n_groups - P.n_spec;
@@ -1370,15 +1374,20 @@ void layout_forward(RegexPlan& P) {
     gd.start_unanchored = d.start_unanchored;
     // slow words carry the next row in 27 bits; larger DFAs walk through L2 only
     const bool fits = d.n_states < (1 << 27);
-    auto image = [&](uint32_t first, uint32_t rows) {
+    // trap: the unanchored image of the walk and the fix-up, whose every
+    // transition that is not into a hot row without a match is the trap
+    // column's offset (an absorbing column: its entries are its own offset);
+    // else slow words (the anchored image of the plain kernel)
+    auto image = [&](uint32_t first, uint32_t rows, bool trap) {
       uint32_t off = (uint32_t)P.hot.size();
       if (!rows) return off;
-      P.hot.resize(P.hot.size() + kImgWords, S_SLOW | S_TRAP);
+      P.hot.resize(P.hot.size() + kImgWords, trap ? kTrapByte : (S_SLOW | S_TRAP));
       uint32_t* img = P.hot.data() + off;
       auto entry = [&](uint32_t w) -> uint32_t {
         uint32_t n = w & DFA_MASK_STATE, nl = n - first;
         bool match = w & DFA_FLAG_MATCH, dead = w & DFA_FLAG_DEAD, hot = nl < rows;
         if (!match && !dead && hot) return nl == 0 ? 0u : slot_word(nl) * 4;
+        if (trap) return kTrapByte;
         return S_SLOW | (match ? S_MATCH : 0u) | (hot ? 0u : S_COLD) | (dead ? S_DEAD : 0u) | n;
       };
       for (uint32_t r = 0; r < rows; ++r)
@@ -1391,10 +1400,10 @@ void layout_forward(RegexPlan& P) {
     };
     const bool spec = g < P.n_spec;
     gd.hot_rows = fits && spec ? std::min(P.nhot_u[g], kHotRowsWalk) : 0;
-    gd.hot_off = image(0, gd.hot_rows);
+    gd.hot_off = image(0, gd.hot_rows, true);
     gd.ahot_base = P.nhot_u[g];
     gd.ahot_rows = fits && spec ? P.nhot_a[g] : 0;
-    gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows);
+    gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows, false);
     gd.mptr_off = (uint32_t)P.mptr.size();
     // one list per state, or per (state, right context) in a context group
     const size_t n_lists = d.match_ptr.size() - 1;
@@ -1682,7 +1691,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   clear_marks(P, p, st);
   check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");
   check_cuda(cudaMemsetAsync(p.count, 0, (size_t)P.n_regex * 4, st), "memset");
-  if (ev) check_cuda(cudaEventRecord(ev[0], st), "event");
+  if (ev) check_cuda(record_phase(ev[0], st), "event");
   launches += candidates_phase(P, t, p, l.mode, st, sm_count, ev);
   int hg = (int)std::min<uint64_t>((uint64_t)sm_count * 8, (L.k_cap + 255) / 256);
   k_hist_kernel<<<hg, 256, 0, st>>>(p);
@@ -1705,7 +1714,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
       P.prof_ctr.reset(h);
     }
     check_cuda(cudaMemcpyAsync(P.prof_ctr.get(), p.ctr, 16 * 8, cudaMemcpyDeviceToHost, st), "D2H counters");
-    check_cuda(cudaEventRecord(ev[5], st), "event");
+    check_cuda(record_phase(ev[5], st), "event");
   }
   P.last_chunks = L.n_q;
   P.last_launches = launches;

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <atomic>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -21,6 +22,39 @@ struct ws_ctx {
 };
 
 namespace ws {
+
+// The arguments of a device batch scan whose launch sequence a CUDA graph
+// holds (ws_scan_batch_device): a later call with the same arguments and the
+// same matcher plan replays the graph.
+struct BatchGraphKey {
+  const void* data = nullptr;
+  uint64_t len = 0;
+  const void* item_end = nullptr;
+  const void* ids = nullptr;
+  uint64_t n_items = 0;
+  const void* out = nullptr;
+  uint64_t cap = 0;
+  const void* count = nullptr;
+  const void* stream = nullptr;
+  uint64_t plan_gen = 0;
+  uint64_t need[2] = {0, 0};
+  uint64_t profile = 0;
+};
+
+struct BatchGraph {
+  BatchGraphKey key;
+  uint32_t seen = 0;            // eager runs with this key (the first sizes every buffer)
+  uint32_t launches = 0;        // kernel launches the graph holds
+  bool broken = false;          // capture or instantiation failed: stay eager
+  cudaGraphExec_t exec = nullptr;
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    seen = 0;
+    broken = false;
+  }
+  ~BatchGraph() { reset(); }
+};
 
 // Per-call scratch: a stream, the device input copy, the output and counters.
 struct Scratch {
@@ -41,6 +75,7 @@ struct Scratch {
   bool pin_busy[2] = {false, false};                         // a DMA may still read the slot
   cudaEvent_t busy = nullptr;  // recorded after the last use
   cudaStream_t copy = nullptr;  // host-to-device copies overlapped with scans (created on first use)
+  BatchGraph batch_graph;       // the last device batch scan's launch sequence
   ~Scratch() {
     if (busy) cudaEventDestroy(busy);
     if (copy) cudaStreamDestroy(copy);
@@ -107,6 +142,10 @@ struct ws_matcher {
   std::mutex info_mu;
   ws_matcher_info info;
   bool profile = false;          // record phase events (single caller at a time)
+  // Bumped whenever the launch sequence of a scan may change (walk chunk,
+  // proposer on or off, re-planned groups or hot rows): captured graphs of
+  // earlier plans are not replayed.
+  std::atomic<uint64_t> plan_gen{0};
   cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t rx_events[8] = {};
   // phase times summed over the windows of the last multi-window scan

@@ -173,6 +173,7 @@ extern "C" ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint6
     rep.walk_chunk = m->rx.walk_chunk;
     rep.proposer_used = (m->rx.proposer && m->rx.use_proposer) ? 1 : 0;
     rep.tune_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    m->plan_gen++;
     if (report) *report = rep;
   });
 }
@@ -190,5 +191,6 @@ extern "C" ws_status ws_matcher_set_walk(ws_matcher* m, uint32_t walk_chunk, uin
       m->cfg.walk_chunk = walk_chunk;
     }
     m->rx.use_proposer = proposer == WS_PROPOSER_MLP;
+    m->plan_gen++;
   });
 }
