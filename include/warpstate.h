@@ -385,6 +385,10 @@ typedef struct {
   uint64_t last_guesses;         /* chunk boundaries guessed (chunks - 1, per group) */
   uint32_t regex_context;        /* 1 when some regex has a look-around assertion */
   uint32_t n_context_groups;     /* DFA groups of such regexes (walked per start position) */
+  uint32_t last_graph_replay;    /* 1 when the last ws_scan_batch_device call replayed a captured CUDA
+                                    graph of its launch sequence (the same arguments as the calls before
+                                    it, on a stream other than the legacy default stream, not profiled) */
+  uint32_t reserved;
 } ws_matcher_info;
 ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
 

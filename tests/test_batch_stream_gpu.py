@@ -313,9 +313,9 @@ def test_scan_batch_device_equals_oracle():
 @pytest.mark.parametrize("profile", [False, True])
 def test_scan_batch_device_graph_replay(profile):
     # repeated device batch scans with the same arguments replay a captured
-    # CUDA graph from the third call on (the first runs eagerly, the second is
-    # captured); every call, and a call with other arguments in between, must
-    # equal the oracle, and a profiled replay still times its phases
+    # CUDA graph (the first runs eagerly, the second is captured and launched);
+    # every call, and a call with other arguments in between, must equal the
+    # oracle; profiled scans time their phases and stay eager
     torch = _torch()
     wl = _batch_workload(n_items=800, seed=47)
     m = matcher(wl.patterns, profile=profile)
@@ -328,11 +328,13 @@ def test_scan_batch_device_graph_replay(profile):
     cap = 1 << 16
     d_out = torch.empty(cap * 3, dtype=torch.int64, device="cuda")
     d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
-    s = torch.cuda.current_stream()
+    s = torch.cuda.Stream()  # a stream of its own: the legacy default stream is never captured
+    torch.cuda.synchronize()
 
     def run(n_items):
-        d_out.fill_(-1)
-        d_cnt.zero_()
+        with torch.cuda.stream(s):
+            d_out.fill_(-1)
+            d_cnt.zero_()
         m.scan_batch_device(d_in.data_ptr(), int(ends[n_items - 1]), d_ends.data_ptr(), d_ids.data_ptr(), n_items,
                             d_out.data_ptr(), cap, d_cnt.data_ptr(), s.cuda_stream)
         torch.cuda.synchronize()
@@ -344,13 +346,17 @@ def test_scan_batch_device_graph_replay(profile):
     full = oracle.batch_scan(wl.patterns, wl.data, wl.items, ids.astype(np.uint64))
     half = oracle.batch_scan(wl.patterns, wl.data, wl.items[:400], ids[:400].astype(np.uint64))
     assert len(full) > 100 and len(half) > 20
-    launches = []
+    launches, replays = [], []
     for n_items, exp in [(800, full)] * 4 + [(400, half)] * 3 + [(800, full)] * 3:
         assert np.array_equal(run(n_items), exp), n_items
         launches.append(m.info()["last_launches"])
+        replays.append(m.info()["last_graph_replay"])
     assert launches[0] == launches[1] == launches[2] == launches[3] > 1
     if profile:
-        assert m.info()["last_kernel_ms"][7] > 0
+        assert replays == [0] * 10 and m.info()["last_kernel_ms"][7] > 0
+    else:
+        # eager, captured and launched, replayed, replayed; a new key starts over
+        assert replays == [0, 1, 1, 1, 0, 1, 1, 0, 1, 1]
 
 
 def test_large_pinned_scan_overlaps_copy_and_stays_exact():

@@ -75,7 +75,8 @@ class WsMatcherInfo(ctypes.Structure):
                 ("max_literal_len", ctypes.c_uint32), ("max_regex_len", ctypes.c_int64),
                 ("last_events", ctypes.c_uint64), ("last_rewalk_bytes", ctypes.c_uint64),
                 ("last_guess_hits", ctypes.c_uint64), ("last_guesses", ctypes.c_uint64),
-                ("regex_context", ctypes.c_uint32), ("n_context_groups", ctypes.c_uint32)]
+                ("regex_context", ctypes.c_uint32), ("n_context_groups", ctypes.c_uint32),
+                ("last_graph_replay", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class WsTuneReport(ctypes.Structure):

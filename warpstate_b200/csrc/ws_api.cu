@@ -113,7 +113,7 @@ uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t*
   uint32_t launches = 0;
   m->use_summed = false;
   check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st), "memset counter");
-  if (prof) check_cuda(record_phase(m->pev[0], st), "event");
+  if (prof) check_cuda(cudaEventRecord(m->pev[0], st), "event");
   if (m->lit.n_literals && x.literals) {
     uint64_t scap = literal_survivor_cap(len);
     ensure(s.lit, literal_scratch_bytes(scap));
@@ -125,7 +125,7 @@ uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t*
     launch_literal_scan(m->lit, ll, st, m->ctx->sm_count);
     launches += 2;
   }
-  if (prof) check_cuda(record_phase(m->pev[1], st), "event");
+  if (prof) check_cuda(cudaEventRecord(m->pev[1], st), "event");
   if (m->rx.n_regex) {
     RegexLaunch rl{d_data, len, d_out, cap, d_counter, m->cfg.regex_mode};
     rl.item_end = x.item_end;
@@ -144,7 +144,7 @@ uint32_t enqueue_scan(ws_matcher* m, Scratch& s, cudaStream_t st, const uint8_t*
     }
     launches += run_regex_scan(m->rx, rl, st, s.rx, m->ctx->sm_count, prof ? m->rx_events : nullptr);
   }
-  if (prof) check_cuda(record_phase(m->pev[2], st), "event");
+  if (prof) check_cuda(cudaEventRecord(m->pev[2], st), "event");
   check_cuda(cudaEventRecord(s.busy, st), "event");
   std::lock_guard<std::mutex> g(m->info_mu);
   m->info.last_launches = launches;

@@ -165,12 +165,16 @@ extern "C" ws_status ws_scan_batch_device(ws_matcher* m, const uint8_t* d_data, 
       bg.key = key;
     }
     uint32_t launches = 0;
+    bool replayed = false;
     if (bg.exec) {
       check_cuda(cudaGraphLaunch(bg.exec, st), "cudaGraphLaunch(batch)");
       launches = bg.launches;
-    } else if (bg.seen >= 1 && !bg.broken) {
+      replayed = true;
+    } else if (bg.seen >= 1 && !bg.broken && !m->profile && st != nullptr && st != cudaStreamLegacy &&
+               cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+      // (the legacy default stream cannot be captured, and profiled scans time
+      // each phase with events: their calls stay eager)
       cudaGraph_t graph = nullptr;
-      check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
       try {
         launches = body();
       } catch (...) {
@@ -191,14 +195,17 @@ extern "C" ws_status ws_scan_batch_device(ws_matcher* m, const uint8_t* d_data, 
       } else {
         bg.launches = launches;
         check_cuda(cudaGraphLaunch(bg.exec, st), "cudaGraphLaunch(batch)");
+        replayed = true;
       }
     } else {
+      cudaGetLastError();  // a refused capture leaves its error behind
       launches = body();
       bg.seen++;
     }
     check_cuda(cudaEventRecord(s->busy, st), "event");
     std::lock_guard<std::mutex> g(m->info_mu);
     m->info.last_launches = launches;
+    m->info.last_graph_replay = replayed ? 1u : 0u;
   });
 }
 

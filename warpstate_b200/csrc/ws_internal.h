@@ -35,11 +35,6 @@ struct WsError : std::exception {
 [[noreturn]] void raise(ws_status s, const std::string& msg, uint64_t index = 0, uint64_t count = 0,
                         uint64_t max = 0);
 void check_cuda(cudaError_t e, const char* what);
-// Records a phase-timing event; inside a stream capture the record becomes a
-// node of the graph (an external event record), so replays still time.
-inline cudaError_t record_phase(cudaEvent_t ev, cudaStream_t st) {
-  return cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
-}
 
 uint32_t fnv1a(const uint8_t* p, size_t len, size_t window);
 
