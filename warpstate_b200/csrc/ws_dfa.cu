@@ -326,24 +326,56 @@ __device__ __forceinline__ bool slow_step(uint32_t w, uint32_t b, uint32_t& st, 
 
 #define WS_STEP_FAST(img, st, b) (*reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(img) + (st) + ((b) << 7)))
 
-// One transition of the unanchored (trap) image: an entry other than the trap
-// column's offset is the next hot row's column; the trap offset sends the
-// transition to the class-indexed table, from the hot row or the cold row the
-// walk is in.  Returns the row of a match state (0xFFFFFFFF when none).
-__device__ __forceinline__ uint32_t trap_step(const uint32_t* img, uint32_t b, uint32_t& st, uint32_t& cold_row,
-                                              uint32_t H, uint32_t lane4, const uint8_t* cls_s, const uint32_t* tab,
-                                              uint32_t C) {
-  const uint32_t w = WS_STEP_FAST(img, st, b);
-  if (w != kTrapByte) {
+// Geometry of the walk's unanchored image: 32-row blocks of `img_cols`
+// entries per row (256: indexed by byte; or the group's class count: indexed
+// by class), block 0 the first row once per lane, the trap column at block 1,
+// column 0.  A walk state is the byte offset of its row's column.
+struct WalkImg {
+  uint32_t blk_words;  // words per block: 32 x img_cols
+  uint32_t trap;       // byte offset of the trap column
+};
+__device__ __forceinline__ WalkImg walk_img(const GroupDev& gd) { return {gd.img_cols * 32, gd.img_cols * 128}; }
+__device__ __forceinline__ uint32_t wslot(const WalkImg& g, uint32_t r, uint32_t lane4) {
+  return r == 0 ? lane4 : ((1 + (r >> 5)) * g.blk_words + (r & 31)) * 4;
+}
+__device__ __forceinline__ uint32_t wrow(const WalkImg& g, uint32_t st, uint32_t cold_row) {
+  if (st < 128) return 0;
+  if (st == g.trap) return cold_row;
+  const uint32_t w = st >> 2;
+  return (w / g.blk_words - 1) * 32 + (w & 31);
+}
+__device__ __forceinline__ uint32_t wstate(const WalkImg& g, uint32_t row, uint32_t rows, uint32_t lane4,
+                                           uint32_t* cold_row) {
+  if (row < rows) return wslot(g, row, lane4);
+  *cold_row = row;
+  return g.trap;
+}
+// The image column of input byte b: the byte itself, or its class.
+template <bool kCls>
+__device__ __forceinline__ uint32_t wcol(const uint8_t* cls_s, uint32_t b) {
+  return kCls ? (uint32_t)cls_s[b] : b;
+}
+
+// One transition of the walk's image: an entry other than the trap column's
+// offset is the next hot row's column; the trap offset sends the transition
+// to the class-indexed table, from the hot row or the cold row the walk is in.
+// Returns the row of a match state (0xFFFFFFFF when none).
+template <bool kCls>
+__device__ __forceinline__ uint32_t trap_step(const uint32_t* img, const WalkImg& gi, uint32_t b, uint32_t& st,
+                                              uint32_t& cold_row, uint32_t H, uint32_t lane4, const uint8_t* cls_s,
+                                              const uint32_t* tab, uint32_t C) {
+  const uint32_t c = cls_s[b];
+  const uint32_t w = WS_STEP_FAST(img, st, kCls ? c : b);
+  if (w != gi.trap) {
     st = max(w, lane4);
     return 0xFFFFFFFFu;
   }
-  const uint32_t t = __ldg(tab + row_of(st, cold_row, 0) * C + cls_s[b]);
+  const uint32_t t = __ldg(tab + wrow(gi, st, cold_row) * C + c);
   const uint32_t n = t & F_MASK;
   if (n < H && !(t & F_DEAD)) {
-    st = slot_byte(n, lane4);
+    st = wslot(gi, n, lane4);
   } else {
-    st = kTrapByte;
+    st = gi.trap;
     cold_row = n;
   }
   return (t & F_MATCH) ? n : 0xFFFFFFFFu;
@@ -478,6 +510,7 @@ __global__ void __launch_bounds__(256) dfa_context_kernel(DevTables t, ScanPtrs 
 // hot-row lookups need; one 16-byte load per lane and step from 32 different
 // chunks would each take a wavefront and an L2 sector.  A lane whose chunk
 // is not a full one (the last, partial chunk) loads its bytes itself.
+template <bool kCls>
 __global__ void __launch_bounds__(kWalkThreads, 1)
     dfa_walk_kernel(DevTables t, ScanPtrs p, const __grid_constant__ CUtensorMap rows, uint64_t n_full) {
   extern __shared__ __align__(128) uint32_t smem[];
@@ -489,7 +522,8 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
   uint8_t* stages = reinterpret_cast<uint8_t*>(smem) + kWalkImgBytes;
   uint8_t* cls_s = stages + kWalkStageBytes;
   uint64_t* sbar = reinterpret_cast<uint64_t*>(cls_s + 256 + 16);
-  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR], kWalkImgBytes)) return;
+  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR], gd.img_bytes)) return;
+  const WalkImg gi = walk_img(gd);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t wfirst = (uint64_t)blockIdx.y * blockDim.x + warp * 32;  // lane 0's chunk
   if (wfirst >= p.n_chunks) return;  // the whole warp
@@ -526,11 +560,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
   }
   uint32_t* ck = p.ckpt + q * p.nck;
   uint32_t cold_row = 0;
-  uint32_t st = state_of(start, 0, H, (uint32_t)lane4, &cold_row);
-  // One 16-byte block: an optimistic pass over fast entries only (a slow word
-  // is negative: it sends the walk to the first row, in bounds, and marks the
-  // block), then, for a marked block, a careful pass for match events and
-  // cold rows.
+  uint32_t st = wstate(gi, start, H, (uint32_t)lane4, &cold_row);
   // One 16-byte block: an optimistic pass over the image alone (a transition
   // that is not a plain hot one lands in the absorbing trap column, so the
   // block ends there), then, for a block that ended in the trap, a careful
@@ -539,14 +569,14 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
     const uint32_t st0 = st;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
-      st = max(WS_STEP_FAST(img, st, b), (uint32_t)lane4);
+      const uint32_t b = __byte_perm(words[k >> 2], 0, 0x4440 + (k & 3));
+      st = max(WS_STEP_FAST(img, st, wcol<kCls>(cls_s, b)), (uint32_t)lane4);
     }
-    if (st == kTrapByte) {
+    if (st == gi.trap) {
       st = st0;
       for (int k = 0; k < 16; ++k) {
         const uint32_t b = (words[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-        const uint32_t m_row = trap_step(img, b, st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
+        const uint32_t m_row = trap_step<kCls>(img, gi, b, st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
         if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + k + 1), m_row, (uint32_t)q, 0);
       }
     }
@@ -585,14 +615,15 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
     const uint32_t words[4] = {cur.x, cur.y, cur.z, cur.w};
     block16(words, c0 + k * 16);
     const uint64_t done = (k + 1) * 16;
-    if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = row_of(st, cold_row, 0);
+    if ((done % kCkpt) == 0) ck[done / kCkpt - 1] = wrow(gi, st, cold_row);
   }
   if (!active) return;
   for (uint64_t pos = c0 + nvec * 16; pos < c1; ++pos) {
-    const uint32_t m_row = trap_step(img, __ldg(p.data + pos), st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
+    const uint32_t m_row =
+        trap_step<kCls>(img, gi, __ldg(p.data + pos), st, cold_row, H, (uint32_t)lane4, cls_s, tab, C);
     if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(pos + 1), m_row, (uint32_t)q, 0);
   }
-  const uint32_t end_row = row_of(st, cold_row, 0);
+  const uint32_t end_row = wrow(gi, st, cold_row);
   p.end[q] = end_row;
   p.spec[q] = end_row;
 }
@@ -645,6 +676,7 @@ __device__ void fix_chunk(const DevTables& t, const ScanPtrs& p, uint32_t g, uin
 // steps: a shared-memory lookup per byte, the class-indexed table in L2 only
 // for cold rows), so that a re-walk is not a chain of L2 round trips.  The
 // input is 16-byte aligned and chunks start at multiples of kCkpt.
+template <bool kCls>
 __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const GroupDev& gd, const uint32_t* img,
                               const uint8_t* cls_s, uint32_t g, uint64_t i, uint32_t tag,
                               unsigned long long* changed, uint32_t lane4) {
@@ -657,10 +689,11 @@ __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const Group
   const uint64_t c0 = i * p.chunk;
   const uint64_t c1 = min(p.len, c0 + p.chunk);
   const uint32_t* ck = p.ckpt + q * p.nck;
+  const WalkImg gi = walk_img(gd);
   uint32_t cold_row = 0;
-  uint32_t st = state_of(S, 0, H, lane4, &cold_row);
+  uint32_t st = wstate(gi, S, H, lane4, &cold_row);
   auto step = [&](uint32_t b, uint64_t at) {
-    const uint32_t m_row = trap_step(img, b, st, cold_row, H, lane4, cls_s, tab, C);
+    const uint32_t m_row = trap_step<kCls>(img, gi, b, st, cold_row, H, lane4, cls_s, tab, C);
     if (m_row != 0xFFFFFFFFu) emit_event(p, (uint32_t)(at + 1), m_row, (uint32_t)q, tag);
   };
   // 16-byte vectors, four in flight ahead of the walk; the state is compared
@@ -682,7 +715,7 @@ __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const Group
 #pragma unroll
     for (int j = 0; j < 16; ++j) step((wd[j >> 2] >> (8 * (j & 3))) & 0xFFu, c0 + k * 16 + j);
     const uint64_t done = (k + 1) * 16;
-    if (done % kCkpt == 0 && done / kCkpt <= p.nck && row_of(st, cold_row, 0) == ck[done / kCkpt - 1]) {
+    if (done % kCkpt == 0 && done / kCkpt <= p.nck && wrow(gi, st, cold_row) == ck[done / kCkpt - 1]) {
       converged = true;
       conv = c0 + done;
       break;
@@ -695,7 +728,7 @@ __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const Group
   p.conv[q] = (uint32_t)conv;
   atomicAdd(&p.ctr[C_FIX], 1ull);
   atomicAdd(&p.ctr[C_REWALK], (unsigned long long)(conv - c0));
-  const uint32_t new_end = converged ? p.spec[q] : row_of(st, cold_row, 0);
+  const uint32_t new_end = converged ? p.spec[q] : wrow(gi, st, cold_row);
   if (new_end != endv[q]) {
     endv[q] = new_end;
     atomicOr(changed, 1ull);
@@ -706,6 +739,7 @@ __device__ void fix_chunk_img(const DevTables& t, const ScanPtrs& p, const Group
 // walk), each over a strided share of the group's chunks.  A block stages the
 // hot-row image only when one of its chunks was walked from a start that
 // differs from its predecessor's end.
+template <bool kCls>
 __global__ void __launch_bounds__(kWalkThreads, 1) dfa_fixup_kernel(DevTables t, ScanPtrs p, int round) {
   if (round > 0 && p.ctr[C_ROUND + round - 1] == 0) return;  // nothing changed last round
   extern __shared__ __align__(16) uint32_t smem[];
@@ -721,10 +755,10 @@ __global__ void __launch_bounds__(kWalkThreads, 1) dfa_fixup_kernel(DevTables t,
   const GroupDev gd = t.groups[g];
   uint32_t* img = smem;
   uint8_t* cls_s = reinterpret_cast<uint8_t*>(smem) + kWalkImgBytes;
-  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR], kWalkImgBytes)) return;
+  if (!stage_hot(t, g, gd.hot_off, gd.hot_rows, img, cls_s, &p.ctr[C_ERR], gd.img_bytes)) return;
   const uint32_t lane4 = (threadIdx.x & 31) * 4;
   for (uint64_t i = first; i < p.n_chunks; i += stride)
-    fix_chunk_img(t, p, gd, img, cls_s, g, i, (uint32_t)round + 1, &p.ctr[C_ROUND + round], lane4);
+    fix_chunk_img<kCls>(t, p, gd, img, cls_s, g, i, (uint32_t)round + 1, &p.ctr[C_ROUND + round], lane4);
 }
 
 // Final sweep, one thread per group, in chunk order: exact whatever happened
@@ -1130,7 +1164,7 @@ void encode_chunk_rows(CUtensorMap* map, const uint8_t* data, uint64_t chunk, ui
 uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, uint32_t mode, cudaStream_t st,
                           int sm_count, cudaEvent_t* ev) {
   uint32_t launches = 0;
-  auto mark = [&](int k) { if (ev) check_cuda(record_phase(ev[k], st), "event"); };
+  auto mark = [&](int k) { if (ev) check_cuda(cudaEventRecord(ev[k], st), "event"); };
   // context groups: one anchored walk per start in either mode
   auto context_groups = [&]() {
     const uint32_t nc = P.n_groups - P.n_spec;
@@ -1182,8 +1216,13 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
   CUtensorMap rows;
   std::memset(&rows, 0, sizeof(rows));
   if (n_full) encode_chunk_rows(&rows, p.data, p.chunk, n_full);
-  set_smem(dfa_walk_kernel, kWalkSmem, "smem(walk)");
-  dfa_walk_kernel<<<cgrid, kWalkThreads, kWalkSmem, st>>>(t, p, rows, n_full);
+  if (P.class_image) {
+    set_smem(dfa_walk_kernel<true>, kWalkSmem, "smem(walk)");
+    dfa_walk_kernel<true><<<cgrid, kWalkThreads, kWalkSmem, st>>>(t, p, rows, n_full);
+  } else {
+    set_smem(dfa_walk_kernel<false>, kWalkSmem, "smem(walk)");
+    dfa_walk_kernel<false><<<cgrid, kWalkThreads, kWalkSmem, st>>>(t, p, rows, n_full);
+  }
   check_cuda(cudaGetLastError(), "dfa_walk_kernel");
   launches++;
   mark(2);
@@ -1191,9 +1230,10 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
   const uint64_t fper = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count / P.n_spec,
                                                                   (p.n_chunks + kWalkThreads - 1) / kWalkThreads));
   dim3 fgrid(P.n_spec, (unsigned)fper);
-  set_smem(dfa_fixup_kernel, kFixSmem, "smem(fixup)");
+  auto fixup = P.class_image ? dfa_fixup_kernel<true> : dfa_fixup_kernel<false>;
+  set_smem(fixup, kFixSmem, "smem(fixup)");
   for (int r = 0; r < kFixRounds; ++r) {
-    dfa_fixup_kernel<<<fgrid, kWalkThreads, kFixSmem, st>>>(t, p, r);
+    fixup<<<fgrid, kWalkThreads, kFixSmem, st>>>(t, p, r);
     check_cuda(cudaGetLastError(), "dfa_fixup_kernel");
     launches++;
   }
@@ -1286,7 +1326,7 @@ void rank_states(GroupBuild& gb) {
   for (int s = 1; s < n; ++s) (in_u[(size_t)s] ? us : as).push_back((uint32_t)s);
   std::stable_sort(us.begin(), us.end(), [&](uint32_t a, uint32_t b) { return pu[a] > pu[b]; });
   std::stable_sort(as.begin(), as.end(), [&](uint32_t a, uint32_t b) { return pa[a] > pa[b]; });
-  gb.n_hot_u = (uint32_t)std::min<size_t>(us.size(), kHotRows);
+  gb.n_hot_u = (uint32_t)std::min<size_t>(us.size(), std::max(kHotRows, walk_hot_rows((uint32_t)C)));
   gb.n_hot_a = (uint32_t)std::min<size_t>(as.size(), kHotRows);
   std::vector<uint32_t> order;
   order.insert(order.end(), us.begin(), us.begin() + gb.n_hot_u);
@@ -1362,6 +1402,10 @@ void layout_forward(RegexPlan& P) {
   P.fwd.clear(); P.hot.clear(); P.mptr.clear(); P.mlist.clear();
   P.total_states = 0;
   P.max_classes = 0;
+  // small alphabets (every speculative group with at most
+  // kClassImageMaxClasses classes) index the walk's image by class
+  P.class_image = P.n_spec > 0;
+  for (uint32_t g = 0; g < P.n_spec; ++g) P.class_image &= (uint32_t)P.fcls[g].count <= kClassImageMaxClasses;
   for (uint32_t g = 0; g < P.n_groups; ++g) {
     const Dfa& d = P.fdfa[g];
     const ByteClasses& bc = P.fcls[g];
@@ -1374,20 +1418,17 @@ void layout_forward(RegexPlan& P) {
     gd.start_unanchored = d.start_unanchored;
     // slow words carry the next row in 27 bits; larger DFAs walk through L2 only
     const bool fits = d.n_states < (1 << 27);
-    // trap: the unanchored image of the walk and the fix-up, whose every
-    // transition that is not into a hot row without a match is the trap
-    // column's offset (an absorbing column: its entries are its own offset);
-    // else slow words (the anchored image of the plain kernel)
-    auto image = [&](uint32_t first, uint32_t rows, bool trap) {
+    // The anchored image of the plain kernel: byte-indexed, slow words for
+    // transitions that are not into a hot row without a match.
+    auto image = [&](uint32_t first, uint32_t rows) {
       uint32_t off = (uint32_t)P.hot.size();
       if (!rows) return off;
-      P.hot.resize(P.hot.size() + kImgWords, trap ? kTrapByte : (S_SLOW | S_TRAP));
+      P.hot.resize(P.hot.size() + kImgWords, S_SLOW | S_TRAP);
       uint32_t* img = P.hot.data() + off;
       auto entry = [&](uint32_t w) -> uint32_t {
         uint32_t n = w & DFA_MASK_STATE, nl = n - first;
         bool match = w & DFA_FLAG_MATCH, dead = w & DFA_FLAG_DEAD, hot = nl < rows;
         if (!match && !dead && hot) return nl == 0 ? 0u : slot_word(nl) * 4;
-        if (trap) return kTrapByte;
         return S_SLOW | (match ? S_MATCH : 0u) | (hot ? 0u : S_COLD) | (dead ? S_DEAD : 0u) | n;
       };
       for (uint32_t r = 0; r < rows; ++r)
@@ -1398,12 +1439,39 @@ void layout_forward(RegexPlan& P) {
         }
       return off;
     };
+    // The walk's image of the unanchored hot rows (the walk and the fix-up):
+    // 32-row blocks of `cols` entries per row (256 by byte, or C by class),
+    // as many blocks as fit in kWalkImgBytes; every transition that is not
+    // into a hot row without a match is the trap column's offset (an
+    // absorbing column: its entries are its own offset).
+    auto walk_image = [&](uint32_t rows, uint32_t cols) {
+      const uint32_t blk = cols * 32, nblk = (kWalkImgBytes / 4) / blk, trap = blk * 4;
+      uint32_t off = (uint32_t)P.hot.size();
+      gd.img_cols = cols;
+      gd.img_bytes = nblk * blk * 4;
+      if (!rows) return off;
+      P.hot.resize(P.hot.size() + (size_t)nblk * blk, trap);
+      uint32_t* img = P.hot.data() + off;
+      auto slot = [&](uint32_t r) { return (1 + r / 32) * blk + r % 32; };
+      for (uint32_t r = 0; r < rows; ++r)
+        for (uint32_t c = 0; c < cols; ++c) {
+          const uint32_t w = d.trans[(size_t)r * C + (cols == 256 ? bc.map[c] : c)];
+          const uint32_t n = w & DFA_MASK_STATE;
+          const bool fast = !(w & (DFA_FLAG_MATCH | DFA_FLAG_DEAD)) && n < rows;
+          const uint32_t e = fast ? (n == 0 ? 0u : slot(n) * 4) : trap;
+          if (r == 0) for (uint32_t l = 0; l < 32; ++l) img[c * 32 + l] = e;
+          else img[slot(r) + c * 32] = e;
+        }
+      return off;
+    };
     const bool spec = g < P.n_spec;
-    gd.hot_rows = fits && spec ? std::min(P.nhot_u[g], kHotRowsWalk) : 0;
-    gd.hot_off = image(0, gd.hot_rows, true);
+    const uint32_t cols = P.class_image ? C : 256;
+    const uint32_t walk_rows = 32 * ((kWalkImgBytes / 4) / (cols * 32) - 1);
+    gd.hot_rows = fits && spec ? std::min(P.nhot_u[g], walk_rows) : 0;
+    gd.hot_off = walk_image(gd.hot_rows, cols);
     gd.ahot_base = P.nhot_u[g];
-    gd.ahot_rows = fits && spec ? P.nhot_a[g] : 0;
-    gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows, false);
+    gd.ahot_rows = fits && spec ? std::min(P.nhot_a[g], kHotRows) : 0;
+    gd.ahot_off = image(P.nhot_u[g], gd.ahot_rows);
     gd.mptr_off = (uint32_t)P.mptr.size();
     // one list per state, or per (state, right context) in a context group
     const size_t n_lists = d.match_ptr.size() - 1;
@@ -1633,7 +1701,7 @@ void regex_rerank_from_corpus(RegexPlan& P, const uint8_t* d_corpus, uint64_t le
     std::stable_sort(us.begin(), us.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
     (void)hu;
     std::vector<uint32_t> order;
-    uint32_t nu = (uint32_t)std::min<size_t>(us.size(), kHotRows);
+    uint32_t nu = (uint32_t)std::min<size_t>(us.size(), std::max(kHotRows, walk_hot_rows(P.groups[g].n_classes)));
     order.insert(order.end(), us.begin(), us.begin() + nu);
     order.insert(order.end(), as.begin(), as.begin() + std::min<size_t>(as.size(), ha));
     order.insert(order.end(), us.begin() + nu, us.end());
@@ -1691,7 +1759,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   clear_marks(P, p, st);
   check_cuda(cudaMemsetAsync(p.ctr, 0, 16 * 8, st), "memset");
   check_cuda(cudaMemsetAsync(p.count, 0, (size_t)P.n_regex * 4, st), "memset");
-  if (ev) check_cuda(record_phase(ev[0], st), "event");
+  if (ev) check_cuda(cudaEventRecord(ev[0], st), "event");
   launches += candidates_phase(P, t, p, l.mode, st, sm_count, ev);
   int hg = (int)std::min<uint64_t>((uint64_t)sm_count * 8, (L.k_cap + 255) / 256);
   k_hist_kernel<<<hg, 256, 0, st>>>(p);
@@ -1714,7 +1782,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
       P.prof_ctr.reset(h);
     }
     check_cuda(cudaMemcpyAsync(P.prof_ctr.get(), p.ctr, 16 * 8, cudaMemcpyDeviceToHost, st), "D2H counters");
-    check_cuda(record_phase(ev[5], st), "event");
+    check_cuda(cudaEventRecord(ev[5], st), "event");
   }
   P.last_chunks = L.n_q;
   P.last_launches = launches;

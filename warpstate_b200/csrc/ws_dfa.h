@@ -36,6 +36,14 @@ constexpr uint32_t kHotRows = 192;
 // of the image's seven 32 KiB blocks (the first row and rows 1..159) and keep
 // the rest of their shared memory for input stages.
 constexpr uint32_t kHotRowsWalk = 160;
+// Groups of at most this many byte classes (small alphabets: nucleotides)
+// index the walk's image by class: a row takes `classes` words instead of
+// 256, so the same 192 KiB hold 32 x (49152 / (32 x classes) - 1) hot rows.
+constexpr uint32_t kClassImageMaxClasses = 32;
+// Unanchored hot rows of a group with `classes` byte classes.
+constexpr uint32_t walk_hot_rows(uint32_t classes) {
+  return classes <= kClassImageMaxClasses ? 32 * (49152 / (32 * classes) - 1) : kHotRowsWalk;
+}
 
 struct GroupDev {
   uint32_t fwd_off;          // class-indexed forward table (u32 words)
@@ -50,6 +58,9 @@ struct GroupDev {
   // context, and match lists per (row, right context) at mptr[4 * row + k].
   uint32_t context;
   uint32_t cstart[4];
+  // The unanchored image of the walk: entries per row (256 byte-indexed, or
+  // the group's class count when class-indexed) and the bytes staged.
+  uint32_t img_cols, img_bytes;
 };
 
 struct Proposer;
@@ -66,6 +77,7 @@ struct RegexPlan {
   // per start position in both modes.
   uint32_t n_spec = 0;
   bool has_context = false;              // some regex has a look-around assertion
+  bool class_image = false;              // the speculative groups' walk images are class-indexed
   uint32_t total_states = 0;
   uint32_t max_classes = 0;
   int64_t max_len = 0;                   // longest match (-1 unbounded)
