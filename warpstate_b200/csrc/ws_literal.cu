@@ -86,14 +86,6 @@ __device__ __forceinline__ uint32_t nib(const uint32_t* tab, uint32_t gram, uint
   return (tab[h >> 3] >> ((h & 7) << 2)) & 0xFu;
 }
 
-// Stage 1b: a nibble that passed the shared-memory table is checked again in
-// the larger table in L2 (same gram hash, more bits), only where it is
-// non-zero: one predicated load per passing gram.
-__device__ __forceinline__ uint32_t nib_big(const uint8_t* big, uint32_t h_full, uint32_t n) {
-  if (!n) return 0;
-  return n & __ldg(big + (h_full >> (32 - kBigBits)));
-}
-
 // Loads the 16 bytes of vector v, zero-filling past the end of the input.
 __device__ __forceinline__ uint4 load_vec(const uint8_t* data, uint64_t len, uint64_t v) {
   uint64_t off = v * 16;
@@ -193,19 +185,21 @@ __device__ __forceinline__ uint32_t stage1(const uint32_t* filt, const uint32_t*
         else if (G == 8) h[j] = mix_words(w[j], w[j + 1], 0, 0, 8);
         else h[j] = mix_words(w[j], w[j + 1], w[j + 2], w[j + 3], 16);
       }
+      // with the stage-1b table, shared memory holds the 2^kLeanBits-bit
+      // bitmap derived from it and the phase bits come from stage 1b alone
+      auto phases = [&](uint32_t hf) -> uint32_t {
+        if (big) {
+          const uint32_t b = hf >> (32 - kLeanBits);
+          return ((filt[b >> 5] >> (b & 31)) & 1u) ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
+        }
+        const uint32_t hs = hf >> (32 - bits);
+        return (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
+      };
       uint32_t n[5];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint32_t hs = h[j] >> (32 - bits);
-        n[j] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
-        if (big) n[j] = nib_big(big, h[j], n[j]);
-      }
+      for (int j = 0; j < 4; ++j) n[j] = phases(h[j]);
       n[4] = __shfl_down_sync(0xFFFFFFFFu, n[0], 1);
-      if (lane == 31) {
-        const uint32_t hs = h[4] >> (32 - bits);
-        n[4] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
-        if (big) n[4] = nib_big(big, h[4], n[4]);
-      }
+      if (lane == 31) n[4] = phases(h[4]);
       const uint32_t m = n[0] | (n[1] << 4) | (n[2] << 8) | (n[3] << 12) | (n[4] << 16);
       mask |= (m >> 3) & 0xFFFFu;
     } else if (P == 2) {
@@ -424,9 +418,10 @@ __device__ __forceinline__ void grams_issue(const uint32_t* filt, const uint8_t*
     if (G == 4) hf = w[j] * 0x9E3779B1u;
     else if (G == 8) hf = mix_words(w[j], w[j + 1], 0, 0, 8);
     else hf = mix_words(w[j], w[j + 1], w[j + 2], w[j + 3], 16);
-    const uint32_t hs = hf >> (32 - bits);
+    // stage 1: the 2^kLeanBits-bit bitmap derived from the stage-1b table
+    const uint32_t b = hf >> (32 - kLeanBits);
     s.h[j] = hf;
-    s.n[j] = (filt[hs >> 3] >> ((hs & 7) << 2)) & 0xFu;
+    s.n[j] = ((filt[b >> 5] >> (b & 31)) & 1u) ? 0xFu : 0u;
     s.bw[j] = s.n[j] ? __ldg(big + (hf >> (32 - kBigBits))) : 0u;
   }
 }
@@ -755,7 +750,8 @@ __global__ void __launch_bounds__(256) literal_verify_kernel(LitArgs a) {
 }  // namespace
 
 size_t literal_smem_bytes(const LiteralPlan& plan) {
-  return (plan.filter.size() + (1u << (kBloomBits - 5)) + (plan.has_short ? 2048 : 0) +
+  const size_t filter_words = plan.has_big ? ((size_t)1 << (kLeanBits - 5)) : plan.filter.size();
+  return (filter_words + (1u << (kBloomBits - 5)) + (plan.has_short ? 2048 : 0) +
           (size_t)kWarps * (kBlockWords + kQueue / 2)) * 4;
 }
 
@@ -766,8 +762,9 @@ void launch_literal_scan(const LiteralPlan& plan, const LiteralLaunch& l, cudaSt
   LitArgs a;
   a.data = l.data;
   a.len = l.len;
-  a.filter = plan.d_filter.as<uint32_t>();
-  a.filter_words = (uint32_t)plan.filter.size();
+  // with a stage-1b table, stage 1 in shared memory is its bitmap
+  a.filter = plan.has_big ? plan.d_lean_bits.as<uint32_t>() : plan.d_filter.as<uint32_t>();
+  a.filter_words = plan.has_big ? (1u << (kLeanBits - 5)) : (uint32_t)plan.filter.size();
   a.bits = plan.table_bits;
   a.period = plan.period;
   a.has_long = plan.has_long;
