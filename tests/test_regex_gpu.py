@@ -109,6 +109,38 @@ def test_regex_config_scaled_vs_oracle(mode):
     assert got.shape == exp.shape and np.array_equal(got, exp)
 
 
+@pytest.mark.parametrize("mode", [PLAIN, SPEC])
+@pytest.mark.parametrize("wide", [False, True])
+def test_walk_image_layouts_vs_oracle(mode, wide):
+    # the walk's image is indexed by class when every speculative group has at
+    # most 32 byte classes, else by byte: a set over a few letters and one over
+    # digits, letters and punctuation (more than 32 classes) take the two
+    # layouts; both against the oracle, with small chunks so that the fix-up
+    # re-walks many chunks over the same image
+    rng = np.random.default_rng(91 if wide else 92)
+    alpha = (b"0123456789abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ_:=@!%,;/" if wide
+             else b"abcdefghijkl")
+    pats = []
+    for k in range(120):
+        lits = [rng.choice(list(alpha), size=int(rng.integers(4, 9))).astype(np.uint8).tobytes() for _ in range(3)]
+        cls = b"[" + bytes(sorted(set(rng.choice(list(alpha), size=4).tolist()))) + b"]"
+        src = b"(?:" + b"|".join(lits) + b")" + cls + b"{1,4}"
+        pats.append((1, src))
+    text = np.frombuffer(alpha, dtype=np.uint8)[rng.integers(0, len(alpha), 3 << 20)].copy()
+    for k in range(400):  # plant matches: a pattern's first literal and one byte of its class
+        src = pats[k % len(pats)][1].decode()
+        lit = src[3:src.index("|")] + src[src.index("[") + 1]
+        at = int(rng.integers(0, text.size - 16))
+        text[at:at + len(lit)] = np.frombuffer(lit.encode(), dtype=np.uint8)
+    m = matcher(pats, mode=mode, walk_chunk=256)
+    info = m.info()
+    assert (info["max_classes"] > 32) == wide
+    got = m.scan_array(text.tobytes())
+    exp = oracle.scan_patterns(pats, text.tobytes())
+    assert len(exp) > 100
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
 def test_candidate_sets_plain_equals_speculative():
     pats, data = _regex_workload(2 << 20, 200, 5)
     m = matcher(pats)
