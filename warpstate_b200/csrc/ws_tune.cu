@@ -99,10 +99,9 @@ extern "C" ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint6
 
       // 1. group size: re-plan at each limit, rank hot rows on the corpus, time
       if (flags & WS_TUNE_GROUPS) {
-        std::vector<uint32_t> cands = {8192, 16384, 32768};
-        if (std::find(cands.begin(), cands.end(), m->cfg.dfa_max_states) == cands.end())
-          cands.insert(cands.begin(), m->cfg.dfa_max_states);
-        cands.resize(std::min<size_t>(cands.size(), 4));
+        // larger groups mean fewer lookups per input byte, as long as their
+        // visited rows stay hot (the class-indexed image holds up to 1,472)
+        std::vector<uint32_t> cands = {16384, 32768, 65536, 131072};
         std::vector<const char*> ptrs;
         const ws_pattern_tables t = regex_tables(m, ptrs);
         double best = 1e300;
