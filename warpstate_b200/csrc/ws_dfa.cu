@@ -1746,10 +1746,31 @@ void ensure_scratch(DeviceBuffer& scratch, size_t need) {
 
 }  // namespace
 
+namespace {
+
+// The walk chunk of one scan: the plan's chunk, made smaller (to at least half
+// of it, in steps of kCkpt) when that fills the last wave of walk blocks --
+// one 1,024-chunk block per SM and group -- so that no SM sits idle while the
+// others walk (one group over 1 GiB in 8 KiB chunks is 128 blocks on 148 SMs;
+// 7 KiB chunks make it 147).
+uint32_t effective_chunk(const RegexPlan& P, uint64_t len, int sm_count) {
+  const uint64_t c0 = P.walk_chunk, G = std::max<uint32_t>(P.n_spec, 1), sm = (uint64_t)std::max(sm_count, 1);
+  auto blocks = [&](uint64_t c) { return G * (((len + c - 1) / c + kWalkThreads - 1) / kWalkThreads); };
+  const uint64_t waves = (blocks(c0) + sm - 1) / sm;
+  const uint64_t per_group = waves * sm / G;  // blocks per group that fill `waves` waves
+  if (per_group == 0) return (uint32_t)c0;
+  uint64_t c = (len + per_group * kWalkThreads - 1) / (per_group * kWalkThreads);
+  c = (c + kCkpt - 1) / kCkpt * kCkpt;
+  c = std::max<uint64_t>(c, std::max<uint64_t>(kCkpt, c0 / 2 / kCkpt * kCkpt));
+  return (uint32_t)std::min<uint64_t>(c, c0);
+}
+
+}  // namespace
+
 uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch, int sm_count,
                         cudaEvent_t* ev) {
   if (!P.n_regex || l.len == 0) return 0;
-  RxLayout L = layout(P, l.len, P.walk_chunk, l.cap, l.k_min, l.ev_min);
+  RxLayout L = layout(P, l.len, effective_chunk(P, l.len, sm_count), l.cap, l.k_min, l.ev_min);
   ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   // profiled speculative scans count the boundary guesses that held
@@ -1816,7 +1837,7 @@ uint64_t regex_candidates(RegexPlan& P, const uint8_t* d_data, uint64_t len, uin
   mode &= ~(uint32_t)WS_CAND_DISTINCT;
   RegexLaunch l{d_data, len, nullptr, cap, nullptr, mode};
   // every candidate must fit: the buffers are sized for the caller's capacity
-  RxLayout L = layout(P, len, P.walk_chunk, std::max<uint64_t>(cap, 1), cap, cap);
+  RxLayout L = layout(P, len, effective_chunk(P, len, sm_count), std::max<uint64_t>(cap, 1), cap, cap);
   ensure_scratch(scratch, L.total);
   ScanPtrs p = make_ptrs(L, scratch.ptr, l);
   p.full_k = full ? 1 : 0;
