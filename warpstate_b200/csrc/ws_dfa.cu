@@ -818,9 +818,12 @@ __global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs 
       uint32_t w = __ldg(tab + st * C + __ldg(cm + __ldg(p.data + pos - 1)));
       if (w & F_DEAD) break;
       st = w & F_MASK;
-      if (p.rmark) {
-        // (pos - 1, g, st) fixes the rest of the walk: stop where another
-        // walk has been (it reports these starts), else leave a mark first
+      // (pos - 1, g, st) fixes the rest of the walk: stop where another walk
+      // has been (it reports these starts), else leave a mark first; marks
+      // are kept at every eighth position only (the same positions for every
+      // walk), which keeps a long run of match ends linear at an eighth of
+      // the mark traffic
+      if (p.rmark && ((pos - 1) & 7) == 0) {
         const uint32_t at = (uint32_t)(pos - 1);
         const unsigned long long key =
             ((unsigned long long)at << 32) | ((unsigned long long)g << kRmarkStateBits) | st;
@@ -992,18 +995,30 @@ __device__ uint32_t lf_walk(const DevTables& t, const ScanPtrs& p, uint32_t r, u
 
 // Leftmost-first end of every distinct candidate start (in parallel), each
 // walk cut off after kLfCap bytes.
+// The regexes' candidate offsets are staged in shared memory when they fit
+// (kLfOffsShared regexes), so that finding a candidate's regex is a binary
+// search in shared memory rather than a chain of dependent global loads.
+constexpr uint32_t kLfOffsShared = 8192;
+
 __global__ void k_lf_kernel(DevTables t, ScanPtrs p, uint32_t n_regex) {
-  const uint32_t total = p.offs[n_regex];
+  extern __shared__ uint32_t offs_s[];
+  const bool staged = n_regex < kLfOffsShared;
+  if (staged) {
+    for (uint32_t r = threadIdx.x; r <= n_regex; r += blockDim.x) offs_s[r] = p.offs[r];
+    __syncthreads();
+  }
+  const uint32_t* offs = staged ? offs_s : p.offs;
+  const uint32_t total = offs[n_regex];
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
     // owning regex: binary search in offs
     uint32_t lo = 0, hi = n_regex;
     while (hi - lo > 1) {
       uint32_t mid = (lo + hi) >> 1;
-      if (p.offs[mid] <= j) lo = mid; else hi = mid;
+      if (offs[mid] <= j) lo = mid; else hi = mid;
     }
     const uint32_t r = lo;
     const uint32_t s = p.starts[j];
-    if (j > p.offs[r] && p.starts[j - 1] == s) { p.lfend[j] = kLfNone; continue; }  // duplicate
+    if (j > offs[r] && p.starts[j - 1] == s) { p.lfend[j] = kLfNone; continue; }  // duplicate
     p.lfend[j] = lf_walk(t, p, r, s, kLfCap);
   }
 }
@@ -1024,11 +1039,16 @@ __global__ void k_chain_kernel(DevTables t, ScanPtrs p) {
   // frontier (both in stream offsets; the buffer starts at p.base <= cursor)
   uint64_t last_end = (p.cursor64 && p.cursor64[r] > p.base) ? p.cursor64[r] - p.base : 0;
   const uint64_t limit = p.cursor64 ? p.frontier - p.base : ~0ull;
+  // each window's candidates are loaded while the previous window is decided
+  uint32_t e_nx = a + lane < b ? p.lfend[a + lane] : kLfNone;
+  uint32_t s_nx = a + lane < b ? p.starts[a + lane] : 0xFFFFFFFFu;
   for (uint32_t j0 = a; j0 < b; j0 += 32) {
     const uint32_t j = j0 + lane;
     const bool in = j < b;
-    uint32_t e = in ? p.lfend[j] : kLfNone;
-    const uint32_t s = in ? p.starts[j] : 0xFFFFFFFFu;
+    uint32_t e = e_nx;
+    const uint32_t s = s_nx;
+    e_nx = j + 32 < b ? p.lfend[j + 32] : kLfNone;
+    s_nx = j + 32 < b ? p.starts[j + 32] : 0xFFFFFFFFu;
     const bool past = in && (uint64_t)s >= limit;
     bool picked = false;
     while (true) {
@@ -1787,7 +1807,7 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   k_scan_kernel<<<1, 1024, 0, st>>>(p, P.n_regex);
   k_scatter_kernel<<<hg, 256, 0, st>>>(p);
   k_sort_kernel<<<(unsigned)std::min<uint32_t>(P.n_regex, 4096), 512, 0, st>>>(p, P.n_regex);
-  k_lf_kernel<<<sm_count * 8, 128, 0, st>>>(t, p, P.n_regex);
+  k_lf_kernel<<<sm_count * 8, 128, P.n_regex < kLfOffsShared ? (P.n_regex + 1) * 4 : 0, st>>>(t, p, P.n_regex);
   k_chain_kernel<<<(P.n_regex + 3) / 4, 128, 0, st>>>(t, p);  // a warp per regex
   check_cuda(cudaGetLastError(), "resolution kernels");
   launches += 6;
