@@ -227,13 +227,15 @@ void plan_literals(const ws_pattern_tables& given, LiteralPlan& plan) {
       plan.d_bloom2.upload(plan.bloom2.data(), plan.bloom2.size() * 4);
     }
   }
-  // Stage 1b: when more than 0.5% of the shared table's phase bits are set,
-  // a 2^kBigBits-byte table in L2 (the same full 32-bit gram hashes, more
-  // of their bits) re-checks each passing gram.
-  if (plan.has_long && P == 4) {
+  // Stage 1b: when more than 0.5% (P = 4) or 0.1% (P = 2: nine grams per
+  // 16 bytes, each passing one sends the warp block to compaction) of the
+  // shared table's phase bits are set, a 2^kBigBits-byte table in L2 (the
+  // same full 32-bit gram hashes, more of their bits) re-checks each passing
+  // gram.
+  if (plan.has_long && (P == 4 || P == 2)) {
     uint64_t set = 0;
     for (uint32_t w : plan.filter) set += (uint64_t)__builtin_popcount(w);
-    if ((double)set / (double)((uint64_t)plan.filter.size() * 32) > 0.005) {
+    if ((double)set / (double)((uint64_t)plan.filter.size() * 32) > (P == 4 ? 0.005 : 0.001)) {
       const uint32_t G = plan.gram_len;
       plan.big.assign((size_t)1 << kBigBits, 0);
       for (uint32_t li = 0; li < t.n_literals; ++li) {

@@ -207,7 +207,14 @@ __device__ __forceinline__ uint32_t stage1(const uint32_t* filt, const uint32_t*
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
         uint32_t g = (j & 1) ? __funnelshift_r(w[j >> 1], w[(j >> 1) + 1], 16) : w[j >> 1];
-        m |= nib(filt, g, bits) << (2 * j);
+        uint32_t n;
+        if (big) {  // the bitmap of the stage-1b table, then its phase bits
+          const uint32_t hf = g * 0x9E3779B1u, b = hf >> (32 - kLeanBits);
+          n = ((filt[b >> 5] >> (b & 31)) & 1u) ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
+        } else {
+          n = nib(filt, g, bits);
+        }
+        m |= n << (2 * j);
       }
       mask |= (m >> 1) & 0xFFFFu;
     } else {
