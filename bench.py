@@ -248,36 +248,6 @@ def run_reference(args, rank):
 
 
 # ------------------------------------------------------------------ ours
-def build_matchers(ws, wl, config, walk_chunk=None, proposer=True, dfa_max_states=None):
-    ps = ws.PatternSet.builder()
-    for kind, p in wl.patterns:
-        ps = ps.literal_bytes(p) if kind == 0 else ps.regex(p.decode())
-    ps = ps.build()
-    cfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_SPECULATIVE)
-    if walk_chunk:
-        cfg.walk_chunk(walk_chunk)
-    if dfa_max_states:
-        cfg.dfa_max_states(dfa_max_states)
-    if not proposer:
-        cfg.proposer(ws.PROPOSER_NONE)
-    m = ws.GpuMatcher.with_config(ps, cfg)
-    plain = None
-    has_regex = any(k == 1 for k, _ in wl.patterns)
-    if has_regex and config in ("regex", "batch", "dna"):
-        pcfg = ws.AutoMatcherConfig().max_matches(CAP).profile(True).regex_mode(ws.REGEX_PLAIN)
-        plain = ws.GpuMatcher.with_config(ps, pcfg)
-    tune = None
-    if has_regex:
-        # a separately seeded 256 MiB corpus of the same distribution: the
-        # autotuner picks group size, hot rows, proposer and chunk on it (knobs
-        # given on the command line stay fixed)
-        corpus = W.dna_training_corpus() if config == "dna" else W.regex_training_corpus()
-        flags = (0 if dfa_max_states else ws.GpuMatcher.TUNE_GROUPS) | (0 if walk_chunk else ws.GpuMatcher.TUNE_CHUNK)
-        tune = m.tune(corpus, flags=flags)
-        del corpus
-    return m, plain, tune
-
-
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -355,6 +325,8 @@ class Runner:
             dist.barrier()
         torch.cuda.synchronize()
         total, infos = 0.0, []
+        # per step: device time, and host time of the scan call (the enqueue)
+        self.step_ms, self.enqueue_ms = [], []
         torch.cuda.nvtx.range_push("timed")  # lets a profiler capture only the timed steps
         for _ in range(steps):
             if self.flush is not None:
@@ -362,10 +334,13 @@ class Runner:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(self.stream)
+            h0 = time.perf_counter()
             self.step(matcher)
+            self.enqueue_ms.append((time.perf_counter() - h0) * 1e3)
             e1.record(self.stream)
             e1.synchronize()
             total += e0.elapsed_time(e1)
+            self.step_ms.append(e0.elapsed_time(e1))
             infos.append(matcher.info())
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
@@ -526,6 +501,8 @@ def main():
     with ClockSampler(local) as clk:
         ms, infos = r.timed_steps(m, args.steps, args.warmup)
     clocks = clk.summary()
+    step_ms = [round(x, 4) for x in r.step_ms]
+    enqueue_ms = round(sum(r.enqueue_ms) / max(1, len(r.enqueue_ms)), 4)
     count = r.count()
     ms_max = max_over_ranks(ms)
     value = world * n_bytes / (ms_max * 1e-3) / 1e9
@@ -682,6 +659,8 @@ def main():
                "proposer_top1_heldout": last["proposer_top1"], "proposer_top4_heldout": last["proposer_top4"],
                "tune": tune, "groups": last["n_groups"], "states": last["total_states"]}
         rec.update(walk_record(last, n_bytes, ms_max))
+        rec["step_ms"] = step_ms
+        rec["enqueue_ms"] = enqueue_ms
         if arms:
             rec["arms"] = arms
         line["regex"] = rec

@@ -125,10 +125,14 @@ struct LiteralPlan {
   // sparse enough; the host copy is released once uploaded (has_big).
   std::vector<uint8_t> big;
   bool has_big = false;
-  // With the stage-1b table: stage 1 of the lean kernel, a bitmap indexed by
-  // the top kLeanBits bits of the same hashes (a bit is set when any of the
-  // 2^(kBigBits - kLeanBits) stage-1b bytes below it is non-zero), so that
-  // only about 3% of the grams of text-like input go on to a stage-1b load.
+  // With the stage-1b table: stage 1 in shared memory, 2^kLeanBits bits.
+  // For 4-byte grams a bitmap indexed by the top kLeanBits bits of the same
+  // hashes (a bit is set when any of the 2^(kBigBits - kLeanBits) stage-1b
+  // bytes below it is non-zero), so that only about 3% of the grams of
+  // text-like input go on to a stage-1b load.  For long grams (dense k-mer
+  // sets) a blocked Bloom filter with two bits per gram (lean2_word,
+  // lean2_mask), which passes 11% instead of 17% of the grams of a
+  // 200,000-gram set.
   std::vector<uint8_t> lean_bits;
   DeviceBuffer d_filter, d_bloom, d_short, d_info, d_bytes, d_meta, d_ranges, d_entries, d_bloom2, d_big,
       d_lean_bits;
@@ -154,6 +158,15 @@ __host__ __device__ inline uint32_t ascii_fold4(uint32_t w) {
 constexpr uint32_t kBloom2Bits = 24;  // 2 MiB, read through L2
 constexpr uint32_t kBigBits = 25;     // stage-1b table: 2^25 bytes, 32 MiB, read through L2
 constexpr uint32_t kLeanBits = 20;    // stage 1 of the lean kernel: a 2^20-bit bitmap, 128 KiB of shared memory
+
+// Blocked Bloom filter of stage 1 for long grams with the stage-1b table: the
+// word of 32-bit gram hash hf (its top kLeanBits - 5 bits) and the two bits
+// set in it (five-bit fields of a second multiplicative hash of hf).
+__host__ __device__ inline uint32_t lean2_word(uint32_t hf) { return hf >> (32 - (kLeanBits - 5)); }
+__host__ __device__ inline uint32_t lean2_mask(uint32_t hf) {
+  const uint32_t h2 = hf * 0x2545F491u;
+  return (1u << (h2 >> 27)) | (1u << ((h2 >> 22) & 31u));
+}
 
 // Gram hash of stage 1 (a multiplicative hash; the constant is 2^32 / phi).
 inline uint32_t gram_hash(uint32_t gram, uint32_t bits) { return (gram * 0x9E3779B1u) >> (32 - bits); }

@@ -238,6 +238,7 @@ void plan_literals(const ws_pattern_tables& given, LiteralPlan& plan) {
     if ((double)set / (double)((uint64_t)plan.filter.size() * 32) > (P == 4 ? 0.005 : 0.001)) {
       const uint32_t G = plan.gram_len;
       plan.big.assign((size_t)1 << kBigBits, 0);
+      std::vector<uint32_t> lean2(G > 4 ? (size_t)1 << (kLeanBits - 5) : 0, 0u);
       for (uint32_t li = 0; li < t.n_literals; ++li) {
         const uint32_t len = t.offsets[2 * li + 1];
         const uint8_t* lit = t.packed_bytes + t.offsets[2 * li];
@@ -250,15 +251,20 @@ void plan_literals(const ws_pattern_tables& given, LiteralPlan& plan) {
                                        : mix_words(g[0], g[1], g[2], g[3], 16);
           const uint32_t h = hf >> (32 - kBigBits);
           plan.big[h] |= (uint8_t)(1u << (P - 1 - k));
+          if (G > 4) lean2[lean2_word(hf)] |= lean2_mask(hf);
         }
       }
       plan.d_big.upload(plan.big.data(), plan.big.size());
       plan.lean_bits.assign((size_t)1 << (kLeanBits - 3), 0);
-      for (size_t h = 0; h < plan.big.size(); ++h)
-        if (plan.big[h]) {
-          const size_t b = h >> (kBigBits - kLeanBits);
-          plan.lean_bits[b >> 3] |= (uint8_t)(1u << (b & 7));
-        }
+      if (G > 4) {
+        std::memcpy(plan.lean_bits.data(), lean2.data(), plan.lean_bits.size());
+      } else {
+        for (size_t h = 0; h < plan.big.size(); ++h)
+          if (plan.big[h]) {
+            const size_t b = h >> (kBigBits - kLeanBits);
+            plan.lean_bits[b >> 3] |= (uint8_t)(1u << (b & 7));
+          }
+      }
       plan.d_lean_bits.upload(plan.lean_bits.data(), plan.lean_bits.size());
       plan.has_big = true;
       std::vector<uint8_t>().swap(plan.big);

@@ -72,7 +72,7 @@ struct LitArgs {
   uint32_t parts16;          // stage-1.5b key lengths (bit i: i+1 bytes)
   const uint32_t* bloom2;    // stage-1.5b bitmap (2^kBloom2Bits bits, L2), or null
   const uint8_t* big;        // stage-1b gram table (2^kBigBits bytes, L2), or null
-  const uint32_t* lean_bits; // stage-1 bitmap of the lean kernel (2^kLeanBits bits), or null
+  const uint32_t* lean_bits; // stage 1 with the stage-1b table (2^kLeanBits bits), or null
   uint32_t verify_bloom;     // the verify kernel runs stage 1.5 first
   uint32_t fold;             // ASCII case-insensitive: input bytes A-Z read as a-z
 };
@@ -185,9 +185,14 @@ __device__ __forceinline__ uint32_t stage1(const uint32_t* filt, const uint32_t*
         else if (G == 8) h[j] = mix_words(w[j], w[j + 1], 0, 0, 8);
         else h[j] = mix_words(w[j], w[j + 1], w[j + 2], w[j + 3], 16);
       }
-      // with the stage-1b table, shared memory holds the 2^kLeanBits-bit
-      // bitmap derived from it and the phase bits come from stage 1b alone
+      // with the stage-1b table, shared memory holds its stage 1 (the
+      // two-bit blocked Bloom filter of long grams, or the bitmap derived
+      // from the table) and the phase bits come from stage 1b alone
       auto phases = [&](uint32_t hf) -> uint32_t {
+        if (big && G > 4) {
+          const uint32_t m = lean2_mask(hf);
+          return (filt[lean2_word(hf)] & m) == m ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
+        }
         if (big) {
           const uint32_t b = hf >> (32 - kLeanBits);
           return ((filt[b >> 5] >> (b & 31)) & 1u) ? (uint32_t)__ldg(big + (hf >> (32 - kBigBits))) : 0u;
