@@ -369,6 +369,16 @@ class Runner:
         return rec
 
 
+def boundary_guess(info, tune) -> str:
+    """How the speculative walk chose each chunk's start state."""
+    spec = info["n_groups"] - info["n_context_groups"]
+    if spec and info["exact_groups"] == spec:
+        return "exact: each chunk's start state from the bytes before it (every regex of bounded length)"
+    if tune and tune["proposer_used"]:
+        return "learned proposer (top-1)"
+    return "unanchored start state (the autotuner turned the proposer off)"
+
+
 def build_matchers(ws, wl, config, walk_chunk=None, proposer=True, dfa_max_states=None, plain_too=True):
     ps = ws.PatternSet.builder()
     for kind, p in wl.patterns:
@@ -590,8 +600,11 @@ def main():
         torch.cuda.synchronize()
         k = max(2, min(args.steps, 5)) if n_bytes < (2 << 30) else 2
         t0 = time.perf_counter()
+        call_ms = []
         for _ in range(k):
+            c0 = time.perf_counter()
             res = call()
+            call_ms.append(round((time.perf_counter() - c0) * 1e3, 3))
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / k
         if len(res) != count:
@@ -608,7 +621,7 @@ def main():
         h2d_gbs = n_bytes * k / (e0.elapsed_time(e1) * 1e-3) / 1e9
         del dbuf
         e2e = {"value": round(world * n_bytes / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": n_bytes,
-               "d2h_bytes_per_step": d2h(count), "ms_per_step": round(dt * 1e3, 3),
+               "d2h_bytes_per_step": d2h(count), "ms_per_step": round(dt * 1e3, 3), "call_ms": call_ms,
                "h2d_copy_gbs": round(h2d_gbs, 2),
                "api": ("scan_batch_packed (ws_scan_batch)" if batch else
                        "StreamPipeline.scan (ws_stream_*)" if r.big else "GpuMatcher.scan (ws_scan)")}
@@ -654,8 +667,7 @@ def main():
                "plain_gbs": round(plain_gbs, 3) if plain_gbs else None,
                "speedup_vs_plain": round(value / plain_gbs, 3) if plain_gbs else None,
                "plain_ms_per_step": round(plain_ms, 4) if plain_ms else None,
-               "boundary_guess": ("learned proposer (top-1)" if tune and tune["proposer_used"]
-                                  else "unanchored start state (the autotuner turned the proposer off)"),
+               "boundary_guess": boundary_guess(last, tune),
                "proposer_top1_heldout": last["proposer_top1"], "proposer_top4_heldout": last["proposer_top4"],
                "tune": tune, "groups": last["n_groups"], "states": last["total_states"]}
         rec.update(walk_record(last, n_bytes, ms_max))

@@ -388,7 +388,9 @@ typedef struct {
   uint32_t last_graph_replay;    /* 1 when the last ws_scan_batch_device call replayed a captured CUDA
                                     graph of its launch sequence (the same arguments as the calls before
                                     it, on a stream other than the legacy default stream, not profiled) */
-  uint32_t reserved;
+  uint32_t exact_groups;         /* speculative groups whose regexes all match at most 512 bytes: the walk
+                                    derives each chunk's start state from the bytes before the chunk (at
+                                    chunks of at least four times that length), so no boundary is guessed */
 } ws_matcher_info;
 ws_status ws_matcher_get_info(const ws_matcher* m, ws_matcher_info* out);
 

@@ -10,6 +10,11 @@ import workloads as w
 
 pytestmark = pytest.mark.gpu
 
+# A regex of unbounded length added to the bounded configuration sets: a group
+# holding it cannot derive its chunk starts from the bytes before each chunk,
+# so the proposer's boundary guesses drive the walk there.
+UNBOUNDED = b"~[0-9]+~"
+
 
 @pytest.mark.parametrize("n", [256, 64, 192])
 def test_tcgen05_gemm_matches_torch_fp32(n):
@@ -36,12 +41,17 @@ def test_tcgen05_and_mma_sync_proposers_agree_and_scan_exactly():
     from warpstate_b200 import _native as N
     wl = w.regex(size=16 << 20, n=150, seed=19)
     corpus = w.fill_markov(16 << 20, w.PRINTABLE, 19 * 1000 + 77, 19 * 1000 + 4)
+    # an unbounded regex: the group holding it has no exact chunk starts, so
+    # the walk takes the proposer's guesses there
+    pats = wl.patterns + [(1, UNBOUNDED)]
     b = ws.PatternSet.builder()
-    for _, p in wl.patterns:
+    for _, p in pats:
         b = b.regex(p.decode())
     m = ws.GpuMatcher.with_config(b.build(), ws.AutoMatcherConfig().regex_mode(ws.REGEX_SPECULATIVE).profile(True))
     m.train_proposer(corpus)
-    exp = oracle.scan_patterns(wl.patterns, wl.data)
+    info = m.info()
+    assert info["exact_groups"] < info["n_groups"] - info["n_context_groups"]
+    exp = oracle.scan_patterns(pats, wl.data)
     sel = N.lib().ws_testing_proposer_path
     sel.restype = None
     sel.argtypes = [ctypes.c_int]
@@ -85,8 +95,9 @@ def test_proposer_training_and_exact_scan():
     import warpstate_b200 as ws
     wl = w.regex(size=8 << 20, n=150, seed=13)
     corpus = w.fill_markov(16 << 20, w.PRINTABLE, 13 * 1000 + 77, 13 * 1000 + 4)
+    pats = wl.patterns + [(1, UNBOUNDED)]
     b = ws.PatternSet.builder()
-    for _, p in wl.patterns:
+    for _, p in pats:
         b = b.regex(p.decode())
     ps = b.build()
     m = ws.GpuMatcher.with_config(ps, ws.AutoMatcherConfig().regex_mode(ws.REGEX_SPECULATIVE))
@@ -94,7 +105,7 @@ def test_proposer_training_and_exact_scan():
     assert 0.0 <= stats["top1"] <= stats["top4"] <= 1.0
     assert stats["top1"] > 0.5, stats
     got = m.scan_array(wl.data)
-    exp = oracle.scan_patterns(wl.patterns, wl.data)
+    exp = oracle.scan_patterns(pats, wl.data)
     assert len(exp) > 100
     assert np.array_equal(got, exp)
     # the plain kernel agrees as well

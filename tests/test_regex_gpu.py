@@ -116,7 +116,8 @@ def test_walk_image_layouts_vs_oracle(mode, wide):
     # most 32 byte classes, else by byte: a set over a few letters and one over
     # digits, letters and punctuation (more than 32 classes) take the two
     # layouts; both against the oracle, with small chunks so that the fix-up
-    # re-walks many chunks over the same image
+    # re-walks many chunks over the same image (one unbounded regex keeps the
+    # walk from deriving the chunk starts exactly)
     rng = np.random.default_rng(91 if wide else 92)
     alpha = (b"0123456789abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ_:=@!%,;/" if wide
              else b"abcdefghijkl")
@@ -126,15 +127,19 @@ def test_walk_image_layouts_vs_oracle(mode, wide):
         cls = b"[" + bytes(sorted(set(rng.choice(list(alpha), size=4).tolist()))) + b"]"
         src = b"(?:" + b"|".join(lits) + b")" + cls + b"{1,4}"
         pats.append((1, src))
+        if k == 0:
+            unbounded = (1, b"(?:" + b"|".join(lits) + b")" + cls + b"+")
     text = np.frombuffer(alpha, dtype=np.uint8)[rng.integers(0, len(alpha), 3 << 20)].copy()
     for k in range(400):  # plant matches: a pattern's first literal and one byte of its class
         src = pats[k % len(pats)][1].decode()
         lit = src[3:src.index("|")] + src[src.index("[") + 1]
         at = int(rng.integers(0, text.size - 16))
         text[at:at + len(lit)] = np.frombuffer(lit.encode(), dtype=np.uint8)
+    pats.append(unbounded)
     m = matcher(pats, mode=mode, walk_chunk=256)
     info = m.info()
     assert (info["max_classes"] > 32) == wide
+    assert info["exact_groups"] < info["n_groups"] - info["n_context_groups"]
     got = m.scan_array(text.tobytes())
     exp = oracle.scan_patterns(pats, text.tobytes())
     assert len(exp) > 100
@@ -152,13 +157,60 @@ def test_candidate_sets_plain_equals_speculative():
 
 @pytest.mark.parametrize("chunk", [256, 512, 4096])
 def test_chunk_boundaries_without_proposer(chunk):
-    # small chunks put many matches across chunk boundaries; with no proposer
-    # every boundary guess is the unanchored start, so the fix-up does the work
+    # small chunks put many matches across chunk boundaries; the walk derives
+    # each chunk's start from the bytes before it (every regex here matches at
+    # most 32 bytes, a quarter of 256 at most needs 64)
     pats, data = _regex_workload(1 << 20, 60, 7)
     m = matcher(pats, mode=SPEC, proposer=1, walk_chunk=chunk)
     got = m.scan_array(data)
     exp = oracle.scan_patterns(pats, data)
     assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("chunk", [4096, 8192])
+def test_exact_chunk_starts_need_no_fixup(chunk):
+    # every regex of the 500-regex configuration matches at most 32 bytes: the
+    # walk of each chunk starts from the state reached over the 32 bytes before
+    # it, which is the state of a walk from the input's start there, so every
+    # boundary holds and the fix-up re-walks nothing
+    pats, data = _regex_workload(8 << 20, 500, 3)
+    m = matcher(pats, mode=SPEC, proposer=1, walk_chunk=chunk, profile=True)
+    info = m.info()
+    spec = info["n_groups"] - info["n_context_groups"]
+    assert spec > 0 and info["exact_groups"] == spec
+    got = m.scan_array(data)
+    info = m.info()
+    assert info["last_fixup_chunks"] == 0 and info["last_rewalk_bytes"] == 0
+    assert info["last_guesses"] > 0 and info["last_guess_hits"] == info["last_guesses"]
+    exp = oracle.scan_patterns(pats, data)
+    assert len(exp) > 100 and np.array_equal(got, exp)
+
+
+def test_unbounded_and_long_regexes_keep_guessing():
+    # a group with an unbounded regex, or with one longer than 512 bytes, has
+    # no exact chunk starts: its boundaries are guessed and fixed up
+    rng = np.random.default_rng(17)
+    data = bytearray(rng.integers(ord("a"), ord("e"), size=1 << 20, dtype=np.uint8).tobytes())
+    for k in range(0, len(data) - 1200, 3000):
+        data[k:k + 1] = b"X"
+        data[k + 700:k + 701] = b"Y"
+    for pats in ([(1, b"X[a-d]+Y"), (1, b"(?:abc|dcb)[a-d]{2}")], [(1, b"X[a-d]{600,800}Y")]):
+        m = matcher(pats, mode=SPEC, proposer=1, walk_chunk=4096, profile=True)
+        assert m.info()["exact_groups"] == 0
+        got = m.scan_array(bytes(data))
+        exp = oracle.scan_patterns(pats, bytes(data))
+        assert len(exp) > 100 and np.array_equal(got, exp), pats
+    # several groups, the last one holding an unbounded regex: the others
+    # still start their chunks exactly
+    pats, text = _regex_workload(4 << 20, 500, 3)
+    pats = pats + [(1, b"~[0-9]+~")]
+    m = matcher(pats, mode=SPEC, proposer=1, dfa_max_states=16384, profile=True)
+    info = m.info()
+    spec = info["n_groups"] - info["n_context_groups"]
+    assert spec >= 2 and 0 < info["exact_groups"] < spec
+    got = m.scan_array(text)
+    exp = oracle.scan_patterns(pats, text)
+    assert len(exp) > 100 and np.array_equal(got, exp)
 
 
 def test_long_partial_matches_across_chunks():

@@ -76,7 +76,7 @@ class WsMatcherInfo(ctypes.Structure):
                 ("last_events", ctypes.c_uint64), ("last_rewalk_bytes", ctypes.c_uint64),
                 ("last_guess_hits", ctypes.c_uint64), ("last_guesses", ctypes.c_uint64),
                 ("regex_context", ctypes.c_uint32), ("n_context_groups", ctypes.c_uint32),
-                ("last_graph_replay", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("last_graph_replay", ctypes.c_uint32), ("exact_groups", ctypes.c_uint32)]
 
 
 class WsTuneReport(ctypes.Structure):

@@ -510,6 +510,12 @@ __global__ void __launch_bounds__(256) dfa_context_kernel(DevTables t, ScanPtrs 
 // hot-row lookups need; one 16-byte load per lane and step from 32 different
 // chunks would each take a wavefront and an L2 sector.  A lane whose chunk
 // is not a full one (the last, partial chunk) loads its bytes itself.
+// Whether a group's chunks start from their exact state: a bounded-length
+// group (GroupDev::warm) whose warm-up is at most a quarter of the chunk.
+__host__ __device__ __forceinline__ bool warm_exact(const GroupDev& gd, uint64_t chunk) {
+  return gd.warm != 0 && 4 * (uint64_t)gd.warm <= chunk;
+}
+
 template <bool kCls>
 __global__ void __launch_bounds__(kWalkThreads, 1)
     dfa_walk_kernel(DevTables t, ScanPtrs p, const __grid_constant__ CUtensorMap rows, uint64_t n_full) {
@@ -550,17 +556,40 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
   const uint64_t q = (uint64_t)g * p.n_chunks + i;
   const uint64_t c0 = i * p.chunk;
   const uint64_t c1 = active ? min(p.len, c0 + p.chunk) : c0;
+  // a bounded-length group derives each chunk's start state from the bytes
+  // before the chunk (exact); other groups start from the boundary guess
+  const bool exact = warm_exact(gd, p.chunk);
   uint32_t start = gd.start_unanchored;
+  if (active && i != 0 && !exact) start = p.guess[q];
+  if (start >= gd.n_states) start = gd.start_unanchored;  // a guess never written
+  uint32_t* ck = p.ckpt + q * p.nck;
+  uint32_t cold_row = 0;
+  uint32_t st = wstate(gi, start, H, (uint32_t)lane4, &cold_row);
+  if (exact && active && i != 0) {
+    // c0 >= chunk >= 4 * warm: the bytes [c0 - warm, c0) exist, 16-aligned
+    for (uint32_t k = 0; k < gd.warm; k += 16) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.data + c0 - gd.warm + k));
+      const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+      const uint32_t st0 = st;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const uint32_t b = __byte_perm(words[j >> 2], 0, 0x4440 + (j & 3));
+        st = max(WS_STEP_FAST(img, st, wcol<kCls>(cls_s, b)), (uint32_t)lane4);
+      }
+      if (st == gi.trap) {  // careful pass; matches before the chunk are not its own
+        st = st0;
+        for (int j = 0; j < 16; ++j)
+          trap_step<kCls>(img, gi, (words[j >> 2] >> (8 * (j & 3))) & 0xFFu, st, cold_row, H, (uint32_t)lane4,
+                          cls_s, tab, C);
+      }
+    }
+    start = wrow(gi, st, cold_row);
+  }
   if (active) {
-    if (i != 0) start = p.guess[q];
-    if (start >= gd.n_states) start = gd.start_unanchored;  // a guess never written
     p.used[q] = start;
     p.conv[q] = (uint32_t)c0;
     p.round[q] = 0;
   }
-  uint32_t* ck = p.ckpt + q * p.nck;
-  uint32_t cold_row = 0;
-  uint32_t st = wstate(gi, start, H, (uint32_t)lane4, &cold_row);
   // One 16-byte block: an optimistic pass over the image alone (a transition
   // that is not a plain hot one lands in the absorbing trap column, so the
   // block ends there), then, for a block that ended in the trap, a careful
@@ -779,8 +808,11 @@ __device__ void count_guess_hits(const DevTables& t, const ScanPtrs& p) {
        x += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t g = (uint32_t)(x / per);
     const uint64_t q = (uint64_t)g * p.n_chunks + x % per + 1;
-    uint32_t guess = p.guess[q];
-    if (guess >= t.groups[g].n_states) guess = t.groups[g].start_unanchored;
+    // the start the walk took: the derived state of an exact group (the
+    // fix-up leaves it untouched when it held), else the boundary guess
+    const GroupDev& gd = t.groups[g];
+    uint32_t guess = warm_exact(gd, p.chunk) ? p.used[q] : p.guess[q];
+    if (guess >= gd.n_states) guess = gd.start_unanchored;
     hits += guess == p.end[q - 1];
     seen += 1;
   }
@@ -1180,6 +1212,14 @@ void encode_chunk_rows(CUtensorMap* map, const uint8_t* data, uint64_t chunk, ui
   if (r != CUDA_SUCCESS) raise(WS_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the walk's input view");
 }
 
+}  // namespace
+
+bool regex_all_exact(const RegexPlan& P, uint64_t chunk) {
+  return P.n_spec > 0 && P.n_warm == P.n_spec && 4 * (uint64_t)P.max_warm <= chunk;
+}
+
+namespace {
+
 // Runs the candidate phase (plain or speculative) and leaves K in scratch.
 uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, uint32_t mode, cudaStream_t st,
                           int sm_count, cudaEvent_t* ev) {
@@ -1223,7 +1263,8 @@ uint32_t candidates_phase(RegexPlan& P, const DevTables& t, const ScanPtrs& p, u
     return launches;
   }
   dim3 cgrid(P.n_spec, (unsigned)((p.n_chunks + kWalkThreads - 1) / kWalkThreads));
-  if (P.proposer && P.use_proposer) {
+  // the walk ignores the guesses of groups with exact chunk starts
+  if (P.proposer && P.use_proposer && !regex_all_exact(P, p.chunk)) {
     launches += proposer_predict(*P.proposer, p.data, p.len, p.chunk, p.n_chunks, p.guess, st);
   } else {
     fill_guess_kernel<<<dim3(std::min<unsigned>((unsigned)((p.n_chunks + 255) / 256), 1024), P.n_spec), 256, 0, st>>>(t, p);
@@ -1602,10 +1643,22 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
   P.lfx.assign(8 * (size_t)t.n_regex, 0);
   P.pid.assign(t.regex_pattern_ids, t.regex_pattern_ids + t.n_regex);
   P.regex_group.assign(t.n_regex, 0);
+  P.n_warm = P.max_warm = 0;
   for (uint32_t g = 0; g < P.n_groups; ++g) {
     GroupBuild& gb = gbs[g];
     GroupDev& gd = P.groups[g];
     const uint32_t C = (uint32_t)gb.cls.count;
+    // exact chunk starts when every regex of a speculative group is bounded
+    int64_t gl = 0;
+    for (uint32_t r : gb.regexes) {
+      const int64_t ml = tree_max_len(trees[r]);
+      gl = (ml < 0 || gl < 0) ? -1 : std::max(gl, ml);
+    }
+    gd.warm = (g < P.n_spec && gl > 0 && gl <= (int64_t)kWarmMax) ? (uint32_t)((gl + 15) / 16 * 16) : 0u;
+    if (gd.warm) {
+      ++P.n_warm;
+      P.max_warm = std::max(P.max_warm, gd.warm);
+    }
     gd.rev_off = append_trans(gb.rev, P.rev);
     gd.rev_start = gb.rev.start_anchored;
     if ((uint64_t)gb.rev.n_states >= (1ull << kRmarkStateBits)) P.rev_marks = false;
@@ -1742,6 +1795,7 @@ void regex_fill_info(const RegexPlan& P, ws_matcher_info& info) {
   info.proposer_top1 = P.top1;
   info.proposer_top4 = P.top4;
   info.max_regex_len = P.n_regex ? P.max_len : 0;
+  info.exact_groups = P.n_warm;
 }
 
 namespace {

@@ -61,7 +61,17 @@ struct GroupDev {
   // The unanchored image of the walk: entries per row (256 byte-indexed, or
   // the group's class count when class-indexed) and the bytes staged.
   uint32_t img_cols, img_bytes;
+  // Speculative groups whose regexes all match at most L bytes (L <= kWarmMax):
+  // L rounded up to 16, else 0.  The state of the unanchored walk at a
+  // position depends only on the L bytes before it (an NFA thread that started
+  // earlier has died or matched), so walking those bytes from the unanchored
+  // start gives a chunk's exact start state.
+  uint32_t warm;
 };
+
+// Longest match for which a chunk's start state is derived from the bytes
+// before it (the walk reads them once per chunk: at most a quarter of a chunk).
+constexpr uint32_t kWarmMax = 512;
 
 struct Proposer;
 // Frees a trained proposer (ws_proposer.cu).
@@ -81,6 +91,9 @@ struct RegexPlan {
   uint32_t total_states = 0;
   uint32_t max_classes = 0;
   int64_t max_len = 0;                   // longest match (-1 unbounded)
+  // Speculative groups with exact chunk starts (GroupDev::warm > 0), and the
+  // largest warm length among them.
+  uint32_t n_warm = 0, max_warm = 0;
   bool rev_marks = false;                // reverse walks may share visited-state marks
   std::vector<GroupDev> groups;
   std::vector<uint32_t> regex_group;     // regex index -> group
@@ -155,6 +168,9 @@ void plan_regex(const ws_pattern_tables& t, const ws_config& cfg, int sm_count, 
 // rows in shared memory versus L2 is learned from the workload.
 void regex_rerank_from_corpus(RegexPlan& plan, const uint8_t* d_corpus, uint64_t len);
 void regex_fill_info(const RegexPlan& plan, ws_matcher_info& info);
+// True when every speculative group starts its chunks (of `chunk` bytes) from
+// their exact states, so that boundary guesses (and the proposer) are unused.
+bool regex_all_exact(const RegexPlan& plan, uint64_t chunk);
 // Enqueues the regex pipeline on `st`.  `events` (8 CUDA events) is non-null
 // when phase timing is wanted.  Returns the number of kernel launches.
 uint32_t run_regex_scan(RegexPlan& plan, const RegexLaunch& l, cudaStream_t st, DeviceBuffer& scratch,

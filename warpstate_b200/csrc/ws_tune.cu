@@ -9,7 +9,9 @@
 //     visits them (regex_rerank_from_corpus);
 //   - the walk chunk trades proposer and fix-up work (per boundary) against
 //     the parallelism of the walk;
-//   - the proposer is kept only where it beats guessing the unanchored start.
+//   - the proposer is kept only where it beats guessing the unanchored start,
+//     and trained only when some group has no exact chunk starts (regexes of
+//     unbounded length).
 // No counterpart in the reference (its regex path has no tunable walk).
 #include <cuda_runtime.h>
 
@@ -131,8 +133,12 @@ extern "C" ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint6
       }
 
       // 2. the proposer, in the chosen plan's state numbering
+      // (not when every group starts its chunks exactly: the walk would ignore
+      // its guesses at every chunk the scans can use, at least half the
+      // configured or smallest tuned chunk)
       bool trained = false;
-      if (m->cfg.proposer == WS_PROPOSER_MLP) {
+      const uint64_t min_chunk = (flags & WS_TUNE_CHUNK) ? 2048 : m->rx.walk_chunk / 2 / 256 * 256;
+      if (m->cfg.proposer == WS_PROPOSER_MLP && !regex_all_exact(m->rx, min_chunk)) {
         ProposerStats st;
         proposer_train(m->rx, dc, len, seed, m->ctx->sm_count, &st);
         m->rx.start_rate = st.start_rate;
