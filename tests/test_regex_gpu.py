@@ -158,8 +158,8 @@ def test_candidate_sets_plain_equals_speculative():
 @pytest.mark.parametrize("chunk", [256, 512, 4096])
 def test_chunk_boundaries_without_proposer(chunk):
     # small chunks put many matches across chunk boundaries; the walk derives
-    # each chunk's start from the bytes before it (every regex here matches at
-    # most 32 bytes, a quarter of 256 at most needs 64)
+    # each chunk's start from the 32 bytes before it (every regex here matches
+    # at most 32 bytes, and 4 x 32 <= 256)
     pats, data = _regex_workload(1 << 20, 60, 7)
     m = matcher(pats, mode=SPEC, proposer=1, walk_chunk=chunk)
     got = m.scan_array(data)
