@@ -331,7 +331,10 @@ void ws_hotswap_destroy(ws_hotswap* h);
  * memory, at least 64 KiB; 256 MiB is the intended size).  No counterpart in
  * the reference (its GPU regex path has no chunked walk).  Until it is called,
  * the walk guesses the unanchored start state at every chunk boundary; results
- * are exact either way (mispredicted chunks are re-walked). */
+ * are exact either way (mispredicted chunks are re-walked).  Groups whose
+ * regexes all match at most 512 bytes (ws_matcher_info.exact_groups) take no
+ * guess at all: each chunk starts from the state derived from the bytes before
+ * it. */
 ws_status ws_matcher_train_proposer(ws_matcher* m, const uint8_t* corpus, uint64_t len, uint64_t seed,
                                     ws_error_info* err);
 
@@ -339,7 +342,8 @@ ws_status ws_matcher_train_proposer(ws_matcher* m, const uint8_t* corpus, uint64
  * reference).  With WS_TUNE_GROUPS it rebuilds the merged group DFAs at
  * several size limits and keeps the plan whose scan of the corpus is fastest;
  * it then learns the hot-row placement from the corpus, trains the proposer
- * (when the config enables it) and, with WS_TUNE_CHUNK, times the speculative
+ * (when the config enables it and some group has no exact chunk starts) and,
+ * with WS_TUNE_CHUNK, times the speculative
  * walk at several chunk sizes with and without the proposer and keeps the
  * fastest.  Every choice gives the same matches; only speed differs.  The
  * corpus is host memory of at least 64 KiB; the timings scan it tiled to 1 GiB.
@@ -359,8 +363,8 @@ ws_status ws_matcher_tune(ws_matcher* m, const uint8_t* corpus, uint64_t len, ui
 
 /* Pins the speculative walk's chunk (bytes, a multiple of 256; 0 keeps the
  * current one) and whether the trained proposer (WS_PROPOSER_MLP) or the
- * unanchored start (WS_PROPOSER_NONE) supplies each chunk's start state,
- * overriding the autotuner's choice.  Matches never change.  No counterpart in
+ * unanchored start (WS_PROPOSER_NONE) supplies each chunk's start state in the
+ * groups without exact chunk starts, overriding the autotuner's choice.  Matches never change.  No counterpart in
  * the reference.  Call it between scans, not while scans run. */
 ws_status ws_matcher_set_walk(ws_matcher* m, uint32_t walk_chunk, uint32_t proposer, ws_error_info* err);
 
