@@ -882,21 +882,35 @@ __global__ void k_hist_kernel(ScanPtrs p) {
 }
 
 __global__ void k_scan_kernel(ScanPtrs p, uint32_t n_regex) {
-  // single block exclusive scan
-  __shared__ uint32_t part[1024];
+  // single-block exclusive scan (blockDim.x a multiple of 32, at most 1024):
+  // each thread sums a run of regexes, the runs are scanned across the block
+  // with warp shuffles, then each thread writes its run's offsets
+  __shared__ uint32_t wsum[32];
   const uint32_t per = (n_regex + blockDim.x - 1) / blockDim.x;
   const uint32_t a = threadIdx.x * per, b = min(n_regex, a + per);
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   uint32_t sum = 0;
   for (uint32_t r = a; r < b; ++r) sum += p.count[r];
-  part[threadIdx.x] = sum;
+  uint32_t incl = sum;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t acc = 0;
-    for (uint32_t k = 0; k < blockDim.x; ++k) { uint32_t x = part[k]; part[k] = acc; acc += x; }
-    p.offs[n_regex] = acc;
+  if (warp == 0) {
+    uint32_t v = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, d);
+      if (lane >= (uint32_t)d) v += y;
+    }
+    wsum[lane] = v;  // inclusive sums of the warps' runs
   }
   __syncthreads();
-  uint32_t acc = part[threadIdx.x];
+  if (threadIdx.x == 0) p.offs[n_regex] = wsum[nw - 1];
+  uint32_t acc = incl - sum + (warp ? wsum[warp - 1] : 0u);
   for (uint32_t r = a; r < b; ++r) { p.offs[r] = acc; p.cursor[r] = acc; acc += p.count[r]; }
 }
 
