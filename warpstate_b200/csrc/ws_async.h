@@ -58,4 +58,22 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int32_t
       : "memory");
 }
 
+// L2 policy that marks the lines a load brings in as the first to evict
+// (streamed input read once, so that it does not push tables out of L2).
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// tma_load_2d with an L2 cache policy (createpolicy) for the loaded lines.
+__device__ __forceinline__ void tma_load_2d_hint(void* dst, const void* tmap, int32_t x, int32_t y, uint64_t* bar,
+                                                 uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
 }  // namespace ws

@@ -537,13 +537,16 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
   uint64_t* bar = sbar + warp * 2;
   uint8_t* stg = stages + warp * 2 * kWalkStage;
   const uint64_t K = p.chunk / 16;  // 16-byte steps of a full chunk
+  // the input is read once: its lines go first when L2 needs room, which
+  // keeps the tables of the later kernels (reverse, resolution) resident
+  const uint64_t in_policy = l2_evict_first_policy();
   if (wtma && lane == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     mbar_init_fence();
     for (uint32_t s = 0; s < 2 && s < K; ++s) {
       mbar_expect_tx(&bar[s], kWalkStage);
-      tma_load_2d(stg + s * kWalkStage, &rows, (int32_t)(s * 16), (int32_t)wfirst, &bar[s]);
+      tma_load_2d_hint(stg + s * kWalkStage, &rows, (int32_t)(s * 16), (int32_t)wfirst, &bar[s], in_policy);
     }
   }
   __syncwarp();
@@ -636,7 +639,7 @@ __global__ void __launch_bounds__(kWalkThreads, 1)
       if (lane == 0 && k + 2 < K) {
         fence_proxy_async_smem();
         mbar_expect_tx(&bar[s], kWalkStage);
-        tma_load_2d(stg + s * kWalkStage, &rows, (int32_t)((k + 2) * 16), (int32_t)wfirst, &bar[s]);
+        tma_load_2d_hint(stg + s * kWalkStage, &rows, (int32_t)((k + 2) * 16), (int32_t)wfirst, &bar[s], in_policy);
       }
     }
     if (k >= nvec) continue;
