@@ -11,10 +11,12 @@
 //        plain:        one thread per start position walking the group's DFA
 //                      from its anchored start (the reference's form, with
 //                      every match reported instead of a bool), or
-//        speculative:  a chunk-parallel walk of the group's unanchored DFA from
-//                      proposed boundary states, exact fix-up of mispredicted
-//                      chunks, then a reverse-DFA walk from every match end to
-//                      enumerate the starts;
+//        speculative:  a chunk-parallel walk of the group's unanchored DFA,
+//                      each chunk from its exact start state (derived from the
+//                      bytes before it when every regex of the group is of
+//                      bounded length) or from a proposed one, exact fix-up of
+//                      mispredicted chunks, then a reverse-DFA walk from every
+//                      match end to enumerate the starts;
 //   2. resolution: per regex, starts sorted, and the regex crate's find_iter
 //      chain rebuilt: take the leftmost start, end it where the regex's
 //      leftmost-first DFA last matched, continue from that end.
