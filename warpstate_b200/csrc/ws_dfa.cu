@@ -196,10 +196,16 @@ __device__ __forceinline__ unsigned long long warp_append(unsigned long long* co
   return base + g.thread_rank();
 }
 
+// Appends a candidate and counts it for its regex (the per-regex counts size
+// the resolution's start lists).
 __device__ __forceinline__ void emit_k(const ScanPtrs& p, uint32_t r, uint32_t s, uint32_t e) {
   unsigned long long i = warp_append(&p.ctr[C_K]);
-  if (i < p.k_cap) p.k[i] = KCand{r, s, e};
-  else atomicOr(&p.ctr[C_ERR], 1ull);
+  if (i < p.k_cap) {
+    p.k[i] = KCand{r, s, e};
+    atomicAdd(&p.count[r], 1u);
+  } else {
+    atomicOr(&p.ctr[C_ERR], 1ull);
+  }
 }
 
 __device__ __forceinline__ void emit_event(const ScanPtrs& p, uint32_t e, uint32_t st, uint32_t q, uint32_t tag) {
@@ -878,12 +884,6 @@ __global__ void __launch_bounds__(256) dfa_reverse_kernel(DevTables t, ScanPtrs 
 }
 
 // ---------------------------------------------------------------- resolution
-__global__ void k_hist_kernel(ScanPtrs p) {
-  unsigned long long n = min(p.ctr[C_K], (unsigned long long)p.k_cap);
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
-    atomicAdd(&p.count[p.k[k].r], 1u);
-}
-
 __global__ void k_scan_kernel(ScanPtrs p, uint32_t n_regex) {
   // single-block exclusive scan (blockDim.x a multiple of 32, at most 1024):
   // each thread sums a run of regexes, the runs are scanned across the block
@@ -1874,14 +1874,13 @@ uint32_t run_regex_scan(RegexPlan& P, const RegexLaunch& l, cudaStream_t st, Dev
   if (ev) check_cuda(cudaEventRecord(ev[0], st), "event");
   launches += candidates_phase(P, t, p, l.mode, st, sm_count, ev);
   int hg = (int)std::min<uint64_t>((uint64_t)sm_count * 8, (L.k_cap + 255) / 256);
-  k_hist_kernel<<<hg, 256, 0, st>>>(p);
   k_scan_kernel<<<1, 1024, 0, st>>>(p, P.n_regex);
   k_scatter_kernel<<<hg, 256, 0, st>>>(p);
   k_sort_kernel<<<(unsigned)std::min<uint32_t>(P.n_regex, 4096), 512, 0, st>>>(p, P.n_regex);
   k_lf_kernel<<<sm_count * 8, 128, P.n_regex < kLfOffsShared ? (P.n_regex + 1) * 4 : 0, st>>>(t, p, P.n_regex);
   k_chain_kernel<<<(P.n_regex + 3) / 4, 128, 0, st>>>(t, p);  // a warp per regex
   check_cuda(cudaGetLastError(), "resolution kernels");
-  launches += 6;
+  launches += 5;
   finalize_kernel<<<1, 1, 0, st>>>(p, l.need);
   check_cuda(cudaGetLastError(), "finalize_kernel");
   launches += 1;
