@@ -38,3 +38,16 @@ def test_reference_arm_line():
 
 def test_reference_arm_other_ranks_exit_quietly():
     assert _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
+
+
+def test_boundary_guess_labels():
+    # the regex record names how the walk chose its chunk starts: exact when
+    # every speculative group starts exactly, else the tuner's choice
+    sys.path.insert(0, str(ROOT))
+    import bench
+    info = {"n_groups": 3, "n_context_groups": 1, "exact_groups": 2}
+    assert bench.boundary_guess(info, None).startswith("exact")
+    info["exact_groups"] = 1
+    assert bench.boundary_guess(info, {"proposer_used": 1}) == "learned proposer (top-1)"
+    assert bench.boundary_guess(info, {"proposer_used": 0}).startswith("unanchored")
+    assert bench.boundary_guess(dict(info, n_groups=1, n_context_groups=1, exact_groups=0), None).startswith("unanchored")
